@@ -1,0 +1,102 @@
+"""ctypes binding of libagimp.so (the C ABI declared in include/agimp.h).
+
+This is the product path: it loads the in-tree CUDA library and raises if it
+cannot; there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libagimp.so")
+
+AGIMP_MEM_DEVICE = 0
+AGIMP_MEM_HOST = 1
+
+ERR_OOB = 1
+ERR_ESCAPED = 2
+ERR_MAP_OOB = 4
+ERR_NOBIN = 8
+
+# every symbol include/agimp.h declares
+EXPORTS = (
+    "agimp_abi_version", "agimp_status_string", "agimp_default_params", "agimp_create", "agimp_destroy",
+    "agimp_last_error", "agimp_set_particles", "agimp_get_particles", "agimp_set_level_map",
+    "agimp_clear_level_map", "agimp_substep", "agimp_set_graphs", "agimp_refine_levels", "agimp_get_grid",
+    "agimp_get_node_mask", "agimp_errors", "agimp_get_stats", "agimp_kernels_per_substep",
+    "agimp_profile_substep",
+)
+PHASES = ("blocks", "topology", "binning", "p2g", "restrict", "gridop", "prolong", "g2p")
+
+
+class Params(ctypes.Structure):
+    _fields_ = [
+        ("dim", ctypes.c_int32), ("level", ctypes.c_int32), ("coarsest_size", ctypes.c_int32),
+        ("boundary_gap", ctypes.c_int32), ("boundary_mode", ctypes.c_int32), ("plasticity", ctypes.c_int32),
+        ("n_particles", ctypes.c_int64), ("radius", ctypes.c_double), ("gravity", ctypes.c_double * 3),
+        ("E", ctypes.c_double), ("nu", ctypes.c_double), ("theta_c", ctypes.c_double),
+        ("theta_s", ctypes.c_double), ("hardening", ctypes.c_double), ("n_colliders", ctypes.c_int32),
+        ("colliders", (ctypes.c_double * 6) * 4),
+    ]
+
+
+class Stats(ctypes.Structure):
+    _fields_ = [("active_blocks", ctypes.c_int32 * 8), ("n_binned", ctypes.c_int32), ("n_chunks", ctypes.c_int32),
+                ("substeps", ctypes.c_int64)]
+
+
+class AgimpError(RuntimeError):
+    pass
+
+
+_lib = None
+
+
+def load(path: str | None = None):
+    """Load libagimp.so; build it first when it is missing and nvcc exists."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    path = path or LIB_PATH
+    if not os.path.exists(path):
+        from . import build as _build
+        _build.build()
+    L = ctypes.CDLL(path)
+    vp, fp, ip = ctypes.c_void_p, ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_int32)
+    L.agimp_abi_version.restype = ctypes.c_int
+    L.agimp_status_string.restype = ctypes.c_char_p
+    L.agimp_status_string.argtypes = [ctypes.c_int]
+    L.agimp_default_params.argtypes = [ctypes.POINTER(Params), ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
+                                       ctypes.c_int64]
+    L.agimp_create.argtypes = [ctypes.POINTER(Params), ctypes.c_int32, ctypes.POINTER(vp)]
+    L.agimp_destroy.argtypes = [vp]
+    L.agimp_last_error.restype = ctypes.c_char_p
+    L.agimp_last_error.argtypes = [vp]
+    L.agimp_set_particles.argtypes = [vp, vp, vp, vp, vp, vp, vp, vp, ctypes.c_int32, vp]
+    L.agimp_get_particles.argtypes = [vp, vp, vp, vp, vp, vp, vp, vp, vp, ctypes.c_int32, vp]
+    L.agimp_set_level_map.argtypes = [vp, vp, ctypes.c_int32, ctypes.c_int32, vp]
+    L.agimp_clear_level_map.argtypes = [vp]
+    L.agimp_substep.argtypes = [vp, ctypes.c_float, ctypes.c_int32, vp]
+    L.agimp_set_graphs.argtypes = [vp, ctypes.c_int32]
+    L.agimp_refine_levels.argtypes = [vp, ctypes.c_int32, vp]
+    L.agimp_get_grid.argtypes = [vp, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, vp, vp, vp, ctypes.c_int32, vp]
+    L.agimp_get_node_mask.argtypes = [vp, vp, ctypes.c_int32, vp]
+    L.agimp_errors.argtypes = [vp, ctypes.POINTER(ctypes.c_uint32), ctypes.c_int32]
+    L.agimp_get_stats.argtypes = [vp, ctypes.POINTER(Stats)]
+    L.agimp_kernels_per_substep.argtypes = [vp]
+    L.agimp_kernels_per_substep.restype = ctypes.c_int32
+    L.agimp_profile_substep.argtypes = [vp, ctypes.c_float, fp, ctypes.c_int32, vp]
+    _lib = L
+    return L
+
+
+def check(status: int, handle=None, what: str = ""):
+    if status != 0:
+        L = load()
+        msg = L.agimp_status_string(status).decode()
+        if handle:
+            detail = L.agimp_last_error(handle).decode()
+            if detail:
+                msg += ": " + detail
+        raise AgimpError("%s failed (%d): %s" % (what or "agimp call", status, msg))

@@ -1,0 +1,238 @@
+"""Scene generators and level maps.
+
+* ``initialize_mask1`` .. ``initialize_mask5``: the reference's static level
+  maps (init.py:34-98) restated as vectorised grid initializers: given finest
+  cell indices ``I[..., dim]`` they return ``(level, activate)``.
+* ``make_config(k)``: seeded synthetic scenes with the shapes, sizes and
+  materials of the benchmark configurations (numpy PCG64, seed 0 by default).
+  Particles fill boxes / spheres on a sub-lattice of the finest cells (2 per
+  axis per cell: 4 per cell in 2D, 8 in 3D) with uniform jitter of +-0.5
+  sub-spacing.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+
+import numpy as np
+
+
+def _vec(fn):
+    fn.vectorized = True
+    return fn
+
+
+def _inner(I, sz):
+    return np.all((I >= 8) & (I < sz - 8), axis=-1)
+
+
+@_vec
+def initialize_mask1(sim, I):
+    """init.py:34-37: every cell at the finest level."""
+    lv = np.full(I.shape[:-1], sim.level - 1)
+    return lv, np.ones(lv.shape, bool)
+
+
+@_vec
+def initialize_mask2(sim, I):
+    """init.py:39-49: level 0 in the left half (8-cell margin), else level 3."""
+    sz = sim.finest_size
+    left = (I[..., 0] < sz / 2) & _inner(I, sz)
+    return np.where(left, 0, 3), np.ones(left.shape, bool)
+
+
+@_vec
+def initialize_mask3(sim, I):
+    """init.py:51-64: levels 0 / 1 / 2 in vertical bands."""
+    sz = sim.finest_size
+    inner = _inner(I, sz)
+    lv = np.where((I[..., 0] < sz / 4) & inner, 0, np.where((I[..., 0] < sz / 2) & inner, 1, 2))
+    return lv, np.ones(lv.shape, bool)
+
+
+@_vec
+def initialize_mask4(sim, I):
+    """init.py:66-80: levels 1 / 2 in the left half, 3 elsewhere in range;
+    out-of-range cells return 3 without activating."""
+    sz = sim.finest_size
+    left = (I[..., 0] < sz / 2) & _inner(I, sz)
+    inr = np.all((I >= 0) & (I < sz), axis=-1)
+    lv = np.where(left, np.where(I[..., 1] < sz / 2, 1, 2), 3)
+    return lv, left | inr
+
+
+@_vec
+def initialize_mask5(sim, I):
+    """init.py:82-98: levels 0 / 1 / 2 in the left half, 3 elsewhere in range."""
+    sz = sim.finest_size
+    left = (I[..., 0] < sz / 2) & _inner(I, sz)
+    inr = np.all((I >= 0) & (I < sz), axis=-1)
+    lv = np.where(left, np.where(I[..., 1] < sz / 4, 0, np.where(I[..., 1] < sz / 2, 1, 2)), 3)
+    return lv, left | inr
+
+
+REFERENCE_MASKS = {1: initialize_mask1, 2: initialize_mask2, 3: initialize_mask3, 4: initialize_mask4,
+                   5: initialize_mask5}
+
+
+def band_level_map(boxes, dim, level, coarsest_size, near=2, mid=4, floor_y=0.25):
+    """Static level map aligned to coarsest cells: the finest level within
+    `near` coarsest cells (Chebyshev) of any box or below `floor_y`, level
+    level-2 within `mid` cells, level 0 elsewhere; halo cells return level-1
+    without activating."""
+    nc = coarsest_size
+    cov = np.zeros((nc,) * dim, bool)
+    for lo, hi in boxes:
+        sl = tuple(slice(int(np.floor(a * nc)), int(np.ceil(b * nc))) for a, b in zip(lo, hi))
+        cov[sl] = True
+    dist = np.full(cov.shape, 1 << 20)
+    idx = np.argwhere(cov)
+    grid = np.stack(np.meshgrid(*[np.arange(nc)] * dim, indexing="ij"), -1)
+    for chunk in np.array_split(idx, max(1, len(idx) // 256)):
+        if len(chunk):
+            d = np.abs(grid[..., None, :] - chunk[None]).max(-1).min(-1)
+            dist = np.minimum(dist, d)
+    y_center = (np.arange(nc) + 0.5) / nc
+    ylow = np.broadcast_to(y_center.reshape((1, nc) + (1,) * (dim - 2)), cov.shape) < floor_y
+    coarse_lv = np.where((dist <= near) | ylow, level - 1, np.where(dist <= mid, max(level - 2, 0), 0))
+    sz = nc << (level - 1)
+    s = level - 1
+
+    @_vec
+    def grid_initializer(sim, I):
+        inr = np.all((I >= 0) & (I < sz), axis=-1)
+        C = np.clip(I >> s, 0, nc - 1)
+        lv = coarse_lv[tuple(np.moveaxis(C, -1, 0))]
+        return np.where(inr, lv, level - 1), inr
+
+    return grid_initializer
+
+
+# ---------------------------------------------------------------------------
+def fill_lattice(rng, dim, finest, inside, lo, hi, per_axis=2, jitter=True):
+    """Points on the sub-lattice (per_axis per finest cell and axis) inside the
+    region lo..hi that satisfy inside(points)."""
+    h = 1.0 / (finest * per_axis)
+    axes = [np.arange(np.floor(a / h), np.ceil(b / h)) * h + 0.5 * h for a, b in zip(lo, hi)]
+    mesh = np.stack(np.meshgrid(*axes, indexing="ij"), -1).reshape(-1, dim)
+    if jitter:
+        mesh = mesh + rng.uniform(-0.5 * h, 0.5 * h, mesh.shape)
+    return mesh[inside(mesh)].astype(np.float32)
+
+
+def box_region(lo, hi):
+    lo, hi = np.asarray(lo), np.asarray(hi)
+    return lambda p: np.all((p >= lo) & (p < hi), axis=1), lo, hi
+
+
+def sphere_region(c, r):
+    c = np.asarray(c)
+    return lambda p: ((p - c) ** 2).sum(1) < r * r, c - r, c + r
+
+
+@dataclass
+class Scene:
+    name: str
+    dim: int
+    level: int
+    coarsest: int
+    x: np.ndarray
+    v: np.ndarray
+    g: np.ndarray
+    m: np.ndarray
+    dt: float
+    steps: int
+    sim_kwargs: dict = field(default_factory=dict)
+    grid_initializer: object = None
+    refine_every: int = 0
+    refine_band: int = 3
+    description: str = ""
+
+    @property
+    def n(self):
+        return len(self.x)
+
+    def build(self, **over):
+        """Construct an AdaptiveGIMP for this scene."""
+        from .simulator import AdaptiveGIMP
+        kw = dict(self.sim_kwargs)
+        kw.update(over)
+        d = self.dim
+        n = self.n
+        F = np.tile(np.eye(d, dtype=np.float32), (n, 1, 1))
+
+        def pinit(sim):
+            sim.set_particles(x=self.x, v=self.v, F=F, C=np.zeros((n, d, d), np.float32), m=self.m, g=self.g,
+                              Jp=np.ones(n, np.float32))
+
+        return AdaptiveGIMP(d, self.level, self.coarsest, n, pinit, self.grid_initializer, **kw)
+
+
+def _mass(rho, finest, dim, ppc):
+    return np.float32(rho * (1.0 / finest) ** dim / ppc)
+
+
+def make_config(k, seed=0, scale=1.0):
+    """Benchmark configurations 1..5 (scale < 1 shrinks the bodies for tests)."""
+    rng = np.random.default_rng(seed)
+    if k == 1:
+        L, c = 3, 64
+        fin = c << (L - 1)
+        boxes = [((0.3 - 0.1 * scale, 0.5 - 0.1 * scale), (0.3 + 0.1 * scale, 0.5 + 0.1 * scale)),
+                 ((0.6 - 0.1 * scale, 0.7 - 0.1 * scale), (0.6 + 0.1 * scale, 0.7 + 0.1 * scale))]
+        xs = [fill_lattice(rng, 2, fin, *box_region(lo, hi)) for lo, hi in boxes]
+        x = np.concatenate(xs)
+        n = len(x)
+        return Scene("config1_2d_static", 2, L, c, x, np.zeros((n, 2), np.float32), np.full(n, L - 1, np.int32),
+                     np.full(n, _mass(1.0, fin, 2, 4)), 1e-4, 1000,
+                     dict(E=1e4, nu=0.2, gravity=(0.0, -9.8), boundary_mode="sticky"),
+                     grid_initializer=band_level_map(boxes, 2, L, c),
+                     description="2D static 3-level quadtree 64^2..256^2, two elastic boxes 0.2x0.2, 4 ppc")
+    if k == 2:
+        L, c = 4, 64
+        fin = c << (L - 1)
+        xs, vs = [], []
+        for _ in range(3):
+            side = rng.uniform(0.1, 0.25, 2) * scale
+            lo = rng.uniform(0.1, 0.9 - side)
+            pts = fill_lattice(rng, 2, fin, *box_region(lo, lo + side))
+            xs.append(pts)
+            vs.append(np.tile(rng.uniform(-1, 1, 2).astype(np.float32), (len(pts), 1)))
+        x, v = np.concatenate(xs), np.concatenate(vs)
+        n = len(x)
+        return Scene("config2_2d_dynamic", 2, L, c, x, v, np.full(n, L - 1, np.int32),
+                     np.full(n, _mass(1.0, fin, 2, 4)), 5e-5, 2000,
+                     dict(E=1.4e5, nu=0.2, gravity=(0.0, -9.8), boundary_mode="sticky", plasticity="snow",
+                          theta_c=2.5e-2, theta_s=7.5e-3, hardening=10.0),
+                     refine_every=10, refine_band=3,
+                     description="2D dynamic 4 levels 64^2..512^2, 3 random snow boxes, 4 ppc, re-refined every 10")
+    if k == 3:
+        L, c = 3, 64
+        fin = c << (L - 1)
+        r = 0.15 * scale
+        x = fill_lattice(rng, 3, fin, *sphere_region((0.5, 0.6, 0.5), r))
+        n = len(x)
+        v = np.tile(np.array([0.0, -3.0, 0.0], np.float32), (n, 1))
+        slab = (0.3, 0.2, 0.3, 0.7, 0.3, 0.7)
+        return Scene("config3_3d_dynamic", 3, L, c, x, v, np.full(n, L - 1, np.int32),
+                     np.full(n, _mass(1.0, fin, 3, 8)), 5e-5, 1000,
+                     dict(E=1e5, nu=0.25, gravity=(0.0, -9.8, 0.0), boundary_mode="sticky", plasticity="snow",
+                          theta_c=2.5e-2, theta_s=7.5e-3, hardening=10.0, colliders=(slab,)),
+                     refine_every=10, refine_band=3,
+                     description="3D dynamic 3 levels 64^3..256^3, snow sphere r=0.15 at y=0.6 moving down at 3 "
+                                 "onto a 0.4x0.1x0.4 static slab collider, 8 ppc")
+    if k == 5:
+        L, c = 4, 64
+        fin = c << (L - 1)
+        r = 0.12 * scale
+        a = fill_lattice(rng, 3, fin, *sphere_region((0.35, 0.5, 0.5), r))
+        b = fill_lattice(rng, 3, fin, *sphere_region((0.65, 0.5, 0.5), r))
+        x = np.concatenate([a, b])
+        v = np.concatenate([np.tile(np.array([2.0, 0, 0], np.float32), (len(a), 1)),
+                            np.tile(np.array([-2.0, 0, 0], np.float32), (len(b), 1))])
+        n = len(x)
+        return Scene("config5_3d_two_spheres", 3, L, c, x, v, np.full(n, L - 1, np.int32),
+                     np.full(n, _mass(1.0, fin, 3, 8)), 3e-5, 1000,
+                     dict(E=1.4e5, nu=0.2, gravity=(0.0, -9.8, 0.0), boundary_mode="sticky", plasticity="snow"),
+                     refine_every=10, refine_band=3,
+                     description="3D 4 levels 64^3..512^3, two colliding snow spheres r=0.12 at +-2")
+    raise ValueError("unknown config %r" % k)

@@ -1,0 +1,601 @@
+// C ABI of libagimp.so (declared in include/agimp.h).
+//
+// Host side of the reference's AdaptiveGIMP class (adaptive_gimp.py:4-352):
+// storage allocation (__init__), particle and level-map upload (the
+// particle_initializer / grid_initializer hooks), substep() and field
+// readback.  Every kernel launch is stream-ordered; the substep is captured as
+// a CUDA graph once per (dt, stream) and replayed.
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/agimp.h"
+#include "common.cuh"
+
+using namespace agimp;
+
+struct agimp_sim {
+  Ctx c;
+  agimp_params p;
+  int device = 0;
+  std::string err;
+  std::vector<void*> allocs;
+  bool graphs = true;
+  cudaGraphExec_t gexec = nullptr;
+  float g_dt = NAN;
+  cudaStream_t g_stream = nullptr;
+  cudaStream_t internal = nullptr;
+  cudaEvent_t ev_in = nullptr, ev_out = nullptr;
+  float* staging = nullptr;
+  size_t staging_floats = 0;
+  int8_t* map_dev = nullptr;
+  long long substeps = 0;
+};
+
+namespace {
+
+agimp_status fail(agimp_sim* s, agimp_status st, const std::string& msg) {
+  if (s) s->err = msg;
+  return st;
+}
+
+agimp_status cuda_fail(agimp_sim* s, cudaError_t e, const char* what) {
+  return fail(s, AGIMP_CUDA_ERROR, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+#define CK(call)                                        \
+  do {                                                  \
+    cudaError_t e_ = (call);                            \
+    if (e_ != cudaSuccess) return cuda_fail(s, e_, #call); \
+  } while (0)
+
+template <typename T>
+cudaError_t dalloc(agimp_sim* s, T** ptr, size_t count) {
+  void* p = nullptr;
+  cudaError_t e = cudaMalloc(&p, count * sizeof(T) + 16);
+  if (e != cudaSuccess) return e;
+  s->allocs.push_back(p);
+  *ptr = (T*)p;
+  return cudaSuccess;
+}
+
+// RAII: run library work on the caller's stream, or on an internal stream
+// ordered after / before the legacy default stream when the caller passes NULL
+// (a graph cannot be captured on the legacy stream).
+struct StreamUse {
+  agimp_sim* s;
+  cudaStream_t user, use;
+  StreamUse(agimp_sim* s_, void* stream) : s(s_), user((cudaStream_t)stream) {
+    use = user ? user : s->internal;
+    if (!user) {
+      cudaEventRecord(s->ev_in, 0);
+      cudaStreamWaitEvent(s->internal, s->ev_in, 0);
+    }
+  }
+  ~StreamUse() {
+    if (!user) {
+      cudaEventRecord(s->ev_out, s->internal);
+      cudaStreamWaitEvent(0, s->ev_out, 0);
+    }
+  }
+};
+
+__global__ void k_aos_to_soa(const float* __restrict__ aos, float* __restrict__ soa, long long n, int comps) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n * comps;
+       i += (long long)gridDim.x * blockDim.x) {
+    const long long p = i / comps;
+    const int c = (int)(i % comps);
+    soa[c * n + p] = aos[i];
+  }
+}
+
+__global__ void k_soa_to_aos(const float* __restrict__ soa, float* __restrict__ aos, long long n, int comps) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n * comps;
+       i += (long long)gridDim.x * blockDim.x) {
+    const long long p = i / comps;
+    const int c = (int)(i % comps);
+    aos[i] = soa[c * n + p];
+  }
+}
+
+template <int D>
+__global__ void k_get_grid(Ctx c, int l, int lo, int n, long long off, long long cnt, float* m, float* v,
+                           int32_t* cell) {
+  const LevelDev& V = c.lev[l];
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < cnt; i += (long long)gridDim.x * blockDim.x) {
+    long long o = off + i;
+    int I[D];
+#pragma unroll
+    for (int d = D - 1; d >= 0; --d) {
+      I[d] = (int)(o % n) + lo;
+      o /= n;
+    }
+    float4 nd = make_float4(0.f, 0.f, 0.f, 0.f);
+    uint32_t cm = 0;
+    if (in_store<D>(V, I)) {
+      const long long e = elem_of<D>(V, I);
+      nd = V.node[e];
+      cm = V.cell[e] & ~CUL;
+    }
+    if (m) m[i] = nd.w;
+    if (v) {
+      v[i * D] = nd.x;
+      v[i * D + 1] = nd.y;
+      if (D == 3) v[i * D + 2] = nd.z;
+    }
+    if (cell) cell[i] = (int32_t)cm;
+  }
+}
+
+template <int D>
+__global__ void k_get_nmask(Ctx c, long long off, long long cnt, int32_t* out) {
+  const int n = c.sz + 1;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < cnt; i += (long long)gridDim.x * blockDim.x) {
+    long long o = off + i;
+    int P[D];
+#pragma unroll
+    for (int d = D - 1; d >= 0; --d) {
+      P[d] = (int)(o % n);
+      o /= n;
+    }
+    out[i] = (int32_t)c.nmask[elem_of<D>(c.lev[c.L - 1], P)];
+  }
+}
+
+int gs_blocks(long long n) {
+  long long b = (n + 255) / 256;
+  if (b > 65535) b = 65535;
+  return (int)(b < 1 ? 1 : b);
+}
+
+}  // namespace
+
+extern "C" {
+
+int agimp_abi_version(void) { return AGIMP_ABI_VERSION; }
+
+const char* agimp_status_string(agimp_status st) {
+  switch (st) {
+    case AGIMP_OK: return "ok";
+    case AGIMP_INVALID_ARG: return "invalid argument";
+    case AGIMP_CAPACITY: return "capacity exceeded";
+    case AGIMP_NAN: return "non-finite value";
+    case AGIMP_DEVICE_TIMEOUT: return "device wait timed out";
+    case AGIMP_CUDA_ERROR: return "CUDA error";
+    case AGIMP_NOT_READY: return "not ready";
+    case AGIMP_OUT_OF_MEMORY: return "out of device memory";
+  }
+  return "unknown status";
+}
+
+void agimp_default_params(agimp_params* p, int32_t dim, int32_t level, int32_t coarsest_size, int64_t n) {
+  std::memset(p, 0, sizeof(*p));
+  p->dim = dim;
+  p->level = level;
+  p->coarsest_size = coarsest_size;
+  p->boundary_gap = 4;
+  p->boundary_mode = 0;
+  p->plasticity = 0;
+  p->n_particles = n;
+  p->radius = 0.5;
+  p->gravity[1] = -100.0;
+  p->E = 5e3;
+  p->nu = 0.2;
+  p->theta_c = 2.5e-2;
+  p->theta_s = 7.5e-3;
+  p->hardening = 10.0;
+}
+
+const char* agimp_last_error(const agimp_sim* s) { return s ? s->err.c_str() : "null handle"; }
+
+agimp_status agimp_create(const agimp_params* p, int32_t device, agimp_sim** out) {
+  if (!p || !out) return AGIMP_INVALID_ARG;
+  *out = nullptr;
+  if ((p->dim != 2 && p->dim != 3) || p->level < 1 || p->level > MAXL || p->coarsest_size < 4 ||
+      (p->coarsest_size & (p->coarsest_size - 1)) || p->n_particles < 0 || p->n_particles > (int64_t)1 << 30 ||
+      p->n_colliders < 0 || p->n_colliders > 4 || !(p->radius > 0.0 && p->radius <= 0.5) ||
+      (p->coarsest_size << (p->level - 1)) > (1 << 13) || p->plasticity < 0 || p->plasticity > 1)
+    return AGIMP_INVALID_ARG;
+  agimp_sim* s = new agimp_sim();
+  s->p = *p;
+  s->device = device;
+  cudaError_t e = cudaSetDevice(device);
+  if (e != cudaSuccess) {
+    delete s;
+    return AGIMP_CUDA_ERROR;
+  }
+  Ctx& c = s->c;
+  std::memset(&c, 0, sizeof(c));
+  const int D = p->dim;
+  c.dim = D;
+  c.L = p->level;
+  c.coarsest = p->coarsest_size;
+  c.sz = p->coarsest_size << (p->level - 1);
+  c.N = (int)p->n_particles;
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+  c.sms = sms;
+  c.gap = p->boundary_gap;
+  c.bmode = p->boundary_mode;
+  c.plast = p->plasticity;
+  c.radius = (float)p->radius;
+  const double mu = p->E / (2.0 * (1.0 + p->nu)), la = p->E * p->nu / ((1.0 + p->nu) * (1.0 - 2.0 * p->nu));
+  c.mu = (float)mu;
+  c.la = (float)la;
+  c.theta_c = (float)p->theta_c;
+  c.theta_s = (float)p->theta_s;
+  c.xi = (float)p->hardening;
+  for (int d = 0; d < 3; ++d) c.grav[d] = (float)p->gravity[d];
+  c.ncol = p->n_colliders;
+  for (int k = 0; k < 4; ++k)
+    for (int j = 0; j < 6; ++j) c.col[k][j] = p->colliders[k][j];
+  const int per = 1 << (2 * D);
+  long long tot_blocks = 0;
+#define AL(ptr, n)                                   \
+  do {                                               \
+    if (dalloc(s, &(ptr), (size_t)(n)) != cudaSuccess) { \
+      agimp_destroy(s);                              \
+      return AGIMP_OUT_OF_MEMORY;                    \
+    }                                                \
+  } while (0)
+  for (int l = 0; l < c.L; ++l) {
+    LevelDev& V = c.lev[l];
+    V.size = c.coarsest << l;
+    V.nb = V.size / 4 + 3;
+    V.nblocks = 1;
+    for (int d = 0; d < D; ++d) V.nblocks *= V.nb;
+    tot_blocks += V.nblocks;
+    AL(V.cell, V.nblocks * per);
+    AL(V.node, V.nblocks * per);
+    AL(V.bmap, V.nblocks);
+    AL(V.blist, V.nblocks);
+    cudaMemset(V.cell, 0, V.nblocks * per * sizeof(uint32_t));
+    cudaMemset(V.node, 0, V.nblocks * per * sizeof(float4));
+    cudaMemset(V.bmap, 0xff, V.nblocks * sizeof(int32_t));
+  }
+  const LevelDev& Vf = c.lev[c.L - 1];
+  AL(c.nmask, Vf.nblocks * per);
+  {
+    long long cells = 1;
+    for (int d = 0; d < D; ++d) cells *= c.sz;
+    AL(c.occ, cells);
+  }
+  cudaMemset(c.nmask, 0, Vf.nblocks * per * sizeof(uint32_t));
+  AL(c.ctr, CTR_COUNT);
+  cudaMemset(c.ctr, 0, CTR_COUNT * sizeof(int32_t));
+  AL(c.touch_flag, Vf.nblocks);
+  AL(c.touch_list, Vf.nblocks);
+  cudaMemset(c.touch_flag, 0, Vf.nblocks * sizeof(uint32_t));
+  AL(c.bin_count, tot_blocks);
+  AL(c.bin_start, tot_blocks);
+  cudaMemset(c.bin_count, 0, tot_blocks * sizeof(int32_t));
+  const long long N = c.N;
+  AL(c.chunks, N / CHUNK + tot_blocks + 1);
+  AL(c.bin_of, N + 1);
+  AL(c.rank_of, N + 1);
+  AL(c.perm, N + 1);
+  AL(c.x, D * N + 1);
+  AL(c.v, D * N + 1);
+  AL(c.F, D * D * N + 1);
+  AL(c.C, D * D * N + 1);
+  AL(c.m, N + 1);
+  AL(c.Jp, N + 1);
+  AL(c.g, N + 1);
+  AL(c.fl, N + 1);
+  cudaMemset(c.x, 0, (D * N + 1) * sizeof(float));
+  cudaMemset(c.v, 0, (D * N + 1) * sizeof(float));
+  cudaMemset(c.F, 0, (D * D * N + 1) * sizeof(float));
+  cudaMemset(c.C, 0, (D * D * N + 1) * sizeof(float));
+  cudaMemset(c.m, 0, (N + 1) * sizeof(float));
+  cudaMemset(c.g, 0, (N + 1) * sizeof(int32_t));
+  cudaMemset(c.fl, 0xff, (N + 1) * sizeof(int32_t));
+  s->staging_floats = std::max<size_t>((size_t)1 << 20, (size_t)(D * D * N));
+  AL(s->staging, s->staging_floats);
+  {
+    // Jp starts at 1
+    std::vector<float> ones(N + 1, 1.0f);
+    cudaMemcpy(c.Jp, ones.data(), (N + 1) * sizeof(float), cudaMemcpyHostToDevice);
+  }
+#undef AL
+  if (cudaStreamCreateWithFlags(&s->internal, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&s->ev_in, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&s->ev_out, cudaEventDisableTiming) != cudaSuccess) {
+    agimp_destroy(s);
+    return AGIMP_CUDA_ERROR;
+  }
+  e = cudaDeviceSynchronize();
+  if (e != cudaSuccess) {
+    agimp_destroy(s);
+    return AGIMP_CUDA_ERROR;
+  }
+  *out = s;
+  return AGIMP_OK;
+}
+
+agimp_status agimp_destroy(agimp_sim* s) {
+  if (!s) return AGIMP_INVALID_ARG;
+  cudaSetDevice(s->device);
+  cudaDeviceSynchronize();
+  if (s->gexec) cudaGraphExecDestroy(s->gexec);
+  for (void* p : s->allocs) cudaFree(p);
+  if (s->map_dev) cudaFree(s->map_dev);
+  if (s->internal) cudaStreamDestroy(s->internal);
+  if (s->ev_in) cudaEventDestroy(s->ev_in);
+  if (s->ev_out) cudaEventDestroy(s->ev_out);
+  delete s;
+  return AGIMP_OK;
+}
+
+static agimp_status upload_soa(agimp_sim* s, const float* src, float* dst, int comps, int memory, cudaStream_t st) {
+  const long long N = s->c.N;
+  if (N == 0) return AGIMP_OK;
+  const float* aos = src;
+  if (memory == AGIMP_MEM_HOST) {
+    CK(cudaMemcpyAsync(s->staging, src, N * comps * sizeof(float), cudaMemcpyHostToDevice, st));
+    aos = s->staging;
+  }
+  k_aos_to_soa<<<gs_blocks(N * comps), 256, 0, st>>>(aos, dst, N, comps);
+  CK(cudaGetLastError());
+  return AGIMP_OK;
+}
+
+static agimp_status download_soa(agimp_sim* s, const float* src, float* dst, int comps, int memory, cudaStream_t st) {
+  const long long N = s->c.N;
+  if (N == 0) return AGIMP_OK;
+  float* aos = (memory == AGIMP_MEM_HOST) ? s->staging : dst;
+  k_soa_to_aos<<<gs_blocks(N * comps), 256, 0, st>>>(src, aos, N, comps);
+  CK(cudaGetLastError());
+  if (memory == AGIMP_MEM_HOST) {
+    CK(cudaMemcpyAsync(dst, s->staging, N * comps * sizeof(float), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+  }
+  return AGIMP_OK;
+}
+
+static agimp_status copy_i32(agimp_sim* s, const int32_t* src, int32_t* dst, int to_dev, int memory, cudaStream_t st) {
+  const long long N = s->c.N;
+  if (N == 0) return AGIMP_OK;
+  cudaMemcpyKind k = memory == AGIMP_MEM_HOST ? (to_dev ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToHost)
+                                              : cudaMemcpyDeviceToDevice;
+  CK(cudaMemcpyAsync(dst, src, N * sizeof(int32_t), k, st));
+  if (!to_dev && memory == AGIMP_MEM_HOST) CK(cudaStreamSynchronize(st));
+  return AGIMP_OK;
+}
+
+agimp_status agimp_set_particles(agimp_sim* s, const float* x, const float* v, const float* F, const float* C,
+                                 const float* m, const int32_t* g, const float* Jp, int32_t memory, void* stream) {
+  if (!s || (memory != AGIMP_MEM_DEVICE && memory != AGIMP_MEM_HOST)) return fail(s, AGIMP_INVALID_ARG, "bad args");
+  CK(cudaSetDevice(s->device));
+  StreamUse su(s, stream);
+  const int D = s->c.dim;
+  agimp_status r;
+  if (x && (r = upload_soa(s, x, s->c.x, D, memory, su.use))) return r;
+  if (v && (r = upload_soa(s, v, s->c.v, D, memory, su.use))) return r;
+  if (F && (r = upload_soa(s, F, s->c.F, D * D, memory, su.use))) return r;
+  if (C && (r = upload_soa(s, C, s->c.C, D * D, memory, su.use))) return r;
+  if (m && (r = upload_soa(s, m, s->c.m, 1, memory, su.use))) return r;
+  if (Jp && (r = upload_soa(s, Jp, s->c.Jp, 1, memory, su.use))) return r;
+  if (g && (r = copy_i32(s, g, s->c.g, 1, memory, su.use))) return r;
+  if (memory == AGIMP_MEM_HOST) CK(cudaStreamSynchronize(su.use));  // host buffers may be reused on return
+  return AGIMP_OK;
+}
+
+agimp_status agimp_get_particles(agimp_sim* s, float* x, float* v, float* F, float* C, float* m, int32_t* g,
+                                 int32_t* fl, float* Jp, int32_t memory, void* stream) {
+  if (!s || (memory != AGIMP_MEM_DEVICE && memory != AGIMP_MEM_HOST)) return fail(s, AGIMP_INVALID_ARG, "bad args");
+  CK(cudaSetDevice(s->device));
+  StreamUse su(s, stream);
+  const int D = s->c.dim;
+  agimp_status r;
+  if (x && (r = download_soa(s, s->c.x, x, D, memory, su.use))) return r;
+  if (v && (r = download_soa(s, s->c.v, v, D, memory, su.use))) return r;
+  if (F && (r = download_soa(s, s->c.F, F, D * D, memory, su.use))) return r;
+  if (C && (r = download_soa(s, s->c.C, C, D * D, memory, su.use))) return r;
+  if (m && (r = download_soa(s, s->c.m, m, 1, memory, su.use))) return r;
+  if (Jp && (r = download_soa(s, s->c.Jp, Jp, 1, memory, su.use))) return r;
+  if (g && (r = copy_i32(s, s->c.g, g, 0, memory, su.use))) return r;
+  if (fl && (r = copy_i32(s, s->c.fl, fl, 0, memory, su.use))) return r;
+  return AGIMP_OK;
+}
+
+agimp_status agimp_set_level_map(agimp_sim* s, const int8_t* table, int32_t halo, int32_t memory, void* stream) {
+  if (!s || !table) return fail(s, AGIMP_INVALID_ARG, "null table");
+  const int need = std::max(2, 1 << (s->c.L - 1));
+  if (halo < need) return fail(s, AGIMP_INVALID_ARG, "level map halo must be >= max(2, 2^(level-1))");
+  CK(cudaSetDevice(s->device));
+  const int n = s->c.sz + 2 * halo;
+  size_t bytes = 1;
+  for (int d = 0; d < s->c.dim; ++d) bytes *= (size_t)n;
+  std::vector<int8_t> host(bytes);
+  if (memory == AGIMP_MEM_HOST)
+    std::memcpy(host.data(), table, bytes);
+  else
+    CK(cudaMemcpy(host.data(), table, bytes, cudaMemcpyDeviceToHost));
+  for (size_t i = 0; i < bytes; ++i) {
+    const int e = host[i];
+    if (e < 0 || (e & 15) >= s->c.L || (e & ~(15 | 64)))
+      return fail(s, AGIMP_INVALID_ARG, "level map entry out of range at " + std::to_string(i));
+  }
+  CK(cudaStreamSynchronize(0));
+  if (s->map_dev) cudaFree(s->map_dev);
+  s->map_dev = nullptr;
+  CK(cudaMalloc(&s->map_dev, bytes));
+  CK(cudaMemcpy(s->map_dev, host.data(), bytes, cudaMemcpyHostToDevice));
+  s->c.map = s->map_dev;
+  s->c.map_h = halo;
+  s->c.map_n = n;
+  s->c.is_static = 1;
+  if (s->gexec) {
+    cudaGraphExecDestroy(s->gexec);
+    s->gexec = nullptr;
+  }
+  (void)stream;
+  return AGIMP_OK;
+}
+
+agimp_status agimp_clear_level_map(agimp_sim* s) {
+  if (!s) return AGIMP_INVALID_ARG;
+  s->c.is_static = 0;
+  if (s->gexec) {
+    cudaGraphExecDestroy(s->gexec);
+    s->gexec = nullptr;
+  }
+  return AGIMP_OK;
+}
+
+agimp_status agimp_set_graphs(agimp_sim* s, int32_t enable) {
+  if (!s) return AGIMP_INVALID_ARG;
+  s->graphs = enable != 0;
+  return AGIMP_OK;
+}
+
+agimp_status agimp_substep(agimp_sim* s, float dt, int32_t n_steps, void* stream) {
+  if (!s || n_steps < 0 || !std::isfinite(dt)) return fail(s, AGIMP_INVALID_ARG, "bad substep args");
+  CK(cudaSetDevice(s->device));
+  StreamUse su(s, stream);
+  if (!s->graphs) {
+    s->c.dt = dt;
+    for (int i = 0; i < n_steps; ++i) launch_substep(s->c, su.use);
+    CK(cudaGetLastError());
+    s->substeps += n_steps;
+    return AGIMP_OK;
+  }
+  if (!s->gexec || s->g_dt != dt || s->g_stream != su.use) {
+    if (s->gexec) {
+      cudaGraphExecDestroy(s->gexec);
+      s->gexec = nullptr;
+    }
+    s->c.dt = dt;
+    cudaGraph_t graph = nullptr;
+    CK(cudaStreamBeginCapture(su.use, cudaStreamCaptureModeThreadLocal));
+    launch_substep(s->c, su.use);
+    cudaError_t e = cudaStreamEndCapture(su.use, &graph);
+    if (e != cudaSuccess) return cuda_fail(s, e, "capture substep");
+    e = cudaGraphInstantiate(&s->gexec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) return cuda_fail(s, e, "instantiate substep graph");
+    s->g_dt = dt;
+    s->g_stream = su.use;
+  }
+  for (int i = 0; i < n_steps; ++i) CK(cudaGraphLaunch(s->gexec, su.use));
+  s->substeps += n_steps;
+  return AGIMP_OK;
+}
+
+agimp_status agimp_refine_levels(agimp_sim* s, int32_t band, void* stream) {
+  if (!s || band < 1 || band > 32) return fail(s, AGIMP_INVALID_ARG, "band must be in [1, 32]");
+  CK(cudaSetDevice(s->device));
+  StreamUse su(s, stream);
+  launch_refine(s->c, band, su.use);
+  CK(cudaGetLastError());
+  return AGIMP_OK;
+}
+
+agimp_status agimp_get_grid(agimp_sim* s, int32_t level, int32_t lo, int32_t n, float* m, float* v, int32_t* cell,
+                            int32_t memory, void* stream) {
+  if (!s || level < 0 || level >= s->c.L || n <= 0) return fail(s, AGIMP_INVALID_ARG, "bad grid readback args");
+  CK(cudaSetDevice(s->device));
+  StreamUse su(s, stream);
+  const int D = s->c.dim;
+  long long total = 1;
+  for (int d = 0; d < D; ++d) total *= n;
+  if (memory == AGIMP_MEM_DEVICE) {
+    if (D == 2)
+      k_get_grid<2><<<gs_blocks(total), 256, 0, su.use>>>(s->c, level, lo, n, 0, total, m, v, cell);
+    else
+      k_get_grid<3><<<gs_blocks(total), 256, 0, su.use>>>(s->c, level, lo, n, 0, total, m, v, cell);
+    CK(cudaGetLastError());
+    return AGIMP_OK;
+  }
+  // host: slabs through the staging buffer (m | v | cell)
+  const long long slab = (long long)(s->staging_floats / (2 + D));
+  for (long long off = 0; off < total; off += slab) {
+    const long long cnt = std::min(slab, total - off);
+    float* sm = s->staging;
+    float* sv = s->staging + cnt;
+    int32_t* sc = (int32_t*)(s->staging + cnt * (1 + D));
+    if (D == 2)
+      k_get_grid<2><<<gs_blocks(cnt), 256, 0, su.use>>>(s->c, level, lo, n, off, cnt, m ? sm : nullptr,
+                                                        v ? sv : nullptr, cell ? sc : nullptr);
+    else
+      k_get_grid<3><<<gs_blocks(cnt), 256, 0, su.use>>>(s->c, level, lo, n, off, cnt, m ? sm : nullptr,
+                                                        v ? sv : nullptr, cell ? sc : nullptr);
+    CK(cudaGetLastError());
+    if (m) CK(cudaMemcpyAsync(m + off, sm, cnt * sizeof(float), cudaMemcpyDeviceToHost, su.use));
+    if (v) CK(cudaMemcpyAsync(v + off * D, sv, cnt * D * sizeof(float), cudaMemcpyDeviceToHost, su.use));
+    if (cell) CK(cudaMemcpyAsync(cell + off, sc, cnt * sizeof(int32_t), cudaMemcpyDeviceToHost, su.use));
+    CK(cudaStreamSynchronize(su.use));
+  }
+  return AGIMP_OK;
+}
+
+agimp_status agimp_get_node_mask(agimp_sim* s, int32_t* out, int32_t memory, void* stream) {
+  if (!s || !out) return fail(s, AGIMP_INVALID_ARG, "bad node mask readback args");
+  CK(cudaSetDevice(s->device));
+  StreamUse su(s, stream);
+  const int D = s->c.dim;
+  long long total = 1;
+  for (int d = 0; d < D; ++d) total *= (s->c.sz + 1);
+  const long long slab = memory == AGIMP_MEM_HOST ? (long long)s->staging_floats : total;
+  for (long long off = 0; off < total; off += slab) {
+    const long long cnt = std::min(slab, total - off);
+    int32_t* dst = memory == AGIMP_MEM_HOST ? (int32_t*)s->staging : out + off;
+    if (D == 2)
+      k_get_nmask<2><<<gs_blocks(cnt), 256, 0, su.use>>>(s->c, off, cnt, dst);
+    else
+      k_get_nmask<3><<<gs_blocks(cnt), 256, 0, su.use>>>(s->c, off, cnt, dst);
+    CK(cudaGetLastError());
+    if (memory == AGIMP_MEM_HOST) {
+      CK(cudaMemcpyAsync(out + off, dst, cnt * sizeof(int32_t), cudaMemcpyDeviceToHost, su.use));
+      CK(cudaStreamSynchronize(su.use));
+    }
+  }
+  return AGIMP_OK;
+}
+
+agimp_status agimp_errors(agimp_sim* s, uint32_t* bits, int32_t clear) {
+  if (!s || !bits) return AGIMP_INVALID_ARG;
+  CK(cudaSetDevice(s->device));
+  CK(cudaDeviceSynchronize());
+  int32_t v = 0;
+  CK(cudaMemcpy(&v, s->c.ctr + CTR_ERR, sizeof(int32_t), cudaMemcpyDeviceToHost));
+  *bits = (uint32_t)v;
+  if (clear) CK(cudaMemset(s->c.ctr + CTR_ERR, 0, sizeof(int32_t)));
+  return AGIMP_OK;
+}
+
+agimp_status agimp_get_stats(agimp_sim* s, agimp_stats* out) {
+  if (!s || !out) return AGIMP_INVALID_ARG;
+  CK(cudaSetDevice(s->device));
+  CK(cudaDeviceSynchronize());
+  int32_t h[CTR_COUNT];
+  CK(cudaMemcpy(h, s->c.ctr, sizeof(h), cudaMemcpyDeviceToHost));
+  std::memset(out, 0, sizeof(*out));
+  for (int l = 0; l < MAXL; ++l) out->active_blocks[l] = l < s->c.L ? h[CTR_LEVEL + l] : 0;
+  out->n_binned = h[CTR_BINCUR];
+  out->n_chunks = h[CTR_CHUNKS];
+  out->substeps = s->substeps;
+  return AGIMP_OK;
+}
+
+int32_t agimp_kernels_per_substep(const agimp_sim* s) { return s ? kernels_per_substep(s->c) : 0; }
+
+agimp_status agimp_profile_substep(agimp_sim* s, float dt, float* ms, int32_t n, void* stream) {
+  if (!s || !ms || n < PHASES || !std::isfinite(dt)) return fail(s, AGIMP_INVALID_ARG, "bad profile args");
+  CK(cudaSetDevice(s->device));
+  StreamUse su(s, stream);
+  cudaEvent_t ev[PHASES + 1];
+  for (int i = 0; i <= PHASES; ++i) CK(cudaEventCreate(&ev[i]));
+  s->c.dt = dt;
+  launch_substep(s->c, su.use, ev);
+  cudaError_t e = cudaEventSynchronize(ev[PHASES]);
+  for (int i = 0; i < PHASES && e == cudaSuccess; ++i) e = cudaEventElapsedTime(&ms[i], ev[i], ev[i + 1]);
+  for (int i = 0; i <= PHASES; ++i) cudaEventDestroy(ev[i]);
+  if (e != cudaSuccess) return cuda_fail(s, e, "profile substep");
+  s->substeps += 1;
+  return AGIMP_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,402 @@
+// Shared definitions of the B200 adaptive GIMP substep.
+//
+// Data layout in HBM (one simulator):
+//  * Every level l stores cells and nodes over indices [-4, size_l + 8) per
+//    axis, blocked in 4^d tiles: element (i,j[,k]) lives at
+//      block(i>>2 +1, j>>2 +1 [, k>>2 +1]) * 4^d + local(i&3, j&3 [, k&3]),
+//    blocks in row-major order (first axis slowest).  A 4^d tile is the
+//    reference's leaf block (adaptive_gimp.py:28-42) and is contiguous
+//    (64 B of masks / 1 KB of node records in 3D).
+//  * node record: float4 {p_x | v_x, p_y | v_y, p_z | v_z, m}: momentum until
+//    grid_op, velocity after, exactly like ad_grid_v / ad_grid_m.
+//  * cell mask: u32 per cell (utils.py:5-9 flags, plus CULLING kept internally
+//    until the next substep; readback masks it out).
+//  * node mask: u32 on the finest lattice, same blocked layout as the finest
+//    level (adaptive_gimp.py:23-26: one mask shared by all levels through
+//    _map, adaptive_gimp.py:126-128).
+//  * per level: bmap (block -> index in the active list, -1 if inactive) and
+//    the active block list itself.  Active blocks are the 4^d blocks within
+//    one block of any particle's position at that level; every nonzero cell,
+//    node value or node flag of a substep lies inside them.
+//  * particles: SoA, one f32 array per component ([c * N + p]).
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace agimp {
+
+constexpr int MAXL = 8;
+constexpr int CHUNK = 256;  // particles per P2G/G2P work item (= CTA size)
+constexpr int HALO = 4;
+
+enum : uint32_t { ACT = 1u, GHO = 2u, TJ = 4u, CUL = 8u };
+enum : uint32_t { ERR_OOB = 1u, ERR_ESCAPED = 2u, ERR_MAP_OOB = 4u, ERR_NOBIN = 8u };
+
+// device counters
+enum {
+  CTR_LEVEL = 0,   // [0, MAXL): active blocks per level
+  CTR_TOUCH = 8,   // touched finest blocks
+  CTR_BINCUR = 9,  // particles placed by the bin allocator
+  CTR_CHUNKS = 10, // P2G/G2P work items
+  CTR_ERR = 11,    // error bits
+  // [16, 22): particle bounding box used by the refinement rule
+  CTR_COUNT = 24
+};
+
+struct LevelDev {
+  int size;          // cells per axis at this level
+  int nb;            // stored blocks per axis (size/4 + 3)
+  long long nblocks; // nb^dim
+  uint32_t* cell;
+  float4* node;
+  int32_t* bmap;
+  int32_t* blist;
+};
+
+struct Ctx {
+  int dim, L, coarsest, sz;
+  int N;
+  int sms;  // multiprocessors of the device (grid-stride launch width)
+  int is_static, gap, bmode, plast, ncol, map_h, map_n;
+  float radius, mu, la, theta_c, theta_s, xi, dt;
+  float grav[3];
+  double col[4][6];  // collider boxes, compared in double like the oracle
+  LevelDev lev[MAXL];
+  uint32_t* nmask;
+  int32_t* ctr;
+  uint32_t* touch_flag;
+  int32_t* touch_list;
+  int32_t* bin_count;
+  int32_t* bin_start;
+  int4* chunks;  // {level, block (stored linear id), start, count}
+  int32_t* bin_of;
+  int32_t* rank_of;
+  int32_t* perm;
+  float* x;
+  float* v;
+  float* F;
+  float* C;
+  float* m;
+  float* Jp;
+  int32_t* g;
+  int32_t* fl;
+  const int8_t* map;
+  uint8_t* occ;  // refinement scratch over the finest cells
+};
+
+// ---------------------------------------------------------------------------
+// index helpers
+template <int D>
+__device__ __forceinline__ bool in_store(const LevelDev& V, const int* I) {
+#pragma unroll
+  for (int d = 0; d < D; ++d)
+    if ((unsigned)(I[d] + HALO) >= (unsigned)(4 * V.nb)) return false;
+  return true;
+}
+
+template <int D>
+__device__ __forceinline__ long long elem_of(const LevelDev& V, const int* I) {
+  long long b = 0;
+  int loc = 0;
+#pragma unroll
+  for (int d = 0; d < D; ++d) {
+    int a = I[d] + HALO;
+    b = b * V.nb + (a >> 2);
+    loc = (loc << 2) | (a & 3);
+  }
+  return (b << (2 * D)) | loc;
+}
+
+template <int D>
+__device__ __forceinline__ long long block_of(const LevelDev& V, const int* I) {
+  long long b = 0;
+#pragma unroll
+  for (int d = 0; d < D; ++d) b = b * V.nb + ((I[d] + HALO) >> 2);
+  return b;
+}
+
+// element coordinates of local index `loc` in stored block `blk`
+template <int D>
+__device__ __forceinline__ void elem_coords(const LevelDev& V, long long blk, int loc, int* I) {
+#pragma unroll
+  for (int d = D - 1; d >= 0; --d) {
+    int bd = (int)(blk % V.nb);
+    blk /= V.nb;
+    I[d] = (bd << 2) + ((loc >> (2 * (D - 1 - d))) & 3) - HALO;
+  }
+}
+
+// node_mask[_map(l, I)] (adaptive_gimp.py:126-131); positions outside the
+// finest lattice [0, sz] read 0.
+template <int D>
+__device__ __forceinline__ uint32_t nm_get(const Ctx& c, int l, const int* I) {
+  const int s = c.L - 1 - l;
+  int P[D];
+#pragma unroll
+  for (int d = 0; d < D; ++d) {
+    P[d] = I[d] * (1 << s);
+    if (P[d] < 0 || P[d] > c.sz) return 0u;
+  }
+  return c.nmask[elem_of<D>(c.lev[c.L - 1], P)];
+}
+
+template <int D>
+__device__ __forceinline__ void nm_or(const Ctx& c, int l, const int* I, uint32_t bits) {
+  const int s = c.L - 1 - l;
+  int P[D];
+#pragma unroll
+  for (int d = 0; d < D; ++d) {
+    P[d] = I[d] * (1 << s);
+    if (P[d] < 0 || P[d] > c.sz) return;  // unobservable: never read by a predicate
+  }
+  uint32_t* w = &c.nmask[elem_of<D>(c.lev[c.L - 1], P)];
+  if ((*w & bits) != bits) atomicOr(w, bits);
+}
+
+__device__ __forceinline__ bool is_valid(uint32_t nm) { return nm > 0u; }
+__device__ __forceinline__ bool is_activated(uint32_t nm) { return (nm & (ACT | TJ)) == ACT; }
+__device__ __forceinline__ bool is_tj(uint32_t nm) { return (nm & TJ) == TJ; }
+__device__ __forceinline__ bool is_ghost(uint32_t nm) { return (nm & (ACT | GHO | TJ)) == GHO; }
+
+__device__ __forceinline__ void set_err(const Ctx& c, uint32_t bits) {
+  if ((((volatile uint32_t*)c.ctr)[CTR_ERR] & bits) != bits) atomicOr((unsigned*)&c.ctr[CTR_ERR], bits);
+}
+
+// Decode flat element e over the active lists of levels [l0, l1) -> level,
+// block, local index.  Returns false past the end.
+template <int D>
+__device__ __forceinline__ bool decode_elem(const Ctx& c, int l0, int l1, long long e, int& l, long long& blk,
+                                            int& loc) {
+  const int per = 1 << (2 * D);
+  long long bi = e >> (2 * D);
+  loc = (int)(e & (per - 1));
+  for (int q = l0; q < l1; ++q) {
+    int n = c.ctr[CTR_LEVEL + q];
+    if (bi < n) {
+      l = q;
+      blk = c.lev[q].blist[bi];
+      return true;
+    }
+    bi -= n;
+  }
+  return false;
+}
+
+__device__ __forceinline__ long long total_elems(const Ctx& c, int l0, int l1, int D) {
+  long long t = 0;
+  for (int q = l0; q < l1; ++q) t += c.ctr[CTR_LEVEL + q];
+  return t << (2 * D);
+}
+
+// ---------------------------------------------------------------------------
+// small dense linear algebra (row-major)
+template <int D>
+__device__ __forceinline__ float det(const float* F) {
+  if (D == 2) return F[0] * F[3] - F[1] * F[2];
+  return F[0] * (F[4] * F[8] - F[5] * F[7]) - F[1] * (F[3] * F[8] - F[5] * F[6]) +
+         F[2] * (F[3] * F[7] - F[4] * F[6]);
+}
+
+// 2x2: polar rotation in closed form.  R maximises tr(R^T F) over rotations,
+// which is U V^T of the rotation-variant SVD used by the reference's
+// get_stress (utils.py:11-16).
+__device__ __forceinline__ void polar2(const float* F, float& c, float& s) {
+  float a = F[0] + F[3], b = F[2] - F[1];
+  float n2 = a * a + b * b;
+  if (n2 > 0.f) {
+    float inv = 1.0f / sqrtf(n2);
+    c = a * inv;
+    s = b * inv;
+  } else {
+    c = 1.f;
+    s = 0.f;
+  }
+}
+
+// 2x2 SVD with det U = det V = +1: R from polar2, then the symmetric factor
+// S = R^T F is diagonalised by one exact Jacobi rotation.
+__device__ __forceinline__ void svd2(const float* F, float* U, float* sig, float* V) {
+  float c, s;
+  polar2(F, c, s);
+  // S = R^T F
+  float s00 = c * F[0] + s * F[2], s01 = c * F[1] + s * F[3];
+  float s11 = -s * F[1] + c * F[3];
+  float cv = 1.f, sv = 0.f;
+  if (s01 != 0.f) {
+    float tau = (s11 - s00) / (2.f * s01);
+    float t = copysignf(1.f, tau) / (fabsf(tau) + sqrtf(1.f + tau * tau));
+    cv = 1.f / sqrtf(1.f + t * t);
+    sv = t * cv;
+  }
+  // eigenvalues: Q^T S Q with Q = [[cv, sv], [-sv, cv]]
+  float e0 = cv * cv * s00 - 2.f * cv * sv * s01 + sv * sv * s11;
+  float e1 = sv * sv * s00 + 2.f * cv * sv * s01 + cv * cv * s11;
+  float V00 = cv, V01 = sv, V10 = -sv, V11 = cv;
+  if (fabsf(e1) > fabsf(e0)) {  // sort descending, keep det V = +1
+    float t = e0; e0 = e1; e1 = t;
+    float a0 = V00, a1 = V10;
+    V00 = V01; V10 = V11;
+    V01 = -a0; V11 = -a1;
+  }
+  sig[0] = e0; sig[1] = e1;
+  V[0] = V00; V[1] = V01; V[2] = V10; V[3] = V11;
+  // U = R V
+  U[0] = c * V00 - s * V10; U[1] = c * V01 - s * V11;
+  U[2] = s * V00 + c * V10; U[3] = s * V01 + c * V11;
+}
+
+// 3x3 SVD, A = U diag(sig) V^T with det U = det V = +1 (rotation-variant).
+// Method: cyclic Jacobi eigenanalysis of A^T A with exact rotations (Golub &
+// Van Loan, Matrix Computations, 4th ed., Alg. 8.5.3), columns of B = A V
+// sorted by norm, then a Givens QR of B gives U and sig (the approach of
+// McAdams et al. 2011, "Computing the SVD of 3x3 matrices with minimal
+// branching and elementary floating point operations", with exact instead of
+// approximate Givens angles).
+__device__ __forceinline__ void jacobi_rot(float* S, float* V, int p, int q) {
+  // symmetric S (row-major 3x3), zero S[p][q]
+  float apq = S[p * 3 + q];
+  if (apq == 0.f) return;
+  float app = S[p * 3 + p], aqq = S[q * 3 + q];
+  float tau = (aqq - app) / (2.f * apq);
+  float t = copysignf(1.f, tau) / (fabsf(tau) + sqrtf(1.f + tau * tau));
+  float c = 1.f / sqrtf(1.f + t * t), s = t * c;
+  // S <- J^T S J, J = rotation in (p,q) with J[p][p]=c, J[p][q]=s, J[q][p]=-s, J[q][q]=c
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {  // columns
+    float skp = S[k * 3 + p], skq = S[k * 3 + q];
+    S[k * 3 + p] = c * skp - s * skq;
+    S[k * 3 + q] = s * skp + c * skq;
+  }
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {  // rows
+    float spk = S[p * 3 + k], sqk = S[q * 3 + k];
+    S[p * 3 + k] = c * spk - s * sqk;
+    S[q * 3 + k] = s * spk + c * sqk;
+  }
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    float vkp = V[k * 3 + p], vkq = V[k * 3 + q];
+    V[k * 3 + p] = c * vkp - s * vkq;
+    V[k * 3 + q] = s * vkp + c * vkq;
+  }
+}
+
+__device__ __forceinline__ void givens_qr(float* B, float* U, int i, int j) {
+  // zero B[i][j] (i > j) using rows j and i; U <- U G^T
+  float a = B[j * 3 + j], b = B[i * 3 + j];
+  float r2 = a * a + b * b;
+  float c = 1.f, s = 0.f;
+  if (r2 > 0.f) {
+    float inv = 1.0f / sqrtf(r2);
+    c = a * inv;
+    s = b * inv;
+  }
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    float bj = B[j * 3 + k], bi = B[i * 3 + k];
+    B[j * 3 + k] = c * bj + s * bi;
+    B[i * 3 + k] = -s * bj + c * bi;
+  }
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    float uj = U[k * 3 + j], ui = U[k * 3 + i];
+    U[k * 3 + j] = c * uj + s * ui;
+    U[k * 3 + i] = -s * uj + c * ui;
+  }
+}
+
+__device__ __forceinline__ void svd3(const float* A, float* U, float* sig, float* V) {
+  float S[9];
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+      float a = 0.f;
+#pragma unroll
+      for (int k = 0; k < 3; ++k) a += A[k * 3 + i] * A[k * 3 + j];
+      S[i * 3 + j] = a;
+    }
+#pragma unroll
+  for (int i = 0; i < 9; ++i) V[i] = (i % 4 == 0) ? 1.f : 0.f;
+#pragma unroll 1
+  for (int sweep = 0; sweep < 5; ++sweep) {
+    float off = fabsf(S[1]) + fabsf(S[2]) + fabsf(S[5]);
+    float dg = fabsf(S[0]) + fabsf(S[4]) + fabsf(S[8]);
+    if (off <= 1e-9f * dg) break;
+    jacobi_rot(S, V, 0, 1);
+    jacobi_rot(S, V, 0, 2);
+    jacobi_rot(S, V, 1, 2);
+  }
+  // B = A V
+  float B[9];
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+      float a = 0.f;
+#pragma unroll
+      for (int k = 0; k < 3; ++k) a += A[i * 3 + k] * V[k * 3 + j];
+      B[i * 3 + j] = a;
+    }
+  // sort columns by norm, descending; each swap negates one column to keep det V = +1
+  auto cn = [&](int j) { return B[j] * B[j] + B[3 + j] * B[3 + j] + B[6 + j] * B[6 + j]; };
+  auto swapc = [&](int a, int b) {
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      float t = B[k * 3 + a]; B[k * 3 + a] = B[k * 3 + b]; B[k * 3 + b] = -t;
+      t = V[k * 3 + a]; V[k * 3 + a] = V[k * 3 + b]; V[k * 3 + b] = -t;
+    }
+  };
+  float n0 = cn(0), n1 = cn(1), n2 = cn(2);
+  if (n0 < n1) { swapc(0, 1); float t = n0; n0 = n1; n1 = t; }
+  if (n0 < n2) { swapc(0, 2); float t = n0; n0 = n2; n2 = t; }
+  if (n1 < n2) { swapc(1, 2); }
+  // QR by Givens: B = U R
+#pragma unroll
+  for (int i = 0; i < 9; ++i) U[i] = (i % 4 == 0) ? 1.f : 0.f;
+  givens_qr(B, U, 1, 0);
+  givens_qr(B, U, 2, 0);
+  givens_qr(B, U, 2, 1);
+  sig[0] = B[0];
+  sig[1] = B[4];
+  sig[2] = B[8];
+  // det U = +1 by construction; make sig[0], sig[1] non-negative by flipping
+  // column pairs of U and V together (keeps both determinants).
+  if (sig[0] < 0.f) {
+    sig[0] = -sig[0]; sig[2] = -sig[2];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) { U[k * 3 + 0] = -U[k * 3 + 0]; U[k * 3 + 2] = -U[k * 3 + 2]; }
+  }
+  if (sig[1] < 0.f) {
+    sig[1] = -sig[1]; sig[2] = -sig[2];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) { U[k * 3 + 1] = -U[k * 3 + 1]; U[k * 3 + 2] = -U[k * 3 + 2]; }
+  }
+}
+
+// R = U V^T of the rotation-variant SVD
+template <int D>
+__device__ __forceinline__ void polar_rot(const float* F, float* R) {
+  if (D == 2) {
+    float c, s;
+    polar2(F, c, s);
+    R[0] = c; R[1] = -s; R[2] = s; R[3] = c;
+  } else {
+    float U[9], sg[3], V[9];
+    svd3(F, U, sg, V);
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+      for (int j = 0; j < 3; ++j) R[i * 3 + j] = U[i * 3] * V[j * 3] + U[i * 3 + 1] * V[j * 3 + 1] + U[i * 3 + 2] * V[j * 3 + 2];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// host-side launchers (defined in topology.cu / transfer.cu)
+// ev (optional): PHASES+1 events recorded at the phase boundaries
+constexpr int PHASES = 8;  // blocks, topology, binning, p2g, restrict, gridop, prolong, g2p
+void launch_substep(const Ctx& c, cudaStream_t s, cudaEvent_t* ev = nullptr);
+void launch_refine(const Ctx& c, int band, cudaStream_t s);
+int kernels_per_substep(const Ctx& c);
+
+}  // namespace agimp

@@ -1,0 +1,565 @@
+// Topology and binning kernels of the adaptive GIMP substep.
+//
+// Reference steps (adaptive_gimp.py, g1n0st/adaptive-gimp):
+//   324-326 deactivate_all            -> k_clear (only the blocks the previous
+//                                         substep touched)
+//   72-96   activate_cell_*           -> k_touch_activate
+//   98-124  _mark_hier_ / _split_hier_-> k_mark_hier + k_resolve
+//   142-153 _activate_mask            -> k_resolve (same pass)
+//   155-187 ghost / T-junction        -> k_ghost_tj (all levels in one pass)
+//   189-216 level_mapping             -> k_bin + k_offsets + k_scatter
+//
+// The reference runs its sparse sweeps level by level.  Here each pass covers
+// every level at once: the reads each pass depends on are not written in the
+// same pass (CULLING bits in k_resolve, == ACTIVATED tests in k_ghost_tj), so
+// the result does not depend on the order.  The one order-dependent bit in the
+// reference (GHOST on a node that also gets T_JUNCTION, adaptive_gimp.py:174
+// against 182-183) never changes a node's class.
+#include "common.cuh"
+
+namespace agimp {
+
+#define GS_LOOP(i, n) \
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < (n); i += (long long)gridDim.x * blockDim.x)
+
+template <int D>
+__device__ __forceinline__ void cell_or(const Ctx& c, int l, const int* I, uint32_t bits) {
+  const LevelDev& V = c.lev[l];
+  if (!in_store<D>(V, I)) {
+    set_err(c, ERR_OOB);
+    return;
+  }
+  uint32_t* w = &V.cell[elem_of<D>(V, I)];
+  if ((*w & bits) != bits) atomicOr(w, bits);
+}
+
+template <int D>
+__device__ __forceinline__ uint32_t cell_get(const Ctx& c, int l, const int* I) {
+  const LevelDev& V = c.lev[l];
+  if (!in_store<D>(V, I)) return 0u;
+  return V.cell[elem_of<D>(V, I)];
+}
+
+// ---------------------------------------------------------------------------
+// Clear everything the previous substep wrote (its active blocks), reset the
+// per-substep counters.
+template <int D>
+__global__ void k_clear(Ctx c) {
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    c.ctr[CTR_TOUCH] = 0;
+    c.ctr[CTR_BINCUR] = 0;
+    c.ctr[CTR_CHUNKS] = 0;
+  }
+  const long long tot = total_elems(c, 0, c.L, D);
+  GS_LOOP(e, tot) {
+    int l, loc;
+    long long blk;
+    decode_elem<D>(c, 0, c.L, e, l, blk, loc);
+    const LevelDev& V = c.lev[l];
+    const long long idx = (blk << (2 * D)) | loc;
+    V.cell[idx] = 0u;
+    V.node[idx] = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (loc == 0) V.bmap[blk] = -1;
+    int I[D];
+    elem_coords<D>(V, blk, loc, I);
+    const int s = c.L - 1 - l;
+    int P[D];
+    bool ok = true;
+#pragma unroll
+    for (int d = 0; d < D; ++d) {
+      P[d] = I[d] * (1 << s);
+      ok = ok && P[d] >= 0 && P[d] <= c.sz;
+    }
+    if (ok) c.nmask[elem_of<D>(c.lev[c.L - 1], P)] = 0u;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Per particle: record the finest block holding it (for the active-block
+// lists) and activate cells, dynamically from g_p (adaptive_gimp.py:87-96) or
+// through the level map (adaptive_gimp.py:72-85).
+template <int D>
+__device__ __forceinline__ int grid_init(const Ctx& c, const int* I) {
+  // grid_initializer(sim, I) with the tabulated map: activate_cell(l, I)
+  // (adaptive_gimp.py:68-70) unless bit 6 is set; returns l.
+  long long o = 0;
+#pragma unroll
+  for (int d = 0; d < D; ++d) {
+    int a = I[d] + c.map_h;
+    if (a < 0 || a >= c.map_n) {
+      set_err(c, ERR_MAP_OOB);
+      return c.L - 1;
+    }
+    o = o * c.map_n + a;
+  }
+  const int e = c.map[o];
+  const int l = e & 15;
+  if (!(e & 64)) {
+    int A[D];
+    const int s = c.L - 1 - l;
+#pragma unroll
+    for (int d = 0; d < D; ++d) A[d] = I[d] >> s;
+    cell_or<D>(c, l, A, ACT);
+  }
+  return l;
+}
+
+template <int D>
+__global__ void k_touch_activate(Ctx c) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  const bool valid = p < c.N;
+  float xp[D];
+  bool esc = !valid;
+#pragma unroll
+  for (int d = 0; d < D; ++d) {
+    xp[d] = valid ? c.x[(long long)d * c.N + p] : 0.f;
+    if (!(xp[d] >= 0.f && xp[d] < 1.f)) esc = true;
+  }
+  if (valid && esc) set_err(c, ERR_ESCAPED);
+  const LevelDev& Vf = c.lev[c.L - 1];
+  int key = -1;
+  if (!esc) {
+    long long b = 0;
+#pragma unroll
+    for (int d = 0; d < D; ++d) b = b * Vf.nb + ((((int)(xp[d] * (float)c.sz)) >> 2) + 1);
+    key = (int)b;
+  }
+  const unsigned grp = __match_any_sync(0xffffffffu, key);
+  if (key >= 0 && (int)(threadIdx.x & 31) == __ffs(grp) - 1) {
+    if (c.touch_flag[key] == 0u && atomicExch(&c.touch_flag[key], 1u) == 0u) {
+      const int i = atomicAdd(&c.ctr[CTR_TOUCH], 1);
+      c.touch_list[i] = key;
+    }
+  }
+  if (esc) return;
+  if (!c.is_static) {
+    const int gl = c.g[p];
+    if (gl < 0 || gl >= c.L) return;
+    const float inv = (float)(c.coarsest << gl);
+    int base[D];
+#pragma unroll
+    for (int d = 0; d < D; ++d) base[d] = (int)(xp[d] * inv + 0.5f) - 1;
+#pragma unroll
+    for (int a = 0; a < (1 << D); ++a) {
+      int I[D];
+#pragma unroll
+      for (int d = 0; d < D; ++d) I[d] = base[d] + ((a >> (D - 1 - d)) & 1);
+      cell_or<D>(c, gl, I, ACT);
+    }
+  } else {
+    int fb[D];
+#pragma unroll
+    for (int d = 0; d < D; ++d) fb[d] = (int)(xp[d] * (float)c.sz + 0.5f) - 1;
+#pragma unroll 1
+    for (int a = 0; a < (1 << (2 * D)); ++a) {
+      int I[D];
+#pragma unroll
+      for (int d = 0; d < D; ++d) I[d] = fb[d] + ((a >> (2 * (D - 1 - d))) & 3) - 1;
+      grid_init<D>(c, I);
+    }
+    const int level = grid_init<D>(c, fb);
+    const float inv = (float)(c.coarsest << level);
+    int base[D];
+#pragma unroll
+    for (int d = 0; d < D; ++d) base[d] = (int)(xp[d] * inv + 0.5f) - 1;
+#pragma unroll
+    for (int a = 0; a < (1 << D); ++a) {
+      int I[D];
+#pragma unroll
+      for (int d = 0; d < D; ++d) I[d] = (base[d] + ((a >> (D - 1 - d)) & 1)) * (1 << (c.L - 1 - level));
+      grid_init<D>(c, I);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Active-block lists: every level gets the blocks within one block of each
+// touched finest block (shifted to that level).
+template <int D>
+__global__ void k_dilate(Ctx c) {
+  constexpr int NB3 = (D == 2) ? 9 : 27;
+  const long long tot = (long long)c.ctr[CTR_TOUCH] * c.L * NB3;
+  const LevelDev& Vf = c.lev[c.L - 1];
+  GS_LOOP(e, tot) {
+    const int nbi = (int)(e % NB3);
+    const long long r = e / NB3;
+    const int l = (int)(r % c.L);
+    const int t = (int)(r / c.L);
+    const int key = c.touch_list[t];
+    if (l == c.L - 1 && nbi == NB3 / 2) c.touch_flag[key] = 0u;
+    int fb[D];
+    long long k = key;
+#pragma unroll
+    for (int d = D - 1; d >= 0; --d) {
+      fb[d] = (int)(k % Vf.nb) - 1;
+      k /= Vf.nb;
+    }
+    const LevelDev& V = c.lev[l];
+    const int s = c.L - 1 - l;
+    int dl[D];
+    int tt = nbi;
+#pragma unroll
+    for (int d = D - 1; d >= 0; --d) {
+      dl[d] = tt % 3 - 1;
+      tt /= 3;
+    }
+    long long b = 0;
+    bool ok = true;
+#pragma unroll
+    for (int d = 0; d < D; ++d) {
+      const int cb = (fb[d] >> s) + dl[d] + 1;
+      ok = ok && cb >= 0 && cb < V.nb;
+      b = b * V.nb + cb;
+    }
+    if (!ok) {
+      set_err(c, ERR_OOB);
+      continue;
+    }
+    int* bm = &V.bmap[b];
+    if (*bm == -1 && atomicCAS(bm, -1, -2) == -1) {
+      const int i = atomicAdd(&c.ctr[CTR_LEVEL + l], 1);
+      V.blist[i] = (int)b;
+      *bm = i;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// _mark_hier_ for every level l >= 1 (adaptive_gimp.py:98-109): an ACTIVATED
+// cell whose finest ACTIVATED ancestor sits at level l0 marks CULLING on its
+// ancestors at levels l0..l-1.  Only ACTIVATED bits are read and only CULLING
+// bits written, so all levels run in one pass.
+template <int D>
+__global__ void k_mark_hier(Ctx c) {
+  const long long tot = total_elems(c, 1, c.L, D);
+  GS_LOOP(e, tot) {
+    int l, loc;
+    long long blk;
+    decode_elem<D>(c, 1, c.L, e, l, blk, loc);
+    const LevelDev& V = c.lev[l];
+    const uint32_t v = V.cell[(blk << (2 * D)) | loc];
+    if (!(v & ACT)) continue;
+    int I[D];
+    elem_coords<D>(V, blk, loc, I);
+    int l0 = -1;
+    for (int q = 0; q < l; ++q) {
+      int A[D];
+#pragma unroll
+      for (int d = 0; d < D; ++d) A[d] = I[d] >> (l - q);
+      if (cell_get<D>(c, q, A) & ACT) l0 = q;
+    }
+    if (l0 < 0) continue;
+    for (int q = l0; q < l; ++q) {
+      int A[D];
+#pragma unroll
+      for (int d = 0; d < D; ++d) A[d] = I[d] >> (l - q);
+      cell_or<D>(c, q, A, CUL);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// _split_hier_ for all levels (adaptive_gimp.py:111-118) resolved in one pass:
+// a cell with CULLING is emptied; a cell whose parent has CULLING becomes
+// ACTIVATED.  CULLING bits are not written here, so the pass is order-free.
+// Cells that end exactly ACTIVATED then mark their corner nodes
+// (_activate_mask, adaptive_gimp.py:142-149).  The CULLING bit itself stays
+// set until the next substep clears the block; readback masks it out.
+template <int D>
+__global__ void k_resolve(Ctx c) {
+  const long long tot = total_elems(c, 0, c.L, D);
+  GS_LOOP(e, tot) {
+    int l, loc;
+    long long blk;
+    decode_elem<D>(c, 0, c.L, e, l, blk, loc);
+    const LevelDev& V = c.lev[l];
+    const long long idx = (blk << (2 * D)) | loc;
+    const uint32_t v = V.cell[idx];
+    int I[D];
+    bool have_I = false;
+    uint32_t nv = v;
+    if (!c.is_static) {
+      bool pc = false;
+      if (l > 0) {
+        elem_coords<D>(V, blk, loc, I);
+        have_I = true;
+        int A[D];
+#pragma unroll
+        for (int d = 0; d < D; ++d) A[d] = I[d] >> 1;
+        pc = (cell_get<D>(c, l - 1, A) & CUL) != 0u;
+      }
+      if (v & CUL)
+        nv = v & ~ACT;
+      else if ((v & ACT) || pc)
+        nv = v | ACT;
+      if (nv != v) V.cell[idx] = nv;
+    }
+    if (nv != ACT) continue;
+    if (!have_I) elem_coords<D>(V, blk, loc, I);
+#pragma unroll
+    for (int a = 0; a < (1 << D); ++a) {
+      int J[D];
+#pragma unroll
+      for (int d = 0; d < D; ++d) J[d] = I[d] + ((a >> (D - 1 - d)) & 1);
+      nm_or<D>(c, l, J, ACT);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// _mark_ghost_and_T_junction for every level (adaptive_gimp.py:155-187).
+template <int D>
+__global__ void k_ghost_tj(Ctx c) {
+  const long long tot = total_elems(c, 0, c.L, D);
+  GS_LOOP(e, tot) {
+    int l, loc;
+    long long blk;
+    decode_elem<D>(c, 0, c.L, e, l, blk, loc);
+    const LevelDev& V = c.lev[l];
+    if (V.cell[(blk << (2 * D)) | loc] != ACT) continue;
+    int I[D];
+    elem_coords<D>(V, blk, loc, I);
+    const int lsz = V.size;
+#pragma unroll 1
+    for (int f = 0; f < 2 * D; ++f) {
+      const int ax = f >> 1, side = f & 1;
+      int I1[D];
+#pragma unroll
+      for (int d = 0; d < D; ++d) I1[d] = I[d];
+      I1[ax] += side ? -1 : 1;
+      bool inr = true;
+#pragma unroll
+      for (int d = 0; d < D; ++d) inr = inr && I1[d] >= 0 && I1[d] < lsz;
+      if (!inr) continue;
+      if (V.cell[elem_of<D>(V, I1)] == ACT) continue;
+      int lp = -1;  // _heriarchical_check
+      for (int q = 0; q <= l; ++q) {
+        int A[D];
+#pragma unroll
+        for (int d = 0; d < D; ++d) A[d] = I1[d] >> (l - q);
+        if (cell_get<D>(c, q, A) == ACT) lp = q;
+      }
+      if (lp < 0) continue;
+      const int md = (1 << (l - lp)) - 1;
+#pragma unroll
+      for (int a = 0; a < (1 << D); ++a) {
+        int J[D];
+        bool off = false;
+        bool face = true;
+#pragma unroll
+        for (int d = 0; d < D; ++d) {
+          const int bit = (a >> (D - 1 - d)) & 1;
+          if (d == ax && bit != side) face = false;
+          J[d] = I1[d] + bit;
+          off = off || (J[d] & md) != 0;
+        }
+        if (face && off) nm_or<D>(c, l, J, TJ);
+      }
+      for (int l0 = lp + 1; l0 <= l; ++l0) {
+        int Ip[D];
+#pragma unroll
+        for (int d = 0; d < D; ++d) Ip[d] = I1[d] >> (l - l0);
+        cell_or<D>(c, l0, Ip, GHO);
+#pragma unroll
+        for (int a = 0; a < (1 << D); ++a) {
+          int J[D];
+#pragma unroll
+          for (int d = 0; d < D; ++d) J[d] = Ip[d] + ((a >> (D - 1 - d)) & 1);
+          if (nm_get<D>(c, l0, J) == 0u) nm_or<D>(c, l0, J, GHO);
+        }
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// level_mapping (adaptive_gimp.py:189-216): fl_p = finest level with an
+// ACTIVATED cell among the 2^d cells around the particle; bin = (fl_p, block
+// of base).  The rank inside the bin comes from a warp-aggregated atomic.
+template <int D>
+__global__ void k_bin(Ctx c) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  const int lane = threadIdx.x & 31;
+  int bin = -1;
+  if (p < c.N) {
+    float xp[D];
+    bool esc = false;
+#pragma unroll
+    for (int d = 0; d < D; ++d) {
+      xp[d] = c.x[(long long)d * c.N + p];
+      if (!(xp[d] >= 0.f && xp[d] < 1.f)) esc = true;
+    }
+    int fl = -1;
+    if (!esc) {
+      for (int l = 0; l < c.L; ++l) {
+        const float inv = (float)(c.coarsest << l);
+        int base[D];
+#pragma unroll
+        for (int d = 0; d < D; ++d) base[d] = (int)(xp[d] * inv + 0.5f) - 1;
+#pragma unroll
+        for (int a = 0; a < (1 << D); ++a) {
+          int I[D];
+#pragma unroll
+          for (int d = 0; d < D; ++d) I[d] = base[d] + ((a >> (D - 1 - d)) & 1);
+          if (cell_get<D>(c, l, I) == ACT) fl = l;
+        }
+      }
+      if (fl >= 0) {
+        const float inv = (float)(c.coarsest << fl);
+        const LevelDev& V = c.lev[fl];
+        long long b = 0;
+        bool ok = true;
+#pragma unroll
+        for (int d = 0; d < D; ++d) {
+          const int cb = ((((int)(xp[d] * inv + 0.5f)) - 1) >> 2) + 1;
+          ok = ok && cb >= 0 && cb < V.nb;
+          b = b * V.nb + cb;
+        }
+        const int bi = ok ? V.bmap[b] : -1;
+        if (bi < 0) {
+          set_err(c, ERR_NOBIN);
+          fl = -1;
+        } else {
+          int lb = 0;
+          for (int q = 0; q < fl; ++q) lb += c.ctr[CTR_LEVEL + q];
+          bin = lb + bi;
+        }
+      }
+    }
+    c.fl[p] = fl;
+  }
+  const unsigned grp = __match_any_sync(0xffffffffu, bin);
+  const int leader = __ffs(grp) - 1;
+  const int rank = __popc(grp & ((1u << lane) - 1u));
+  int base = 0;
+  if (bin >= 0 && lane == leader) base = atomicAdd(&c.bin_count[bin], __popc(grp));
+  base = __shfl_sync(0xffffffffu, base, leader);
+  if (bin >= 0) {
+    c.bin_of[p] = bin;
+    c.rank_of[p] = base + rank;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Bin storage: each CTA scans 1024 bins, reserves their particles and work
+// items with one atomic each, and writes the work-item descriptors.  Bins of
+// different CTAs land in any order; a bin's particles stay contiguous.
+__device__ __forceinline__ int2 block_incl_scan2(int a, int b, int2* warp_sums) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int ya = __shfl_up_sync(0xffffffffu, a, o);
+    const int yb = __shfl_up_sync(0xffffffffu, b, o);
+    if (lane >= o) {
+      a += ya;
+      b += yb;
+    }
+  }
+  if (lane == 31) warp_sums[w] = make_int2(a, b);
+  __syncthreads();
+  if (w == 0) {
+    const int nw = blockDim.x >> 5;
+    int2 s = lane < nw ? warp_sums[lane] : make_int2(0, 0);
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int ya = __shfl_up_sync(0xffffffffu, s.x, o);
+      const int yb = __shfl_up_sync(0xffffffffu, s.y, o);
+      if (lane >= o) {
+        s.x += ya;
+        s.y += yb;
+      }
+    }
+    if (lane < nw) warp_sums[lane] = s;
+  }
+  __syncthreads();
+  if (w > 0) {
+    const int2 pre = warp_sums[w - 1];
+    a += pre.x;
+    b += pre.y;
+  }
+  return make_int2(a, b);
+}
+
+__global__ void __launch_bounds__(1024) k_offsets(Ctx c) {
+  __shared__ int2 warp_sums[32];
+  __shared__ int2 s_base;
+  long long nb = 0;
+  for (int q = 0; q < c.L; ++q) nb += c.ctr[CTR_LEVEL + q];
+  for (long long t0 = (long long)blockIdx.x * blockDim.x; t0 < nb; t0 += (long long)gridDim.x * blockDim.x) {
+    const long long b = t0 + threadIdx.x;
+    int cnt = 0;
+    if (b < nb) {
+      cnt = c.bin_count[b];
+      if (cnt) c.bin_count[b] = 0;
+    }
+    const int nch = (cnt + CHUNK - 1) / CHUNK;
+    const int2 inc = block_incl_scan2(cnt, nch, warp_sums);
+    if (threadIdx.x == blockDim.x - 1) {
+      s_base.x = inc.x ? atomicAdd(&c.ctr[CTR_BINCUR], inc.x) : 0;
+      s_base.y = inc.y ? atomicAdd(&c.ctr[CTR_CHUNKS], inc.y) : 0;
+    }
+    __syncthreads();
+    if (cnt > 0) {
+      const int start = s_base.x + inc.x - cnt;
+      c.bin_start[b] = start;
+      const int ch0 = s_base.y + inc.y - nch;
+      int l = 0;
+      long long r = b;
+      while (l < c.L - 1 && r >= c.ctr[CTR_LEVEL + l]) {
+        r -= c.ctr[CTR_LEVEL + l];
+        ++l;
+      }
+      const int blk = c.lev[l].blist[r];
+      for (int j = 0; j < nch; ++j) c.chunks[ch0 + j] = make_int4(l, blk, start + j * CHUNK, min(CHUNK, cnt - j * CHUNK));
+    }
+    __syncthreads();
+  }
+}
+
+__global__ void k_scatter(Ctx c) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= c.N || c.fl[p] < 0) return;
+  c.perm[c.bin_start[c.bin_of[p]] + c.rank_of[p]] = p;
+}
+
+// ---------------------------------------------------------------------------
+// launch sequence (transfer kernels are in transfer.cu)
+template <int D>
+void launch_transfer(const Ctx& c, cudaStream_t s, cudaEvent_t* ev);
+
+template <int D>
+static void run_topology(const Ctx& c, cudaStream_t s, cudaEvent_t* ev) {
+  const int G = c.sms * 8;
+  const int Gp = (c.N + 255) / 256;
+  if (ev) cudaEventRecord(ev[0], s);
+  k_clear<D><<<G, 256, 0, s>>>(c);
+  cudaMemsetAsync(c.ctr + CTR_LEVEL, 0, MAXL * sizeof(int32_t), s);
+  if (Gp) k_touch_activate<D><<<Gp, 256, 0, s>>>(c);
+  k_dilate<D><<<G, 256, 0, s>>>(c);
+  if (ev) cudaEventRecord(ev[1], s);
+  if (!c.is_static) k_mark_hier<D><<<G, 256, 0, s>>>(c);
+  k_resolve<D><<<G, 256, 0, s>>>(c);
+  k_ghost_tj<D><<<G, 256, 0, s>>>(c);
+  if (ev) cudaEventRecord(ev[2], s);
+  if (Gp) k_bin<D><<<Gp, 256, 0, s>>>(c);
+  k_offsets<<<G / 4, 1024, 0, s>>>(c);
+  if (Gp) k_scatter<<<Gp, 256, 0, s>>>(c);
+  if (ev) cudaEventRecord(ev[3], s);
+}
+
+void launch_substep(const Ctx& c, cudaStream_t s, cudaEvent_t* ev) {
+  if (c.dim == 2) {
+    run_topology<2>(c, s, ev);
+    launch_transfer<2>(c, s, ev);
+  } else {
+    run_topology<3>(c, s, ev);
+    launch_transfer<3>(c, s, ev);
+  }
+}
+
+int kernels_per_substep(const Ctx& c) {
+  const int topo = 9 - (c.is_static ? 1 : 0) - (c.N ? 0 : 3);  // kernels (the memset node is not counted)
+  return topo + 3 + 2 * (c.L - 1);
+}
+
+}  // namespace agimp

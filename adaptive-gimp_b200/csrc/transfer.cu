@@ -1,0 +1,545 @@
+// Particle/grid transfer kernels of the adaptive GIMP substep.
+//
+// Reference steps (adaptive_gimp.py, g1n0st/adaptive-gimp):
+//   230-250 p2g               -> k_p2g      (all levels in one launch)
+//   289-301 grid_restriction  -> k_restrict (one launch per level, fine->coarse)
+//   277-287 grid_op           -> k_gridop   (all levels in one launch)
+//   303-321 grid_prolongation -> k_prolong  (one launch per level, coarse->fine)
+//   252-275 g2p               -> k_g2p      (all levels in one launch)
+//
+// P2G/G2P: one CTA per work item = up to CHUNK particles of one bin (one 4^d
+// block of one level).  A bin's particles touch only the (4+2)^d nodes from
+// the block origin, so P2G accumulates into that tile in shared memory and
+// flushes it with one float4 atomic per touched node; G2P stages the same tile
+// of velocities in shared memory before gathering.
+//
+// Restriction and prolongation are written as gathers (each destination node
+// sums its sources) instead of the reference's scatters, so they need no
+// atomics; the set of terms and their weights are the reference's.
+#include "common.cuh"
+
+namespace agimp {
+
+#define GS_LOOP(i, n) \
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < (n); i += (long long)gridDim.x * blockDim.x)
+
+// GIMP weights factorised per axis.  get_weight_stencil (adaptive_gimp.py:
+// 218-228) sums get_linear_weight (utils.py:18-42) over the 2^d cells dI and
+// 2^d corners cell_ that meet at node n = dI + cell_; the summand is a product
+// over axes, so the sum is the product of per-axis sums:
+//   w[n] = prod_d W_d[n_d] / (2^d (2r)^d),
+//   dw[n]_a = G_a[n_a] prod_{d!=a} W_d[n_d] / (2^(d-1) (2r)^d).
+__device__ __forceinline__ void axis_weights(float t, float r, float* W, float* G) {
+  // dI = 0: interval around t + 1; dI = 1: around t
+  const float bmin0 = fminf(fmaxf(t + 1.f - r, 0.f), 1.f), bmax0 = fminf(fmaxf(t + 1.f + r, 0.f), 1.f);
+  const float bmin1 = fminf(fmaxf(t - r, 0.f), 1.f), bmax1 = fminf(fmaxf(t + r, 0.f), 1.f);
+  // corner cell_ = 0: mx = 1 - bmin, mn = 1 - bmax; cell_ = 1: mx = bmax, mn = bmin
+  const float a0 = 1.f - bmin0, b0 = 1.f - bmax0;
+  const float a1 = 1.f - bmin1, b1 = 1.f - bmax1;
+  const float w00 = a0 * a0 - b0 * b0, g00 = b0 - a0;                 // dI 0, cell 0 -> node 0
+  const float w01 = bmax0 * bmax0 - bmin0 * bmin0, g01 = bmax0 - bmin0; // dI 0, cell 1 -> node 1
+  const float w10 = a1 * a1 - b1 * b1, g10 = b1 - a1;                 // dI 1, cell 0 -> node 1
+  const float w11 = bmax1 * bmax1 - bmin1 * bmin1, g11 = bmax1 - bmin1; // dI 1, cell 1 -> node 2
+  W[0] = w00;
+  W[1] = w01 + w10;
+  W[2] = w11;
+  G[0] = g00;
+  G[1] = g01 + g10;
+  G[2] = g11;
+}
+
+template <int D>
+struct Stencil {
+  float W[D][3], G[D][3];
+  float kw, kg;
+};
+
+template <int D>
+__device__ __forceinline__ void make_stencil(const float* tc, float r, Stencil<D>& s) {
+#pragma unroll
+  for (int d = 0; d < D; ++d) axis_weights(tc[d], r, s.W[d], s.G[d]);
+  const float r2 = 2.f * r;
+  s.kw = (D == 2) ? 1.f / (4.f * r2 * r2) : 1.f / (8.f * r2 * r2 * r2);
+  s.kg = (D == 2) ? 1.f / (2.f * r2 * r2) : 1.f / (4.f * r2 * r2 * r2);
+}
+
+template <int D>
+__device__ __forceinline__ void node_weight(const Stencil<D>& s, const int* n, float& w, float* g) {
+  if (D == 2) {
+    const float wx = s.W[0][n[0]], wy = s.W[1][n[1]];
+    w = wx * wy * s.kw;
+    g[0] = s.G[0][n[0]] * wy * s.kg;
+    g[1] = wx * s.G[1][n[1]] * s.kg;
+  } else {
+    const float wx = s.W[0][n[0]], wy = s.W[1][n[1]], wz = s.W[2][n[2]];
+    w = wx * wy * wz * s.kw;
+    g[0] = s.G[0][n[0]] * wy * wz * s.kg;
+    g[1] = wx * s.G[1][n[1]] * wz * s.kg;
+    g[2] = wx * wy * s.G[2][n[2]] * s.kg;
+  }
+}
+
+template <int D>
+__device__ __forceinline__ void chunk_origin(const LevelDev& V, long long blk, int* O) {
+#pragma unroll
+  for (int d = D - 1; d >= 0; --d) {
+    O[d] = (int)(blk % V.nb) * 4 - HALO;
+    blk /= V.nb;
+  }
+}
+
+// ---------------------------------------------------------------------------
+template <int D>
+__global__ void __launch_bounds__(CHUNK) k_p2g(Ctx c) {
+  constexpr int TN = (D == 2) ? 36 : 216;  // (4+2)^d node tile
+  __shared__ float sm[4][TN];
+  const int nch = c.ctr[CTR_CHUNKS];
+  const float pw = (D == 2) ? 0.25f : 0.125f;                                  // 0.5**dim
+  const float rd = (D == 2) ? c.radius * c.radius : c.radius * c.radius * c.radius;  // radius**dim
+  for (int ch = blockIdx.x; ch < nch; ch += gridDim.x) {
+    const int4 wd = c.chunks[ch];
+    const int l = wd.x;
+    const LevelDev& V = c.lev[l];
+    for (int i = threadIdx.x; i < 4 * TN; i += blockDim.x) (&sm[0][0])[i] = 0.f;
+    int O[D];
+    chunk_origin<D>(V, wd.y, O);
+    __syncthreads();
+    if ((int)threadIdx.x < wd.w) {
+      const int p = c.perm[wd.z + threadIdx.x];
+      const long long N = c.N;
+      const float inv = (float)(c.coarsest << l);
+      const float dx = 1.f / inv;
+      float xp[D], vp[D], F[D * D], Cm[D * D];
+#pragma unroll
+      for (int d = 0; d < D; ++d) {
+        xp[d] = c.x[d * N + p];
+        vp[d] = c.v[d * N + p];
+      }
+#pragma unroll
+      for (int i = 0; i < D * D; ++i) {
+        F[i] = c.F[i * N + p];
+        Cm[i] = c.C[i * N + p];
+      }
+      const float mp = c.m[p];
+      int base[D];
+      float tc[D];
+#pragma unroll
+      for (int d = 0; d < D; ++d) {
+        const float xs = xp[d] * inv;
+        base[d] = (int)(xs + 0.5f) - 1;
+        tc[d] = xs - (float)(base[d] + 1);
+      }
+      // get_stress (utils.py:11-16), scaled as in adaptive_gimp.py:240
+      float mu = c.mu, la = c.la;
+      if (c.plast == 1) {
+        const float h = expf(c.xi * (1.f - c.Jp[p]));
+        mu *= h;
+        la *= h;
+      }
+      float Rm[D * D];
+      polar_rot<D>(F, Rm);
+      const float J = det<D>(F);
+      const float tmu = 2.f * mu;
+      const float diag = la * J * (J - 1.f);
+      const float sc = (-c.dt * pw) / (rd * dx);
+      float S[D * D];
+#pragma unroll
+      for (int i = 0; i < D; ++i)
+#pragma unroll
+        for (int j = 0; j < D; ++j) {
+          float a = 0.f;
+#pragma unroll
+          for (int k = 0; k < D; ++k) a += (tmu * (F[i * D + k] - Rm[i * D + k])) * F[j * D + k];
+          S[i * D + j] = sc * (a + (i == j ? diag : 0.f));
+        }
+      Stencil<D> st;
+      make_stencil<D>(tc, c.radius, st);
+      int rb[D];
+#pragma unroll
+      for (int d = 0; d < D; ++d) rb[d] = base[d] - O[d];
+#pragma unroll
+      for (int k = 0; k < ((D == 2) ? 9 : 27); ++k) {
+        int n[D];
+        int t = k;
+#pragma unroll
+        for (int d = D - 1; d >= 0; --d) {
+          n[d] = t % 3;
+          t /= 3;
+        }
+        float w, gw[D];
+        node_weight<D>(st, n, w, gw);
+        const float wm = w * mp;
+        float mom[D];
+#pragma unroll
+        for (int i = 0; i < D; ++i) {
+          float cd = 0.f, sg = 0.f;
+#pragma unroll
+          for (int j = 0; j < D; ++j) {
+            cd += Cm[i * D + j] * ((float)n[j] - (tc[j] + 1.f));
+            sg += S[i * D + j] * gw[j];
+          }
+          mom[i] = wm * (vp[i] + cd) + sg;
+        }
+        int ti = 0;
+#pragma unroll
+        for (int d = 0; d < D; ++d) ti = ti * 6 + rb[d] + n[d];
+#pragma unroll
+        for (int i = 0; i < D; ++i) atomicAdd(&sm[i][ti], mom[i]);
+        atomicAdd(&sm[3][ti], wm);
+      }
+    }
+    __syncthreads();
+    for (int t = threadIdx.x; t < TN; t += blockDim.x) {
+      const float4 val = make_float4(sm[0][t], sm[1][t], sm[2][t], sm[3][t]);
+      if (val.x == 0.f && val.y == 0.f && val.z == 0.f && val.w == 0.f) continue;
+      int I[D];
+      int tt = t;
+#pragma unroll
+      for (int d = D - 1; d >= 0; --d) {
+        I[d] = O[d] + tt % 6;
+        tt /= 6;
+      }
+      if (!in_store<D>(V, I)) {
+        set_err(c, ERR_OOB);
+        continue;
+      }
+      atomicAdd(&V.node[elem_of<D>(V, I)], val);
+    }
+    __syncthreads();
+  }
+}
+
+// ---------------------------------------------------------------------------
+// grid_restriction(l) as a gather over coarse nodes K of level l-1.
+template <int D>
+__global__ void k_restrict(Ctx c, int l) {
+  const LevelDev& Vc = c.lev[l - 1];
+  const LevelDev& Vf = c.lev[l];
+  const long long tot = (long long)c.ctr[CTR_LEVEL + l - 1] << (2 * D);
+  const int lsz = Vf.size, l0sz = Vc.size;
+  GS_LOOP(e, tot) {
+    const long long blk = Vc.blist[e >> (2 * D)];
+    const int loc = (int)(e & ((1 << (2 * D)) - 1));
+    int K[D];
+    elem_coords<D>(Vc, blk, loc, K);
+    bool inr = true;
+#pragma unroll
+    for (int d = 0; d < D; ++d) inr = inr && K[d] >= 0 && K[d] <= l0sz;
+    if (!inr || !is_valid(nm_get<D>(c, l - 1, K))) continue;
+    float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
+    bool any = false;
+#pragma unroll
+    for (int a = 0; a < ((D == 2) ? 9 : 27); ++a) {
+      int I[D], nrm = 0;
+      int t = a;
+      bool ok = true;
+#pragma unroll
+      for (int d = D - 1; d >= 0; --d) {
+        const int dI = t % 3 - 1;
+        t /= 3;
+        I[d] = 2 * K[d] - dI;
+        nrm += dI != 0;
+        ok = ok && I[d] >= 0 && I[d] <= lsz;
+      }
+      if (!ok) continue;
+      const uint32_t nm = nm_get<D>(c, l, I);
+      if (!((is_activated(nm) && nrm == 0) || is_tj(nm) || is_ghost(nm))) continue;
+      const float w = (nrm == 0) ? 1.f : (nrm == 1) ? 0.5f : (nrm == 2) ? 0.25f : 0.125f;
+      const float4 f = Vf.node[elem_of<D>(Vf, I)];
+      acc.x += f.x * w;
+      acc.y += f.y * w;
+      acc.z += f.z * w;
+      acc.w += f.w * w;
+      any = true;
+    }
+    if (!any) continue;
+    float4* dst = &Vc.node[(blk << (2 * D)) | loc];
+    float4 o = *dst;
+    o.x += acc.x;
+    o.y += acc.y;
+    o.z += acc.z;
+    o.w += acc.w;
+    *dst = o;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// grid_op (adaptive_gimp.py:277-287) for all levels.
+template <int D>
+__global__ void k_gridop(Ctx c) {
+  const long long tot = total_elems(c, 0, c.L, D);
+  GS_LOOP(e, tot) {
+    int l, loc;
+    long long blk;
+    decode_elem<D>(c, 0, c.L, e, l, blk, loc);
+    const LevelDev& V = c.lev[l];
+    int I[D];
+    elem_coords<D>(V, blk, loc, I);
+    bool inr = true;
+#pragma unroll
+    for (int d = 0; d < D; ++d) inr = inr && I[d] >= 0 && I[d] <= V.size;
+    if (!inr) continue;
+    const long long idx = (blk << (2 * D)) | loc;
+    const float4 nd = V.node[idx];
+    if (!(nd.w > 0.f)) continue;
+    if (!is_activated(nm_get<D>(c, l, I))) continue;
+    float vv[3] = {nd.x, nd.y, nd.z};
+    const int s = c.L - 1 - l;
+    bool band = false;
+#pragma unroll
+    for (int d = 0; d < D; ++d) {
+      vv[d] = vv[d] / nd.w;
+      vv[d] = vv[d] + c.grav[d] * c.dt;
+      const int P = I[d] * (1 << s);
+      if (P < c.gap || P > c.sz - c.gap) {
+        band = true;
+        if (c.bmode == 0) vv[d] = 0.f;
+      }
+    }
+    if (c.bmode == 1 && band)
+#pragma unroll
+      for (int d = 0; d < D; ++d) vv[d] = 0.f;
+    if (c.ncol) {
+      const double ldx = 1.0 / (double)(c.coarsest << l);
+      for (int k = 0; k < c.ncol; ++k) {
+        bool in = true;
+#pragma unroll
+        for (int d = 0; d < D; ++d) {
+          const double pos = (double)I[d] * ldx;
+          in = in && pos >= c.col[k][d] && pos <= c.col[k][3 + d];
+        }
+        if (in)
+#pragma unroll
+          for (int d = 0; d < D; ++d) vv[d] = 0.f;
+      }
+    }
+    V.node[idx] = make_float4(vv[0], vv[1], vv[2], nd.w);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// grid_prolongation(l) as a gather over fine nodes J of level l: T-junction
+// and ghost nodes take the weighted sum of their valid coarse neighbours,
+// other all-even nodes take the coincident coarse velocity if they are
+// activated and it is valid, else 0; the rest keep their value.
+template <int D>
+__global__ void k_prolong(Ctx c, int l) {
+  const LevelDev& Vc = c.lev[l - 1];
+  const LevelDev& Vf = c.lev[l];
+  const long long tot = (long long)c.ctr[CTR_LEVEL + l] << (2 * D);
+  const int lsz = Vf.size;
+  GS_LOOP(e, tot) {
+    const long long blk = Vf.blist[e >> (2 * D)];
+    const int loc = (int)(e & ((1 << (2 * D)) - 1));
+    int J[D];
+    elem_coords<D>(Vf, blk, loc, J);
+    bool inr = true, even = true;
+#pragma unroll
+    for (int d = 0; d < D; ++d) {
+      inr = inr && J[d] >= 0 && J[d] <= lsz;
+      even = even && (J[d] & 1) == 0;
+    }
+    if (!inr) continue;
+    const uint32_t nm = nm_get<D>(c, l, J);
+    const bool tg = is_tj(nm) || is_ghost(nm);
+    if (!tg && !even) continue;
+    float acc[3] = {0.f, 0.f, 0.f};
+    if (tg) {
+      int nodd = 0;
+#pragma unroll
+      for (int d = 0; d < D; ++d) nodd += J[d] & 1;
+      const float w = (nodd == 0) ? 1.f : (nodd == 1) ? 0.5f : (nodd == 2) ? 0.25f : 0.125f;
+#pragma unroll
+      for (int a = 0; a < (1 << D); ++a) {
+        int K[D];
+        bool use = true;
+#pragma unroll
+        for (int d = 0; d < D; ++d) {
+          const int bit = (a >> d) & 1;
+          if (J[d] & 1)
+            K[d] = (J[d] - 1) / 2 + bit;
+          else {
+            K[d] = J[d] / 2;
+            use = use && bit == 0;
+          }
+        }
+        if (!use || !is_valid(nm_get<D>(c, l - 1, K))) continue;
+        const float4 cv = Vc.node[elem_of<D>(Vc, K)];
+        acc[0] += cv.x * w;
+        acc[1] += cv.y * w;
+        acc[2] += cv.z * w;
+      }
+    } else if (is_activated(nm)) {
+      int K[D];
+#pragma unroll
+      for (int d = 0; d < D; ++d) K[d] = J[d] / 2;
+      if (is_valid(nm_get<D>(c, l - 1, K))) {
+        const float4 cv = Vc.node[elem_of<D>(Vc, K)];
+        acc[0] = cv.x;
+        acc[1] = cv.y;
+        acc[2] = cv.z;
+      }
+    }
+    float4* dst = &Vf.node[(blk << (2 * D)) | loc];
+    float4 o = *dst;
+    o.x = acc[0];
+    o.y = acc[1];
+    o.z = acc[2];
+    *dst = o;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// g2p (adaptive_gimp.py:252-275), plus the snow return map (extension).
+template <int D>
+__device__ __forceinline__ void snow_project(const Ctx& c, float* F, int p) {
+  float U[D * D], sg[D], V[D * D];
+  if (D == 2)
+    svd2(F, U, sg, V);
+  else
+    svd3(F, U, sg, V);
+  float Jo = 1.f, Jn = 1.f, sc[D];
+#pragma unroll
+  for (int d = 0; d < D; ++d) {
+    const float cl = fminf(fmaxf(sg[d], 1.f - c.theta_c), 1.f + c.theta_s);
+    Jo *= sg[d];
+    Jn *= cl;
+    sc[d] = cl;
+  }
+  c.Jp[p] = c.Jp[p] * Jo / Jn;
+#pragma unroll
+  for (int i = 0; i < D; ++i)
+#pragma unroll
+    for (int j = 0; j < D; ++j) {
+      float a = 0.f;
+#pragma unroll
+      for (int k = 0; k < D; ++k) a += U[i * D + k] * sc[k] * V[j * D + k];
+      F[i * D + j] = a;
+    }
+}
+
+template <int D>
+__global__ void __launch_bounds__(CHUNK) k_g2p(Ctx c) {
+  constexpr int TN = (D == 2) ? 36 : 216;
+  __shared__ float sv[D][TN];
+  const int nch = c.ctr[CTR_CHUNKS];
+  const float pw = (D == 2) ? 0.25f : 0.125f;
+  const float rd = (D == 2) ? c.radius * c.radius : c.radius * c.radius * c.radius;
+  for (int ch = blockIdx.x; ch < nch; ch += gridDim.x) {
+    const int4 wd = c.chunks[ch];
+    const int l = wd.x;
+    const LevelDev& V = c.lev[l];
+    int O[D];
+    chunk_origin<D>(V, wd.y, O);
+    for (int t = threadIdx.x; t < TN; t += blockDim.x) {
+      int I[D];
+      int tt = t;
+#pragma unroll
+      for (int d = D - 1; d >= 0; --d) {
+        I[d] = O[d] + tt % 6;
+        tt /= 6;
+      }
+      float4 nd = make_float4(0.f, 0.f, 0.f, 0.f);
+      if (in_store<D>(V, I)) nd = V.node[elem_of<D>(V, I)];
+      sv[0][t] = nd.x;
+      sv[1][t] = nd.y;
+      if (D == 3) sv[D - 1][t] = nd.z;
+    }
+    __syncthreads();
+    if ((int)threadIdx.x < wd.w) {
+      const int p = c.perm[wd.z + threadIdx.x];
+      const long long N = c.N;
+      const float inv = (float)(c.coarsest << l);
+      const float dx = 1.f / inv;
+      float xp[D];
+#pragma unroll
+      for (int d = 0; d < D; ++d) xp[d] = c.x[d * N + p];
+      int base[D], rb[D];
+      float tc[D];
+#pragma unroll
+      for (int d = 0; d < D; ++d) {
+        const float xs = xp[d] * inv;
+        base[d] = (int)(xs + 0.5f) - 1;
+        tc[d] = xs - (float)(base[d] + 1);
+        rb[d] = base[d] - O[d];
+      }
+      Stencil<D> st;
+      make_stencil<D>(tc, c.radius, st);
+      float nv[D], G[D * D];
+#pragma unroll
+      for (int i = 0; i < D; ++i) nv[i] = 0.f;
+#pragma unroll
+      for (int i = 0; i < D * D; ++i) G[i] = 0.f;
+#pragma unroll
+      for (int k = 0; k < ((D == 2) ? 9 : 27); ++k) {
+        int n[D];
+        int t = k;
+#pragma unroll
+        for (int d = D - 1; d >= 0; --d) {
+          n[d] = t % 3;
+          t /= 3;
+        }
+        float w, gw[D];
+        node_weight<D>(st, n, w, gw);
+        int ti = 0;
+#pragma unroll
+        for (int d = 0; d < D; ++d) ti = ti * 6 + rb[d] + n[d];
+        float gv[D];
+#pragma unroll
+        for (int i = 0; i < D; ++i) gv[i] = sv[i][ti];
+#pragma unroll
+        for (int i = 0; i < D; ++i) {
+          nv[i] += gv[i] * w;
+#pragma unroll
+          for (int j = 0; j < D; ++j) G[i * D + j] += gv[i] * gw[j];
+        }
+      }
+      float F[D * D];
+#pragma unroll
+      for (int i = 0; i < D * D; ++i) F[i] = c.F[i * N + p];
+#pragma unroll
+      for (int d = 0; d < D; ++d) {
+        c.v[d * N + p] = nv[d];
+        c.x[d * N + p] = xp[d] + c.dt * nv[d];
+      }
+#pragma unroll
+      for (int i = 0; i < D * D; ++i) c.C[i * N + p] = G[i];
+      const float s = (c.dt * pw) / (rd * dx);
+      float Fn[D * D];
+#pragma unroll
+      for (int i = 0; i < D; ++i)
+#pragma unroll
+        for (int j = 0; j < D; ++j) {
+          float a = 0.f;
+#pragma unroll
+          for (int k = 0; k < D; ++k) a += ((i == k ? 1.f : 0.f) + s * G[i * D + k]) * F[k * D + j];
+          Fn[i * D + j] = a;
+        }
+      if (c.plast == 1) snow_project<D>(c, Fn, p);
+#pragma unroll
+      for (int i = 0; i < D * D; ++i) c.F[i * N + p] = Fn[i];
+    }
+    __syncthreads();
+  }
+}
+
+// ---------------------------------------------------------------------------
+template <int D>
+void launch_transfer(const Ctx& c, cudaStream_t s, cudaEvent_t* ev) {
+  const int G = c.sms * 8;
+  k_p2g<D><<<G, CHUNK, 0, s>>>(c);
+  if (ev) cudaEventRecord(ev[4], s);
+  for (int l = c.L - 1; l >= 1; --l) k_restrict<D><<<G, 256, 0, s>>>(c, l);
+  if (ev) cudaEventRecord(ev[5], s);
+  k_gridop<D><<<G, 256, 0, s>>>(c);
+  if (ev) cudaEventRecord(ev[6], s);
+  for (int l = 1; l < c.L; ++l) k_prolong<D><<<G, 256, 0, s>>>(c, l);
+  if (ev) cudaEventRecord(ev[7], s);
+  k_g2p<D><<<G, CHUNK, 0, s>>>(c);
+  if (ev) cudaEventRecord(ev[8], s);
+}
+
+template void launch_transfer<2>(const Ctx&, cudaStream_t, cudaEvent_t*);
+template void launch_transfer<3>(const Ctx&, cudaStream_t, cudaEvent_t*);
+
+}  // namespace agimp

@@ -1,0 +1,360 @@
+#!/usr/bin/env python
+"""Benchmark of the adaptive GIMP substep on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl agimp|reference] [--config 3]
+
+Metric: particle-substeps/s (particles x substeps / time) of the whole job.
+Default workload: the 3D dynamic-adaptivity scene (3 levels, 64^3..256^3,
+~1.9M particles, snow plasticity, slab collider, prescribed levels recomputed
+every 10 substeps), synthetic seeded data.  A step is one substep of the
+whole scene; the refinement every 10th step is inside the timed region.
+
+--impl agimp (default): the CUDA path.  `value` is device time (CUDA events
+  on the launching stream, max over ranks) with the state resident in HBM;
+  `e2e` is the same metric through the public Python API with host buffers:
+  the scene is uploaded from pinned host memory and x_p is read back to
+  pinned host memory after every substep, all inside the timed region.
+--impl reference: the reference's algorithm on the host cores (the CPU
+  oracle restatement, OpenMP on all host threads) on the same scene; rank 0
+  only.
+
+Multi-GPU: replicas only (one independent scene per rank, seeded by rank);
+the single-scene substep does not shard.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import re
+import statistics
+import subprocess
+import sys
+import time
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(REPO, "adaptive-gimp_b200"))
+sys.path.insert(0, os.path.join(REPO, "oracle"))
+
+METRIC = "particle-substeps/s"
+FALLBACK_HBM_GBS = 6650.0
+# algorithmic bytes per particle-substep (f32 SoA), counted once per kernel
+BYTES = {  # (dim, with Jp) -> (P2G, G2P)
+    (2, False): (52, 72), (2, True): (56, 80),
+    (3, False): (100, 144), (3, True): (104, 152),
+}
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", default="agimp", choices=["agimp", "reference"])
+    ap.add_argument("--config", type=int, default=3)
+    ap.add_argument("--cpu-seconds", type=float, default=20.0, help="budget of the CPU baseline sample")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+def peaks():
+    try:
+        with open(os.path.join(REPO, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def profile_traffic(kernel, workload):
+    """dram bytes per particle for `kernel` from the committed ncu summary
+    (profiles/*.md lines 'TRAFFIC <kernel> <workload> <bytes per particle>')."""
+    pdir = os.path.join(REPO, "profiles")
+    if not os.path.isdir(pdir):
+        return None
+    for fn in sorted(os.listdir(pdir)):
+        if not fn.endswith((".md", ".txt")):
+            continue
+        for line in open(os.path.join(pdir, fn)):
+            m = re.match(r"\s*TRAFFIC\s+(\S+)\s+(\S+)\s+([0-9.eE+-]+)", line)
+            if m and m.group(1) == kernel and m.group(2) == workload:
+                return float(m.group(3))
+    return None
+
+
+class Clocks:
+    """nvidia-smi sampling of SM clocks and throttle reasons during a region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu):
+        self.gpu = gpu
+        self.p = None
+        self.path = os.path.join("/tmp", "agimp_clocks_%d_%d.csv" % (os.getpid(), gpu))
+
+    def __enter__(self):
+        try:
+            self.f = open(self.path, "w")
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.Q,
+                                       "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                                      stderr=subprocess.DEVNULL)
+            time.sleep(0.3)
+        except Exception:
+            self.p = None
+        return self
+
+    def __exit__(self, *a):
+        if self.p:
+            self.p.terminate()
+            try:
+                self.p.wait(5)
+            except Exception:
+                self.p.kill()
+            self.f.close()
+
+    def summary(self):
+        if not self.p:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            f = [t.strip() for t in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx.append(float(f[2]))
+            except ValueError:
+                continue
+            for nm, val in zip(names, f[5:9]):
+                if val.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def refine_kernels(scene):
+    kmax = min(scene.refine_band * ((1 << (scene.level - 1)) - 1) + 1, 250)
+    return 5 + (kmax - 1)
+
+
+def run_steps(sim, scene, first, count, stream=None):
+    for i in range(first, first + count):
+        if scene.refine_every and i % scene.refine_every == 0:
+            sim.refine_levels(scene.refine_band, stream=stream)
+        sim.substep(scene.dt, stream=stream)
+
+
+def cpu_oracle_run(scene, seconds, threads, steps_cap=None, warmup=1):
+    """Time the oracle (OpenMP, `threads` threads) on the full scene; returns
+    (particle-substeps/s, substeps timed, seconds)."""
+    import numpy as np
+
+    import oracle as O
+    from agimp.simulator import tabulate_level_map
+    d, n = scene.dim, scene.n
+    kw = {}
+    sk = scene.sim_kwargs
+    if "gravity" in sk:
+        kw["gravity"] = tuple(sk["gravity"]) + (0.0,) * (3 - len(sk["gravity"]))
+    for k in ("E", "nu", "theta_c", "theta_s", "hardening"):
+        if k in sk:
+            kw[k] = sk[k]
+    kw["boundary_mode"] = {"ref_slip": 0, "sticky": 1}[sk.get("boundary_mode", "ref_slip")]
+    kw["plasticity"] = {None: 0, "snow": 1}[sk.get("plasticity")]
+    kw["colliders"] = tuple(sk.get("colliders", ()))
+    o = O.Oracle(d, scene.level, scene.coarsest, n, **kw)
+    o.set_particles(scene.x, scene.v, np.tile(np.eye(d), (n, 1, 1)), np.zeros((n, d, d)), scene.m, scene.g)
+    if scene.grid_initializer is not None:
+        t, H = tabulate_level_map(scene.grid_initializer, d, scene.level, scene.coarsest)
+        o.set_level_map(t, H)
+
+    def one(i):
+        if scene.refine_every and i % scene.refine_every == 0:
+            o.refine_levels(scene.refine_band)
+        o.substep(scene.dt, 1, threads)
+
+    for i in range(warmup):
+        one(i)
+    t0 = time.perf_counter()
+    done = 0
+    while True:
+        one(warmup + done)
+        done += 1
+        el = time.perf_counter() - t0
+        if (steps_cap and done >= steps_cap) or el >= seconds:
+            break
+    el = time.perf_counter() - t0
+    return n * done / el, done, el
+
+
+def run_reference(a):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from agimp import scenes
+    scene = scenes.make_config(a.config)
+    threads = os.cpu_count() or 1
+    budget = max(10.0, min(150.0, 2.0 * a.steps))
+    val, done, el = cpu_oracle_run(scene, budget, threads, steps_cap=a.steps, warmup=min(a.warmup, 1))
+    sample = "%s: %d substeps of the full %d-particle scene after %d warm-up, %.1f s" % (
+        scene.name, done, scene.n, min(a.warmup, 1), el)
+    out = {
+        "impl": "reference", "metric": METRIC, "value": val, "unit": METRIC, "n_gpus": a.gpus, "steps": done,
+        "warmup": min(a.warmup, 1), "ms_per_step": 1e3 * el / done, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": scene.name, "particles": scene.n, "levels": scene.level,
+                   "finest": scene.coarsest << (scene.level - 1), "description": scene.description},
+        "cpu_baseline": {"value": val, "unit": METRIC, "cores": threads, "kind": "port", "sample": sample},
+        "e2e": {"value": val, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "note": "the reference is Taichi code and Taichi cannot be installed offline; this arm runs the CPU "
+                "restatement of its algorithm (oracle/oracle.cpp) with OpenMP on all host threads",
+    }
+    print(json.dumps(out))
+
+
+def run_agimp(a):
+    import numpy as np
+    import torch
+
+    from agimp import scenes
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    scene = scenes.make_config(a.config, seed=rank)
+    sim = scene.build(device=local)
+    import ctypes
+    stream = torch.cuda.Stream()
+    st = ctypes.c_void_p(stream.cuda_stream)
+    with torch.cuda.stream(stream):
+        run_steps(sim, scene, 0, a.warmup, st)
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        with Clocks(local) as clk:
+            e0.record(stream)
+            run_steps(sim, scene, a.warmup, a.steps, st)
+            e1.record(stream)
+            torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        ms = e0.elapsed_time(e1)
+        errors = sim.errors()
+        stats = sim.stats()
+        # per-phase timing of single substeps (direct launches, CUDA events)
+        prof = [sim.profile_substep(scene.dt, stream=st) for _ in range(5)]
+    ms_t = torch.tensor([ms], device="cuda")
+    if dist:
+        dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
+    ms_max = float(ms_t.item())
+    value = world * scene.n * a.steps / (ms_max / 1e3)
+    phases = {k: statistics.median(p[k] for p in prof) for k in prof[0]}
+    d = scene.dim
+    jp = scene.sim_kwargs.get("plasticity") == "snow"
+    b_p2g, b_g2p = BYTES[(d, jp)]
+    nb = stats["n_binned"]
+    hbm, src = peaks()
+    dom = "p2g" if phases["p2g"] >= phases["g2p"] else "g2p"
+    dom_bytes = nb * (b_p2g if dom == "p2g" else b_g2p)
+    achieved = dom_bytes / (phases[dom] / 1e3) / 1e9
+    tr = profile_traffic("k_" + dom, scene.name)
+    roof = {"bound": "hbm", "kernel": "k_" + dom, "achieved": achieved, "peak": hbm, "peak_source": src,
+            "unit": "GB/s", "frac": achieved / hbm, "traffic": (tr * nb) if tr is not None else None,
+            "algorithmic_bytes": dom_bytes,
+            "p2g_g2p_combined_frac": (nb * (b_p2g + b_g2p) / ((phases["p2g"] + phases["g2p"]) / 1e3) / 1e9) / hbm}
+    n_refines = sum(1 for i in range(a.warmup, a.warmup + a.steps) if scene.refine_every and i % scene.refine_every == 0)
+    launches = a.steps * sim.kernels_per_substep() + n_refines * refine_kernels(scene)
+    out = {
+        "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
+        "ms_per_step": ms_max / a.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic",
+        "config": {"workload": scene.name, "particles": scene.n, "levels": scene.level,
+                   "finest": scene.coarsest << (scene.level - 1), "dt": scene.dt,
+                   "refine_every": scene.refine_every, "parallelism": "replicas" if world > 1 else "single",
+                   "l2": "inputs exceed L2 (particle state %.0f MB)" % (scene.n * (4 * (2 * d + 2 * d * d + 2)) / 1e6),
+                   "description": scene.description},
+        "roofline": roof,
+        "phases_ms": phases,
+        "gpu_launches": launches,
+        "clocks": clk.summary(),
+        "device_errors": errors,
+    }
+    if not a.no_e2e:
+        out["e2e"] = e2e_run(a, scene, local)
+    if rank == 0 and world == 1 and not a.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        val, done, el = cpu_oracle_run(scene, a.cpu_seconds, threads)
+        out["cpu_baseline"] = {"value": val, "unit": METRIC, "cores": threads, "kind": "port",
+                               "sample": "%s: %d substeps of the full %d-particle scene after 1 warm-up, %.1f s, "
+                                         "OpenMP" % (scene.name, done, scene.n, el)}
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    sim.close()
+    if rank == 0:
+        print(json.dumps(out))
+
+
+def e2e_run(a, scene, local):
+    """Same metric through the public API with host buffers: upload the scene
+    from pinned host memory, then per substep call substep() and read x_p back
+    into pinned host memory."""
+    import numpy as np
+    import torch
+    n, d = scene.n, scene.dim
+
+    def pinned(shape, dt=torch.float32):
+        return torch.empty(shape, dtype=dt, pin_memory=True).numpy()
+
+    hx, hv, hF, hC, hm, hg, hJ = (pinned((n, d)), pinned((n, d)), pinned((n, d, d)), pinned((n, d, d)), pinned((n,)),
+                                  pinned((n,), torch.int32), pinned((n,)))
+    hx[:] = scene.x
+    hv[:] = scene.v
+    hF[:] = np.eye(d, dtype=np.float32)
+    hC[:] = 0
+    hm[:] = scene.m
+    hg[:] = scene.g
+    hJ[:] = 1
+    out = pinned((n, d))
+    sim = scene.build(device=local)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    sim.set_particles(x=hx, v=hv, F=hF, C=hC, m=hm, g=hg, Jp=hJ)
+    for i in range(a.steps):
+        if scene.refine_every and i % scene.refine_every == 0:
+            sim.refine_levels(scene.refine_band)
+        sim.substep(scene.dt)
+        sim.x_p.to_numpy(out=out)
+    torch.cuda.synchronize()
+    el = time.perf_counter() - t0
+    sim.close()
+    h2d = n * 4 * (2 * d + 2 * d * d + 3)
+    return {"value": n * a.steps / el, "unit": METRIC, "h2d_bytes_per_step": h2d / a.steps,
+            "d2h_bytes_per_step": n * d * 4, "timing": "wall clock, host-synchronous readback every substep",
+            "note": "h2d is the one-time upload of the scene state spread over the timed substeps"}
+
+
+def main():
+    a = parse()
+    if a.impl == "reference":
+        run_reference(a)
+    else:
+        run_agimp(a)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,172 @@
+/*
+ * agimp.h -- C ABI of the B200 adaptive GIMP substep library (libagimp.so).
+ *
+ * The reference project (g1n0st/adaptive-gimp) exposes this path as the Python
+ * class AdaptiveGIMP (adaptive_gimp.py:4-352).  Each entry point below names
+ * the part of that interface it replaces.  The Python facade in
+ * adaptive-gimp_b200/agimp/simulator.py binds these functions with ctypes and
+ * mirrors the reference's constructor, fields and substep().
+ *
+ * Conventions
+ *  - Plain pointers and sizes only.  `stream` is a cudaStream_t (NULL = legacy
+ *    default stream).  Every call is ordered on `stream`; calls that return
+ *    data into HOST memory synchronize `stream` before returning.
+ *  - `memory` says where caller buffers live: AGIMP_MEM_DEVICE (device
+ *    pointers on the simulator's device) or AGIMP_MEM_HOST (host pointers,
+ *    pinned or pageable).
+ *  - Particle arrays use the reference's field layout (Taichi to_numpy):
+ *    vectors [N][dim], matrices [N][dim][dim] row-major, f32.
+ *  - Grid readback is a dense box of indices [lo, lo+n) per axis, first axis
+ *    slowest (the reference's ti.ij / ti.ijk order).  The library stores every
+ *    level over indices [-4, size+8); readback outside reads 0.
+ *  - The library owns all of its device memory (allocated in agimp_create,
+ *    freed in agimp_destroy).  A handle is not thread-safe; distinct handles are
+ *    independent.
+ *  - Status codes are returned, never raised.  agimp_last_error() gives a
+ *    message for the last failing call on a handle.
+ */
+#ifndef AGIMP_H
+#define AGIMP_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define AGIMP_ABI_VERSION 1
+
+typedef enum {
+  AGIMP_OK = 0,
+  AGIMP_INVALID_ARG = 1,
+  AGIMP_CAPACITY = 2,
+  AGIMP_NAN = 3,
+  AGIMP_DEVICE_TIMEOUT = 4,
+  AGIMP_CUDA_ERROR = 5,
+  AGIMP_NOT_READY = 6,
+  AGIMP_OUT_OF_MEMORY = 7
+} agimp_status;
+
+enum { AGIMP_MEM_DEVICE = 0, AGIMP_MEM_HOST = 1 };
+
+/* Device error word bits (agimp_errors).  The library records these instead of
+ * faulting; each names a condition the reference leaves undefined. */
+#define AGIMP_ERR_OOB 1u      /* an index left the stored lattice; access skipped */
+#define AGIMP_ERR_ESCAPED 2u  /* a particle left [0,1)^dim; it is frozen (fl_p = -1) */
+#define AGIMP_ERR_MAP_OOB 4u  /* a level-map lookup left the table */
+#define AGIMP_ERR_NOBIN 8u    /* a particle's bin block was not active (internal) */
+
+/* Mask flags, utils.py:5-9. */
+#define AGIMP_ACTIVATED 1
+#define AGIMP_GHOST 2
+#define AGIMP_T_JUNCTION 4
+
+/* Simulator parameters.  agimp_default_params() fills the reference's
+ * constants (adaptive_gimp.py:17-18, 48-53): radius 0.5 cells, gravity
+ * (0,-100,0), E 5e3, nu 0.2, boundary_gap 4 finest cells, per-axis wall clamp,
+ * no plasticity, no colliders. */
+typedef struct agimp_params {
+  int32_t dim;            /* 2 or 3 (adaptive_gimp.py:12) */
+  int32_t level;          /* number of levels L, 1..8 (adaptive_gimp.py:14) */
+  int32_t coarsest_size;  /* power of two >= 4 (adaptive_gimp.py:15) */
+  int32_t boundary_gap;   /* finest cells (adaptive_gimp.py:18) */
+  int32_t boundary_mode;  /* 0: per-axis normal clamp (adaptive_gimp.py:284-287); 1: sticky walls */
+  int32_t plasticity;     /* 0: none (reference); 1: snow (Stomakhin et al. 2013), extension */
+  int64_t n_particles;    /* adaptive_gimp.py:51 */
+  double radius;          /* GIMP half-width in cells (adaptive_gimp.py:48) */
+  double gravity[3];      /* adaptive_gimp.py:50 */
+  double E, nu;           /* adaptive_gimp.py:52-53 */
+  double theta_c, theta_s, hardening; /* snow parameters (extension) */
+  int32_t n_colliders;    /* sticky box colliders, extension, <= 4 */
+  double colliders[4][6]; /* lo[3], hi[3] in domain units */
+} agimp_params;
+
+typedef struct agimp_stats {
+  int32_t active_blocks[8]; /* 4^dim-cell blocks visited per level in the last substep */
+  int32_t n_binned;         /* particles with fl_p >= 0 in the last substep */
+  int32_t n_chunks;         /* P2G/G2P work items in the last substep */
+  int64_t substeps;         /* substeps run since creation */
+} agimp_stats;
+
+typedef struct agimp_sim agimp_sim;
+
+int agimp_abi_version(void);
+const char* agimp_status_string(agimp_status s);
+
+/* Reference constants for (dim, level, coarsest_size, n_particles). */
+void agimp_default_params(agimp_params* p, int32_t dim, int32_t level, int32_t coarsest_size, int64_t n_particles);
+
+/* Replaces AdaptiveGIMP.__init__ storage and constants (adaptive_gimp.py:6-62).
+ * Allocates every device buffer for the dense blocked lattices of all levels
+ * and the particle arrays; nothing is allocated afterwards. */
+agimp_status agimp_create(const agimp_params* p, int32_t device, agimp_sim** out);
+agimp_status agimp_destroy(agimp_sim* s);
+const char* agimp_last_error(const agimp_sim* s);
+
+/* Replaces the particle_initializer hook (adaptive_gimp.py:64, init.py:3-32):
+ * writes x_p, v_p, F_p, C_p, m_p, g_p (adaptive_gimp.py:55-61) and, with snow
+ * plasticity, Jp (NULL = 1).  Any array may be NULL to leave it unchanged. */
+agimp_status agimp_set_particles(agimp_sim* s, const float* x, const float* v, const float* F, const float* C,
+                                 const float* m, const int32_t* g, const float* Jp, int32_t memory, void* stream);
+
+/* Field readback of x_p, v_p, F_p, C_p, m_p, g_p, fl_p (adaptive_gimp.py:55-62)
+ * and Jp.  NULL outputs are skipped. */
+agimp_status agimp_get_particles(agimp_sim* s, float* x, float* v, float* F, float* C, float* m, int32_t* g,
+                                 int32_t* fl, float* Jp, int32_t memory, void* stream);
+
+/* Replaces the grid_initializer hook and static adaptivity
+ * (adaptive_gimp.py:65-66, 72-85; init.py:34-98).  `table` tabulates the
+ * initializer over finest cells [-halo, finest+halo)^dim, first axis slowest:
+ * low 4 bits = the level it returns; bit 6 set = it activates nothing (else it
+ * activates the cell of that level containing the finest cell).
+ * halo must be >= max(2, 2^(level-1)).  Selecting a map switches the substep
+ * to static activation; agimp_clear_level_map() switches back to dynamic
+ * activation from g_p (adaptive_gimp.py:87-96). */
+agimp_status agimp_set_level_map(agimp_sim* s, const int8_t* table, int32_t halo, int32_t memory, void* stream);
+agimp_status agimp_clear_level_map(agimp_sim* s);
+
+/* Replaces AdaptiveGIMP.substep(dt0) (adaptive_gimp.py:323-352), run n_steps
+ * times back to back.  Asynchronous on `stream`.  With graphs enabled (the
+ * default) the substep is captured once per (dt, stream) as a CUDA graph and
+ * replayed. */
+agimp_status agimp_substep(agimp_sim* s, float dt, int32_t n_steps, void* stream);
+agimp_status agimp_set_graphs(agimp_sim* s, int32_t enable);
+
+/* Extension with no counterpart in the reference (which fixes g_p once, in
+ * init.py:17-29 / run_3d.py:151-156): recompute g_p from the current positions.
+ * A particle whose finest cell is within `band` finest cells (Chebyshev) of an
+ * empty finest cell gets the finest level, within band*3 the next coarser,
+ * band*7 the next, ..., deeper particles level 0. */
+agimp_status agimp_refine_levels(agimp_sim* s, int32_t band, void* stream);
+
+/* Readback of cell_mask[l], ad_grid_m[l], ad_grid_v[l] (adaptive_gimp.py:35-42)
+ * as they stand after the last substep, over indices [lo, lo+n)^dim.  v is
+ * [n^dim][dim].  NULL outputs are skipped. */
+agimp_status agimp_get_grid(agimp_sim* s, int32_t level, int32_t lo, int32_t n, float* m, float* v, int32_t* cell_mask,
+                            int32_t memory, void* stream);
+
+/* Readback of node_mask over the finest lattice [0, finest]^dim
+ * (adaptive_gimp.py:23-26); the predicates of adaptive_gimp.py:126-140 apply
+ * to it unchanged. */
+agimp_status agimp_get_node_mask(agimp_sim* s, int32_t* out, int32_t memory, void* stream);
+
+/* Device error word (AGIMP_ERR_*) accumulated since the last clear.
+ * Synchronizes the device. */
+agimp_status agimp_errors(agimp_sim* s, uint32_t* bits, int32_t clear);
+agimp_status agimp_get_stats(agimp_sim* s, agimp_stats* out);
+
+/* Number of kernels one substep launches (for launch accounting). */
+int32_t agimp_kernels_per_substep(const agimp_sim* s);
+
+/* One substep with direct launches and CUDA events between its phases;
+ * writes 8 durations in ms: active blocks, topology, binning, P2G,
+ * restriction, grid_op, prolongation, G2P.  Synchronizes the stream.  The
+ * reference's closest counterpart is the Taichi kernel profiler
+ * (run_3d.py:12, 43). */
+agimp_status agimp_profile_substep(agimp_sim* s, float dt, float* ms, int32_t n, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* AGIMP_H */
