@@ -167,8 +167,22 @@ class Scene:
         return AdaptiveGIMP(d, self.level, self.coarsest, n, pinit, self.grid_initializer, **kw)
 
 
-def _mass(rho, finest, dim, ppc):
-    return np.float32(rho * (1.0 / finest) ** dim / ppc)
+# Units.  The reference's P2G stress term carries no particle volume
+# (adaptive_gimp.py:240, i.e. V_p = 1) and its particle mass is p_mass = 1
+# (adaptive_gimp.py:49): the density is 1 and only E/rho enters the dynamics.
+# The scenes keep that convention (m_p = 1) and pass E/rho as the modulus, so
+# the wave speed sqrt(E/rho) is the configuration's.  The configurations'
+# (E, dt) with rho = 1 violate the explicit CFL limit (sqrt(E/rho) dt/dx > 1),
+# so each uses a density that keeps the CFL number near 0.3: 100 for config 1,
+# 400 (snow, Stomakhin et al. 2013) for configs 3 and 5, 1000 for config 2.
+# Scaling the mass instead would break the reference's scheme: invalid odd
+# nodes keep raw P2G momentum through G2P (adaptive_gimp.py:281 converts only
+# activated nodes), which stays of the order of a velocity only when m_p = 1.
+RHO = {1: 100.0, 2: 1000.0, 3: 400.0, 5: 400.0}
+
+
+def _unit_mass(n):
+    return np.ones(n, np.float32)
 
 
 def make_config(k, seed=0, scale=1.0):
@@ -183,10 +197,10 @@ def make_config(k, seed=0, scale=1.0):
         x = np.concatenate(xs)
         n = len(x)
         return Scene("config1_2d_static", 2, L, c, x, np.zeros((n, 2), np.float32), np.full(n, L - 1, np.int32),
-                     np.full(n, _mass(1.0, fin, 2, 4)), 1e-4, 1000,
-                     dict(E=1e4, nu=0.2, gravity=(0.0, -9.8), boundary_mode="sticky"),
+                     _unit_mass(n), 1e-4, 1000,
+                     dict(E=1e4 / RHO[1], nu=0.2, gravity=(0.0, -9.8), boundary_mode="sticky"),
                      grid_initializer=band_level_map(boxes, 2, L, c),
-                     description="2D static 3-level quadtree 64^2..256^2, two elastic boxes 0.2x0.2, 4 ppc")
+                     description="2D static 3-level quadtree 64^2..256^2, two elastic boxes 0.2x0.2, 4 ppc, E=1e4 rho=100")
     if k == 2:
         L, c = 4, 64
         fin = c << (L - 1)
@@ -200,11 +214,11 @@ def make_config(k, seed=0, scale=1.0):
         x, v = np.concatenate(xs), np.concatenate(vs)
         n = len(x)
         return Scene("config2_2d_dynamic", 2, L, c, x, v, np.full(n, L - 1, np.int32),
-                     np.full(n, _mass(1.0, fin, 2, 4)), 5e-5, 2000,
-                     dict(E=1.4e5, nu=0.2, gravity=(0.0, -9.8), boundary_mode="sticky", plasticity="snow",
+                     _unit_mass(n), 5e-5, 2000,
+                     dict(E=1.4e5 / RHO[2], nu=0.2, gravity=(0.0, -9.8), boundary_mode="sticky", plasticity="snow",
                           theta_c=2.5e-2, theta_s=7.5e-3, hardening=10.0),
                      refine_every=10, refine_band=3,
-                     description="2D dynamic 4 levels 64^2..512^2, 3 random snow boxes, 4 ppc, re-refined every 10")
+                     description="2D dynamic 4 levels 64^2..512^2, 3 random snow boxes, 4 ppc, E=1.4e5 rho=1000, re-refined every 10")
     if k == 3:
         L, c = 3, 64
         fin = c << (L - 1)
@@ -214,12 +228,12 @@ def make_config(k, seed=0, scale=1.0):
         v = np.tile(np.array([0.0, -3.0, 0.0], np.float32), (n, 1))
         slab = (0.3, 0.2, 0.3, 0.7, 0.3, 0.7)
         return Scene("config3_3d_dynamic", 3, L, c, x, v, np.full(n, L - 1, np.int32),
-                     np.full(n, _mass(1.0, fin, 3, 8)), 5e-5, 1000,
-                     dict(E=1e5, nu=0.25, gravity=(0.0, -9.8, 0.0), boundary_mode="sticky", plasticity="snow",
+                     _unit_mass(n), 5e-5, 1000,
+                     dict(E=1e5 / RHO[3], nu=0.25, gravity=(0.0, -9.8, 0.0), boundary_mode="sticky", plasticity="snow",
                           theta_c=2.5e-2, theta_s=7.5e-3, hardening=10.0, colliders=(slab,)),
                      refine_every=10, refine_band=3,
                      description="3D dynamic 3 levels 64^3..256^3, snow sphere r=0.15 at y=0.6 moving down at 3 "
-                                 "onto a 0.4x0.1x0.4 static slab collider, 8 ppc")
+                                 "onto a 0.4x0.1x0.4 static slab collider, 8 ppc, E=1e5 rho=400, re-refined every 10")
     if k == 5:
         L, c = 4, 64
         fin = c << (L - 1)
@@ -231,8 +245,8 @@ def make_config(k, seed=0, scale=1.0):
                             np.tile(np.array([-2.0, 0, 0], np.float32), (len(b), 1))])
         n = len(x)
         return Scene("config5_3d_two_spheres", 3, L, c, x, v, np.full(n, L - 1, np.int32),
-                     np.full(n, _mass(1.0, fin, 3, 8)), 3e-5, 1000,
-                     dict(E=1.4e5, nu=0.2, gravity=(0.0, -9.8, 0.0), boundary_mode="sticky", plasticity="snow"),
+                     _unit_mass(n), 3e-5, 1000,
+                     dict(E=1.4e5 / RHO[5], nu=0.2, gravity=(0.0, -9.8, 0.0), boundary_mode="sticky", plasticity="snow"),
                      refine_every=10, refine_band=3,
-                     description="3D 4 levels 64^3..512^3, two colliding snow spheres r=0.12 at +-2")
+                     description="3D 4 levels 64^3..512^3, two colliding snow spheres r=0.12 at +-2, E=1.4e5 rho=400")
     raise ValueError("unknown config %r" % k)

@@ -173,20 +173,40 @@ __global__ void k_touch_activate(Ctx c) {
 }
 
 // ---------------------------------------------------------------------------
-// Active-block lists: every level gets the blocks within one block of each
-// touched finest block (shifted to that level).
+// Active-block lists: level l gets the blocks within R_l blocks of each
+// touched finest block (shifted to that level).  Dynamic activation, culling,
+// ghost/T marking and the transfers stay within 2 cells of a particle at every
+// level, so R_l = 1.  A static level-map lookup (adaptive_gimp.py:82-85) can
+// land up to two cells of the particle's own level away, i.e. up to 2^L finest
+// cells, and activate a cell of any level there; with the ghost / T /
+// corner reach on top, level l then needs ceil((2^(l+1) + 6) / 4) blocks.
+__device__ __forceinline__ int dilate_radius(const Ctx& c, int l) {
+  return c.is_static ? ((1 << (l + 1)) + 9) / 4 : 1;
+}
+
 template <int D>
 __global__ void k_dilate(Ctx c) {
-  constexpr int NB3 = (D == 2) ? 9 : 27;
-  const long long tot = (long long)c.ctr[CTR_TOUCH] * c.L * NB3;
+  int per_level[MAXL];
+  long long W = 0;
+  for (int l = 0; l < c.L; ++l) {
+    const int w = 2 * dilate_radius(c, l) + 1;
+    per_level[l] = (D == 2) ? w * w : w * w * w;
+    W += per_level[l];
+  }
+  const long long tot = (long long)c.ctr[CTR_TOUCH] * W;
   const LevelDev& Vf = c.lev[c.L - 1];
   GS_LOOP(e, tot) {
-    const int nbi = (int)(e % NB3);
-    const long long r = e / NB3;
-    const int l = (int)(r % c.L);
-    const int t = (int)(r / c.L);
+    const int t = (int)(e / W);
+    int r = (int)(e % W);
+    int l = 0;
+    while (l < c.L - 1 && r >= per_level[l]) {
+      r -= per_level[l];
+      ++l;
+    }
+    const int R = dilate_radius(c, l);
+    const int w = 2 * R + 1;
     const int key = c.touch_list[t];
-    if (l == c.L - 1 && nbi == NB3 / 2) c.touch_flag[key] = 0u;
+    if (l == c.L - 1 && r == per_level[l] / 2) c.touch_flag[key] = 0u;
     int fb[D];
     long long k = key;
 #pragma unroll
@@ -197,11 +217,11 @@ __global__ void k_dilate(Ctx c) {
     const LevelDev& V = c.lev[l];
     const int s = c.L - 1 - l;
     int dl[D];
-    int tt = nbi;
+    int tt = r;
 #pragma unroll
     for (int d = D - 1; d >= 0; --d) {
-      dl[d] = tt % 3 - 1;
-      tt /= 3;
+      dl[d] = tt % w - R;
+      tt /= w;
     }
     long long b = 0;
     bool ok = true;
@@ -211,10 +231,7 @@ __global__ void k_dilate(Ctx c) {
       ok = ok && cb >= 0 && cb < V.nb;
       b = b * V.nb + cb;
     }
-    if (!ok) {
-      set_err(c, ERR_OOB);
-      continue;
-    }
+    if (!ok) continue;  // beyond the stored lattice: nothing can be written there
     int* bm = &V.bmap[b];
     if (*bm == -1 && atomicCAS(bm, -1, -2) == -1) {
       const int i = atomicAdd(&c.ctr[CTR_LEVEL + l], 1);
