@@ -25,7 +25,7 @@ EXPORTS = (
     "agimp_last_error", "agimp_set_particles", "agimp_get_particles", "agimp_set_level_map",
     "agimp_clear_level_map", "agimp_substep", "agimp_set_graphs", "agimp_refine_levels", "agimp_get_grid",
     "agimp_get_node_mask", "agimp_errors", "agimp_get_stats", "agimp_kernels_per_substep",
-    "agimp_profile_substep",
+    "agimp_profile_substep", "agimp_refine_levels_noalloc",
 )
 PHASES = ("blocks", "topology", "binning", "p2g", "restrict", "gridop", "prolong", "g2p")
 
@@ -87,6 +87,8 @@ def load(path: str | None = None):
     L.agimp_kernels_per_substep.argtypes = [vp]
     L.agimp_kernels_per_substep.restype = ctypes.c_int32
     L.agimp_profile_substep.argtypes = [vp, ctypes.c_float, fp, ctypes.c_int32, vp]
+    L.agimp_refine_levels_noalloc.argtypes = [vp, ctypes.c_int64, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
+                                              ctypes.c_int32, vp, vp]
     _lib = L
     return L
 

@@ -52,6 +52,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="agimp", choices=["agimp", "reference"])
     ap.add_argument("--config", type=int, default=3)
+    ap.add_argument("--scale", type=float, default=1.0, help="body scale of the scene (profiling cases)")
     ap.add_argument("--cpu-seconds", type=float, default=20.0, help="budget of the CPU baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
@@ -197,7 +198,7 @@ def run_reference(a):
     if rank != 0:
         return
     from agimp import scenes
-    scene = scenes.make_config(a.config)
+    scene = scenes.make_config(a.config, scale=a.scale)
     threads = os.cpu_count() or 1
     budget = max(10.0, min(150.0, 2.0 * a.steps))
     val, done, el = cpu_oracle_run(scene, budget, threads, steps_cap=a.steps, warmup=min(a.warmup, 1))
@@ -232,7 +233,7 @@ def run_agimp(a):
 
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
-    scene = scenes.make_config(a.config, seed=rank)
+    scene = scenes.make_config(a.config, seed=rank, scale=a.scale)
     sim = scene.build(device=local)
     import ctypes
     stream = torch.cuda.Stream()

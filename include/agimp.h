@@ -165,6 +165,22 @@ int32_t agimp_kernels_per_substep(const agimp_sim* s);
  * (run_3d.py:12, 43). */
 agimp_status agimp_profile_substep(agimp_sim* s, float dt, float* ms, int32_t n, void* stream);
 
+/* No counterpart in the reference.  The refinement rule of
+ * agimp_refine_levels for callers that cannot allocate device memory (a host
+ * whose own arena or pool owns the device memory, so a library cudaMalloc
+ * would fail or bypass its accounting, or a loop that cannot take the
+ * synchronisation cudaMalloc/cudaFree may imply).  It takes no handle and
+ * allocates nothing: x [n][dim] f32 and g [n] i32 are caller device buffers,
+ * and its scratch is a static 16 MiB device array inside libagimp.so, held by
+ * every GPU that loads the library until exit, which limits it to
+ * finest^dim <= 16,777,216 cells (3D 256^3, 2D 4096^2); larger grids return
+ * AGIMP_CAPACITY.  The first call on a device looks up the array's device
+ * address with that device current; make that first call before any stream
+ * capture.  All calls share the array: calls that overlap on the GPU race.
+ * Asynchronous on `stream`. */
+agimp_status agimp_refine_levels_noalloc(const float* x, int64_t n, int32_t dim, int32_t level, int32_t coarsest_size,
+                                         int32_t band, int32_t* g, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
