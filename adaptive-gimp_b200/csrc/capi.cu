@@ -217,6 +217,7 @@ agimp_status agimp_create(const agimp_params* p, int32_t device, agimp_sim** out
   int sms = 148;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
   c.sms = sms;
+  prepare_transfer_kernels();
   c.gap = p->boundary_gap;
   c.bmode = p->boundary_mode;
   c.plast = p->plasticity;

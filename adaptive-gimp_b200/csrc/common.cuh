@@ -397,6 +397,7 @@ __device__ __forceinline__ void polar_rot(const float* F, float* R) {
 constexpr int PHASES = 8;  // blocks, topology, binning, p2g, restrict, gridop, prolong, g2p
 void launch_substep(const Ctx& c, cudaStream_t s, cudaEvent_t* ev = nullptr);
 void launch_refine(const Ctx& c, int band, cudaStream_t s);
+void prepare_transfer_kernels();  // kernel attributes (shared-memory opt-in); once per device
 int kernels_per_substep(const Ctx& c);
 
 }  // namespace agimp

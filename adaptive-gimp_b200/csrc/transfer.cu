@@ -89,23 +89,80 @@ __device__ __forceinline__ void chunk_origin(const LevelDev& V, long long blk, i
 }
 
 // ---------------------------------------------------------------------------
+// P2G (adaptive_gimp.py:230-250).  Per work item (up to CHUNK particles of one
+// 4^d block of one level):
+//  1. one thread per particle computes the scaled stress (utils.py:11-16,
+//     adaptive_gimp.py:240), its per-axis GIMP weights and gradients, m,
+//     a = m (v - C (tc+1)) and B = m C, and its base cell inside the block,
+//     and stores them in shared memory;
+//  2. the particles are counting-sorted by base cell in shared memory and cut
+//     into tasks of <= 32 particles of one cell;
+//  3. a warp takes a task with one lane per stencil node (3^d lanes; in 2D
+//     three lane groups take every third particle): all particles of a base
+//     cell touch the same nodes, so each lane sums its node's mass and
+//     momentum, w m and w (a + B n) + S grad w, over the task in registers;
+//  4. each lane adds its sums once into the (4+2)^d node tile in shared
+//     memory; the tile is flushed with one float4 atomic per touched node.
+// Shared-memory atomics from different lanes of a warp never hit the same
+// node, which removes the serialisation of a per-particle scatter when many
+// particles share a cell (hundreds per cell on coarse levels).
+template <int D>
+struct P2GLayout {
+  static constexpr int NC = 1 << (2 * D);      // cells per block
+  static constexpr int G3 = (D == 2) ? 9 : 27;  // stencil nodes
+  static constexpr int NGROUP = 32 / G3;        // lane groups per warp
+  static constexpr int TN = (D == 2) ? 36 : 216;
+  static constexpr int OFF_W = 0;               // W[d][3]
+  static constexpr int OFF_G = 3 * D;           // G[d][3]
+  static constexpr int OFF_M = 6 * D;           // m
+  static constexpr int OFF_A = OFF_M + 1;       // a[d]
+  static constexpr int OFF_B = OFF_A + D;       // B[d][d]
+  static constexpr int OFF_S = OFF_B + D * D;   // S[d][d]
+  static constexpr int NF = OFF_S + D * D;
+  static constexpr int STRIDE = NF | 1;         // odd: conflict-free per-particle columns
+  static constexpr int MAXTASK = NC + CHUNK / 32;
+  static constexpr size_t bytes() {
+    return sizeof(float) * ((size_t)CHUNK * STRIDE + 4 * TN) +
+           sizeof(int) * (3 * NC + 2 * CHUNK + 3 * MAXTASK + 4);
+  }
+};
+
 template <int D>
 __global__ void __launch_bounds__(CHUNK) k_p2g(Ctx c) {
-  constexpr int TN = (D == 2) ? 36 : 216;  // (4+2)^d node tile
-  __shared__ float sm[4][TN];
+  using Y = P2GLayout<D>;
+  extern __shared__ float dsm[];
+  float* pd = dsm;                              // [CHUNK][STRIDE]
+  float* tile = pd + CHUNK * Y::STRIDE;         // [4][TN]: p_x, p_y, p_z, m
+  int* s_cnt = (int*)(tile + 4 * Y::TN);        // [NC]
+  int* s_off = s_cnt + Y::NC;                   // [NC]
+  int* s_tpre = s_off + Y::NC;                  // [NC]
+  int* s_sorted = s_tpre + Y::NC;               // [CHUNK]
+  int* s_unused = s_sorted + CHUNK;             // [CHUNK] (keeps the layout of bytes())
+  int* t_cell = s_unused + CHUNK;               // [MAXTASK]
+  int* t_start = t_cell + Y::MAXTASK;
+  int* t_len = t_start + Y::MAXTASK;
+  int* s_ntask = t_len + Y::MAXTASK;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
   const int nch = c.ctr[CTR_CHUNKS];
-  const float pw = (D == 2) ? 0.25f : 0.125f;                                  // 0.5**dim
+  const float pw = (D == 2) ? 0.25f : 0.125f;                                        // 0.5**dim
   const float rd = (D == 2) ? c.radius * c.radius : c.radius * c.radius * c.radius;  // radius**dim
+  const float r2 = 2.f * c.radius;
+  const float kw = (D == 2) ? 1.f / (4.f * r2 * r2) : 1.f / (8.f * r2 * r2 * r2);
+  const float kg = (D == 2) ? 1.f / (2.f * r2 * r2) : 1.f / (4.f * r2 * r2 * r2);
   for (int ch = blockIdx.x; ch < nch; ch += gridDim.x) {
     const int4 wd = c.chunks[ch];
     const int l = wd.x;
     const LevelDev& V = c.lev[l];
-    for (int i = threadIdx.x; i < 4 * TN; i += blockDim.x) (&sm[0][0])[i] = 0.f;
+    for (int i = threadIdx.x; i < 4 * Y::TN; i += blockDim.x) tile[i] = 0.f;
+    for (int i = threadIdx.x; i < Y::NC; i += blockDim.x) s_cnt[i] = 0;
     int O[D];
     chunk_origin<D>(V, wd.y, O);
     __syncthreads();
-    if ((int)threadIdx.x < wd.w) {
-      const int p = c.perm[wd.z + threadIdx.x];
+    // -- 1. per-particle quantities ------------------------------------------
+    const int i = threadIdx.x;
+    int cell = -1;
+    if (i < wd.w) {
+      const int p = c.perm[wd.z + i];
       const long long N = c.N;
       const float inv = (float)(c.coarsest << l);
       const float dx = 1.f / inv;
@@ -116,20 +173,20 @@ __global__ void __launch_bounds__(CHUNK) k_p2g(Ctx c) {
         vp[d] = c.v[d * N + p];
       }
 #pragma unroll
-      for (int i = 0; i < D * D; ++i) {
-        F[i] = c.F[i * N + p];
-        Cm[i] = c.C[i * N + p];
+      for (int k = 0; k < D * D; ++k) {
+        F[k] = c.F[k * N + p];
+        Cm[k] = c.C[k * N + p];
       }
       const float mp = c.m[p];
-      int base[D];
       float tc[D];
+      cell = 0;
 #pragma unroll
       for (int d = 0; d < D; ++d) {
         const float xs = xp[d] * inv;
-        base[d] = (int)(xs + 0.5f) - 1;
-        tc[d] = xs - (float)(base[d] + 1);
+        const int base = (int)(xs + 0.5f) - 1;
+        tc[d] = xs - (float)(base + 1);
+        cell = (cell << 2) | ((base - O[d]) & 3);
       }
-      // get_stress (utils.py:11-16), scaled as in adaptive_gimp.py:240
       float mu = c.mu, la = c.la;
       if (c.plast == 1) {
         const float h = expf(c.xi * (1.f - c.Jp[p]));
@@ -142,55 +199,155 @@ __global__ void __launch_bounds__(CHUNK) k_p2g(Ctx c) {
       const float tmu = 2.f * mu;
       const float diag = la * J * (J - 1.f);
       const float sc = (-c.dt * pw) / (rd * dx);
-      float S[D * D];
+      float* P = pd + i * Y::STRIDE;
 #pragma unroll
-      for (int i = 0; i < D; ++i)
+      for (int a = 0; a < D; ++a)
 #pragma unroll
-        for (int j = 0; j < D; ++j) {
-          float a = 0.f;
+        for (int b = 0; b < D; ++b) {
+          float s = 0.f;
 #pragma unroll
-          for (int k = 0; k < D; ++k) a += (tmu * (F[i * D + k] - Rm[i * D + k])) * F[j * D + k];
-          S[i * D + j] = sc * (a + (i == j ? diag : 0.f));
+          for (int k = 0; k < D; ++k) s += (tmu * (F[a * D + k] - Rm[a * D + k])) * F[b * D + k];
+          P[Y::OFF_S + a * D + b] = sc * (s + (a == b ? diag : 0.f));
         }
-      Stencil<D> st;
-      make_stencil<D>(tc, c.radius, st);
-      int rb[D];
 #pragma unroll
-      for (int d = 0; d < D; ++d) rb[d] = base[d] - O[d];
+      for (int d = 0; d < D; ++d) axis_weights(tc[d], c.radius, P + Y::OFF_W + 3 * d, P + Y::OFF_G + 3 * d);
+      P[Y::OFF_M] = mp;
 #pragma unroll
-      for (int k = 0; k < ((D == 2) ? 9 : 27); ++k) {
-        int n[D];
+      for (int a = 0; a < D; ++a) {
+        float cd = 0.f;
+#pragma unroll
+        for (int b = 0; b < D; ++b) {
+          cd += Cm[a * D + b] * (tc[b] + 1.f);
+          P[Y::OFF_B + a * D + b] = mp * Cm[a * D + b];
+        }
+        P[Y::OFF_A + a] = mp * (vp[a] - cd);
+      }
+    }
+    // rank inside the cell (warp-aggregated shared atomics)
+    int rank = 0;
+    {
+      const unsigned grp = __match_any_sync(0xffffffffu, cell);
+      const int leader = __ffs(grp) - 1;
+      int old = 0;
+      if (cell >= 0 && lane == leader) old = atomicAdd(&s_cnt[cell], __popc(grp));
+      old = __shfl_sync(0xffffffffu, old, leader);
+      rank = old + __popc(grp & ((1u << lane) - 1u));
+    }
+    __syncthreads();
+    // -- 2. cell offsets and tasks (warp 0) ----------------------------------
+    if (warp == 0) {
+      int run_c = 0, run_t = 0;
+      for (int c0 = 0; c0 < Y::NC; c0 += 32) {
+        const int cc = c0 + lane;
+        const int n = cc < Y::NC ? s_cnt[cc] : 0;
+        const int nt = (n + 31) >> 5;
+        int ic = n, it = nt;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+          const int yc = __shfl_up_sync(0xffffffffu, ic, o), yt = __shfl_up_sync(0xffffffffu, it, o);
+          if (lane >= o) {
+            ic += yc;
+            it += yt;
+          }
+        }
+        if (cc < Y::NC) {
+          s_off[cc] = run_c + ic - n;
+          s_tpre[cc] = run_t + it - nt;
+        }
+        run_c += __shfl_sync(0xffffffffu, ic, 31);
+        run_t += __shfl_sync(0xffffffffu, it, 31);
+      }
+      if (lane == 0) *s_ntask = run_t;
+    }
+    __syncthreads();
+    if (cell >= 0) s_sorted[s_off[cell] + rank] = i;
+    for (int cc = threadIdx.x; cc < Y::NC; cc += blockDim.x) {
+      const int n = s_cnt[cc];
+      for (int j = 0, t = s_tpre[cc]; j < n; j += 32, ++t) {
+        t_cell[t] = cc;
+        t_start[t] = s_off[cc] + j;
+        t_len[t] = min(32, n - j);
+      }
+    }
+    __syncthreads();
+    // -- 3. tasks: lane <-> stencil node --------------------------------------
+    {
+      const int ntask = *s_ntask;
+      const int g = lane / Y::G3, k = lane % Y::G3;
+      const bool on = g < Y::NGROUP;
+      int n[D];
+      {
         int t = k;
 #pragma unroll
         for (int d = D - 1; d >= 0; --d) {
           n[d] = t % 3;
           t /= 3;
         }
-        float w, gw[D];
-        node_weight<D>(st, n, w, gw);
-        const float wm = w * mp;
-        float mom[D];
+      }
+      for (int t = warp; t < ntask; t += nwarps) {
+        const int cc = t_cell[t], s0 = t_start[t], len = t_len[t];
+        float am = 0.f, ap[D];
 #pragma unroll
-        for (int i = 0; i < D; ++i) {
-          float cd = 0.f, sg = 0.f;
+        for (int d = 0; d < D; ++d) ap[d] = 0.f;
+        if (on) {
+          for (int j = g; j < len; j += Y::NGROUP) {
+            const float* P = pd + s_sorted[s0 + j] * Y::STRIDE;
+            float w, gw[D];
+            if (D == 2) {
+              const float wx = P[Y::OFF_W + n[0]], wy = P[Y::OFF_W + 3 + n[1]];
+              w = wx * wy * kw;
+              gw[0] = P[Y::OFF_G + n[0]] * wy * kg;
+              gw[1] = wx * P[Y::OFF_G + 3 + n[1]] * kg;
+            } else {
+              const float wx = P[Y::OFF_W + n[0]], wy = P[Y::OFF_W + 3 + n[1]], wz = P[Y::OFF_W + 6 + n[2]];
+              w = wx * wy * wz * kw;
+              gw[0] = P[Y::OFF_G + n[0]] * wy * wz * kg;
+              gw[1] = wx * P[Y::OFF_G + 3 + n[1]] * wz * kg;
+              gw[2] = wx * wy * P[Y::OFF_G + 6 + n[2]] * kg;
+            }
+            am += w * P[Y::OFF_M];
 #pragma unroll
-          for (int j = 0; j < D; ++j) {
-            cd += Cm[i * D + j] * ((float)n[j] - (tc[j] + 1.f));
-            sg += S[i * D + j] * gw[j];
+            for (int a = 0; a < D; ++a) {
+              float u = P[Y::OFF_A + a];
+#pragma unroll
+              for (int b = 0; b < D; ++b) u += P[Y::OFF_B + a * D + b] * (float)n[b];
+              float s = 0.f;
+#pragma unroll
+              for (int b = 0; b < D; ++b) s += P[Y::OFF_S + a * D + b] * gw[b];
+              ap[a] += w * u + s;
+            }
           }
-          mom[i] = wm * (vp[i] + cd) + sg;
         }
-        int ti = 0;
+        if (Y::NGROUP > 1) {  // 2D: fold lane groups 1.. onto group 0 (sources read before any add)
+          __syncwarp();
+          float sm_ = 0.f, sp_[D];
 #pragma unroll
-        for (int d = 0; d < D; ++d) ti = ti * 6 + rb[d] + n[d];
+          for (int d = 0; d < D; ++d) sp_[d] = 0.f;
 #pragma unroll
-        for (int i = 0; i < D; ++i) atomicAdd(&sm[i][ti], mom[i]);
-        atomicAdd(&sm[3][ti], wm);
+          for (int q = 1; q < Y::NGROUP; ++q) {
+            sm_ += __shfl_down_sync(0xffffffffu, am, q * Y::G3);
+#pragma unroll
+            for (int d = 0; d < D; ++d) sp_[d] += __shfl_down_sync(0xffffffffu, ap[d], q * Y::G3);
+          }
+          am += sm_;
+#pragma unroll
+          for (int d = 0; d < D; ++d) ap[d] += sp_[d];
+        }
+        if (g == 0) {
+          int ti = 0;
+#pragma unroll
+          for (int d = 0; d < D; ++d) ti = ti * 6 + ((cc >> (2 * (D - 1 - d))) & 3) + n[d];
+          if (am != 0.f) atomicAdd(&tile[3 * Y::TN + ti], am);
+#pragma unroll
+          for (int d = 0; d < D; ++d)
+            if (ap[d] != 0.f) atomicAdd(&tile[d * Y::TN + ti], ap[d]);
+        }
       }
     }
     __syncthreads();
-    for (int t = threadIdx.x; t < TN; t += blockDim.x) {
-      const float4 val = make_float4(sm[0][t], sm[1][t], sm[2][t], sm[3][t]);
+    // -- 4. flush ------------------------------------------------------------
+    for (int t = threadIdx.x; t < Y::TN; t += blockDim.x) {
+      const float4 val = make_float4(tile[t], tile[Y::TN + t], D == 3 ? tile[2 * Y::TN + t] : 0.f, tile[3 * Y::TN + t]);
       if (val.x == 0.f && val.y == 0.f && val.z == 0.f && val.w == 0.f) continue;
       int I[D];
       int tt = t;
@@ -524,10 +681,15 @@ __global__ void __launch_bounds__(CHUNK) k_g2p(Ctx c) {
 }
 
 // ---------------------------------------------------------------------------
+void prepare_transfer_kernels() {
+  cudaFuncSetAttribute(k_p2g<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)P2GLayout<2>::bytes());
+  cudaFuncSetAttribute(k_p2g<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)P2GLayout<3>::bytes());
+}
+
 template <int D>
 void launch_transfer(const Ctx& c, cudaStream_t s, cudaEvent_t* ev) {
   const int G = c.sms * 8;
-  k_p2g<D><<<G, CHUNK, 0, s>>>(c);
+  k_p2g<D><<<G, CHUNK, P2GLayout<D>::bytes(), s>>>(c);
   if (ev) cudaEventRecord(ev[4], s);
   for (int l = c.L - 1; l >= 1; --l) k_restrict<D><<<G, 256, 0, s>>>(c, l);
   if (ev) cudaEventRecord(ev[5], s);
