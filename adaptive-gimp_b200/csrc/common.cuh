@@ -191,7 +191,7 @@ __device__ __forceinline__ long long total_elems(const Ctx& c, int l0, int l1, i
 // ---------------------------------------------------------------------------
 // small dense linear algebra (row-major)
 template <int D>
-__device__ __forceinline__ float det(const float* F) {
+__host__ __device__ __forceinline__ float det(const float* F) {
   if (D == 2) return F[0] * F[3] - F[1] * F[2];
   return F[0] * (F[4] * F[8] - F[5] * F[7]) - F[1] * (F[3] * F[8] - F[5] * F[6]) +
          F[2] * (F[3] * F[7] - F[4] * F[6]);
@@ -200,7 +200,7 @@ __device__ __forceinline__ float det(const float* F) {
 // 2x2: polar rotation in closed form.  R maximises tr(R^T F) over rotations,
 // which is U V^T of the rotation-variant SVD used by the reference's
 // get_stress (utils.py:11-16).
-__device__ __forceinline__ void polar2(const float* F, float& c, float& s) {
+__host__ __device__ __forceinline__ void polar2(const float* F, float& c, float& s) {
   float a = F[0] + F[3], b = F[2] - F[1];
   float n2 = a * a + b * b;
   if (n2 > 0.f) {
@@ -215,7 +215,7 @@ __device__ __forceinline__ void polar2(const float* F, float& c, float& s) {
 
 // 2x2 SVD with det U = det V = +1: R from polar2, then the symmetric factor
 // S = R^T F is diagonalised by one exact Jacobi rotation.
-__device__ __forceinline__ void svd2(const float* F, float* U, float* sig, float* V) {
+__host__ __device__ __forceinline__ void svd2(const float* F, float* U, float* sig, float* V) {
   float c, s;
   polar2(F, c, s);
   // S = R^T F
@@ -252,7 +252,7 @@ __device__ __forceinline__ void svd2(const float* F, float* U, float* sig, float
 // McAdams et al. 2011, "Computing the SVD of 3x3 matrices with minimal
 // branching and elementary floating point operations", with exact instead of
 // approximate Givens angles).
-__device__ __forceinline__ void jacobi_rot(float* S, float* V, int p, int q) {
+__host__ __device__ __forceinline__ void jacobi_rot(float* S, float* V, int p, int q) {
   // symmetric S (row-major 3x3), zero S[p][q]
   float apq = S[p * 3 + q];
   if (apq == 0.f) return;
@@ -281,7 +281,7 @@ __device__ __forceinline__ void jacobi_rot(float* S, float* V, int p, int q) {
   }
 }
 
-__device__ __forceinline__ void givens_qr(float* B, float* U, int i, int j) {
+__host__ __device__ __forceinline__ void givens_qr(float* B, float* U, int i, int j) {
   // zero B[i][j] (i > j) using rows j and i; U <- U G^T
   float a = B[j * 3 + j], b = B[i * 3 + j];
   float r2 = a * a + b * b;
@@ -305,7 +305,7 @@ __device__ __forceinline__ void givens_qr(float* B, float* U, int i, int j) {
   }
 }
 
-__device__ __forceinline__ void svd3(const float* A, float* U, float* sig, float* V) {
+__host__ __device__ __forceinline__ void svd3(const float* A, float* U, float* sig, float* V) {
   float S[9];
 #pragma unroll
   for (int i = 0; i < 3; ++i)
@@ -374,14 +374,69 @@ __device__ __forceinline__ void svd3(const float* A, float* U, float* sig, float
   }
 }
 
+// Polar rotation of a 3x3 F with det F > 0 by the scaled Newton iteration
+// X <- (g X + X^{-T} / g) / 2 (Higham, "Computing the polar decomposition
+// with applications", SIAM J. Sci. Stat. Comput. 7, 1986), with the
+// Frobenius-norm scaling g = (|X^{-1}| / |X|)^(1/2) in the first iterations.
+// For det F > 0 the limit is U V^T of the SVD.  Returns false (R undefined)
+// when det X <= 0 is met or the iteration has not settled after 12 steps.
+__host__ __device__ __forceinline__ bool polar_newton3(const float* F, float* R) {
+  float X[9];
+#pragma unroll
+  for (int i = 0; i < 9; ++i) X[i] = F[i];
+#pragma unroll 1
+  for (int it = 0; it < 12; ++it) {
+    float Y[9];
+    Y[0] = X[4] * X[8] - X[5] * X[7];
+    Y[1] = X[5] * X[6] - X[3] * X[8];
+    Y[2] = X[3] * X[7] - X[4] * X[6];
+    Y[3] = X[2] * X[7] - X[1] * X[8];
+    Y[4] = X[0] * X[8] - X[2] * X[6];
+    Y[5] = X[1] * X[6] - X[0] * X[7];
+    Y[6] = X[1] * X[5] - X[2] * X[4];
+    Y[7] = X[2] * X[3] - X[0] * X[5];
+    Y[8] = X[0] * X[4] - X[1] * X[3];
+    const float dt = X[0] * Y[0] + X[1] * Y[1] + X[2] * Y[2];
+    if (!(dt > 1e-20f)) return false;
+    const float id = 1.0f / dt;  // Y = cofactor(X) / det X = X^{-T}
+#pragma unroll
+    for (int i = 0; i < 9; ++i) Y[i] *= id;
+    float g = 1.f, gi = 1.f;
+    if (it < 3) {
+      float nx = 0.f, ny = 0.f;
+#pragma unroll
+      for (int i = 0; i < 9; ++i) {
+        nx += X[i] * X[i];
+        ny += Y[i] * Y[i];
+      }
+      g = sqrtf(sqrtf(ny / nx));
+      gi = 1.0f / g;
+    }
+    float diff = 0.f;
+#pragma unroll
+    for (int i = 0; i < 9; ++i) {
+      const float xn = 0.5f * (g * X[i] + gi * Y[i]);
+      diff = fmaxf(diff, fabsf(xn - X[i]));
+      X[i] = xn;
+    }
+    if (diff <= 1e-6f) {
+#pragma unroll
+      for (int i = 0; i < 9; ++i) R[i] = X[i];
+      return true;
+    }
+  }
+  return false;
+}
+
 // R = U V^T of the rotation-variant SVD
 template <int D>
-__device__ __forceinline__ void polar_rot(const float* F, float* R) {
+__host__ __device__ __forceinline__ void polar_rot(const float* F, float* R) {
   if (D == 2) {
     float c, s;
     polar2(F, c, s);
     R[0] = c; R[1] = -s; R[2] = s; R[3] = c;
   } else {
+    if (polar_newton3(F, R)) return;
     float U[9], sg[3], V[9];
     svd3(F, U, sg, V);
 #pragma unroll
@@ -389,6 +444,59 @@ __device__ __forceinline__ void polar_rot(const float* F, float* R) {
 #pragma unroll
       for (int j = 0; j < 3; ++j) R[i * 3 + j] = U[i * 3] * V[j * 3] + U[i * 3 + 1] * V[j * 3 + 1] + U[i * 3 + 2] * V[j * 3 + 2];
   }
+}
+
+// True when every singular value of F provably lies in [lo, hi] and det F > 0
+// (Gershgorin discs of F^T F inside [lo^2, hi^2]): a clamp of the singular
+// values to [lo, hi] then leaves F unchanged.
+template <int D>
+__host__ __device__ __forceinline__ bool singular_values_within(const float* F, float lo, float hi) {
+  if (!(det<D>(F) > 0.f)) return false;
+  float S[D * D];
+#pragma unroll
+  for (int i = 0; i < D; ++i)
+#pragma unroll
+    for (int j = 0; j < D; ++j) {
+      float a = 0.f;
+#pragma unroll
+      for (int k = 0; k < D; ++k) a += F[k * D + i] * F[k * D + j];
+      S[i * D + j] = a;
+    }
+  const float lo2 = lo * lo, hi2 = hi * hi;
+#pragma unroll
+  for (int i = 0; i < D; ++i) {
+    float r = 0.f;
+#pragma unroll
+    for (int j = 0; j < D; ++j)
+      if (j != i) r += fabsf(S[i * D + j]);
+    if (S[i * D + i] - r < lo2 || S[i * D + i] + r > hi2) return false;
+  }
+  return true;
+}
+
+// GIMP weights factorised per axis.  get_weight_stencil (adaptive_gimp.py:
+// 218-228) sums get_linear_weight (utils.py:18-42) over the 2^d cells dI and
+// 2^d corners cell_ that meet at node n = dI + cell_; the summand is a product
+// over axes, so the sum is the product of per-axis sums:
+//   w[n] = prod_d W_d[n_d] / (2^d (2r)^d),
+//   dw[n]_a = G_a[n_a] prod_{d!=a} W_d[n_d] / (2^(d-1) (2r)^d).
+__host__ __device__ __forceinline__ void axis_weights(float t, float r, float* W, float* G) {
+  // dI = 0: interval around t + 1; dI = 1: around t
+  const float bmin0 = fminf(fmaxf(t + 1.f - r, 0.f), 1.f), bmax0 = fminf(fmaxf(t + 1.f + r, 0.f), 1.f);
+  const float bmin1 = fminf(fmaxf(t - r, 0.f), 1.f), bmax1 = fminf(fmaxf(t + r, 0.f), 1.f);
+  // corner cell_ = 0: mx = 1 - bmin, mn = 1 - bmax; cell_ = 1: mx = bmax, mn = bmin
+  const float a0 = 1.f - bmin0, b0 = 1.f - bmax0;
+  const float a1 = 1.f - bmin1, b1 = 1.f - bmax1;
+  const float w00 = a0 * a0 - b0 * b0, g00 = b0 - a0;                 // dI 0, cell 0 -> node 0
+  const float w01 = bmax0 * bmax0 - bmin0 * bmin0, g01 = bmax0 - bmin0; // dI 0, cell 1 -> node 1
+  const float w10 = a1 * a1 - b1 * b1, g10 = b1 - a1;                 // dI 1, cell 0 -> node 1
+  const float w11 = bmax1 * bmax1 - bmin1 * bmin1, g11 = bmax1 - bmin1; // dI 1, cell 1 -> node 2
+  W[0] = w00;
+  W[1] = w01 + w10;
+  W[2] = w11;
+  G[0] = g00;
+  G[1] = g01 + g10;
+  G[2] = g11;
 }
 
 // ---------------------------------------------------------------------------

@@ -23,31 +23,6 @@ namespace agimp {
 #define GS_LOOP(i, n) \
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < (n); i += (long long)gridDim.x * blockDim.x)
 
-// GIMP weights factorised per axis.  get_weight_stencil (adaptive_gimp.py:
-// 218-228) sums get_linear_weight (utils.py:18-42) over the 2^d cells dI and
-// 2^d corners cell_ that meet at node n = dI + cell_; the summand is a product
-// over axes, so the sum is the product of per-axis sums:
-//   w[n] = prod_d W_d[n_d] / (2^d (2r)^d),
-//   dw[n]_a = G_a[n_a] prod_{d!=a} W_d[n_d] / (2^(d-1) (2r)^d).
-__device__ __forceinline__ void axis_weights(float t, float r, float* W, float* G) {
-  // dI = 0: interval around t + 1; dI = 1: around t
-  const float bmin0 = fminf(fmaxf(t + 1.f - r, 0.f), 1.f), bmax0 = fminf(fmaxf(t + 1.f + r, 0.f), 1.f);
-  const float bmin1 = fminf(fmaxf(t - r, 0.f), 1.f), bmax1 = fminf(fmaxf(t + r, 0.f), 1.f);
-  // corner cell_ = 0: mx = 1 - bmin, mn = 1 - bmax; cell_ = 1: mx = bmax, mn = bmin
-  const float a0 = 1.f - bmin0, b0 = 1.f - bmax0;
-  const float a1 = 1.f - bmin1, b1 = 1.f - bmax1;
-  const float w00 = a0 * a0 - b0 * b0, g00 = b0 - a0;                 // dI 0, cell 0 -> node 0
-  const float w01 = bmax0 * bmax0 - bmin0 * bmin0, g01 = bmax0 - bmin0; // dI 0, cell 1 -> node 1
-  const float w10 = a1 * a1 - b1 * b1, g10 = b1 - a1;                 // dI 1, cell 0 -> node 1
-  const float w11 = bmax1 * bmax1 - bmin1 * bmin1, g11 = bmax1 - bmin1; // dI 1, cell 1 -> node 2
-  W[0] = w00;
-  W[1] = w01 + w10;
-  W[2] = w11;
-  G[0] = g00;
-  G[1] = g01 + g10;
-  G[2] = g11;
-}
-
 template <int D>
 struct Stencil {
   float W[D][3], G[D][3];
@@ -550,6 +525,9 @@ __global__ void k_prolong(Ctx c, int l) {
 // g2p (adaptive_gimp.py:252-275), plus the snow return map (extension).
 template <int D>
 __device__ __forceinline__ void snow_project(const Ctx& c, float* F, int p) {
+  // Stomakhin et al. 2013: clamp the singular values to [1-theta_c, 1+theta_s].
+  // When they are provably inside already, F and Jp are unchanged.
+  if (singular_values_within<D>(F, 1.f - c.theta_c, 1.f + c.theta_s)) return;
   float U[D * D], sg[D], V[D * D];
   if (D == 2)
     svd2(F, U, sg, V);

@@ -1,0 +1,29 @@
+// Host-side harness over the small-matrix math of the CUDA kernels
+// (adaptive-gimp_b200/csrc/common.cuh: the same __host__ __device__ source),
+// so CPU tests can check it against numpy / scipy.  Test infrastructure only.
+#include "../../adaptive-gimp_b200/csrc/common.cuh"
+
+using namespace agimp;
+
+extern "C" {
+void h_polar_newton3(const float* F, float* R, int* ok, int n) {
+  for (int i = 0; i < n; ++i) ok[i] = polar_newton3(F + 9 * i, R + 9 * i) ? 1 : 0;
+}
+void h_polar_rot(int dim, const float* F, float* R, int n) {
+  for (int i = 0; i < n; ++i) {
+    if (dim == 2) polar_rot<2>(F + 4 * i, R + 4 * i);
+    else polar_rot<3>(F + 9 * i, R + 9 * i);
+  }
+}
+void h_svd(int dim, const float* A, float* U, float* S, float* V, int n) {
+  for (int i = 0; i < n; ++i) {
+    if (dim == 2) svd2(A + 4 * i, U + 4 * i, S + 2 * i, V + 4 * i);
+    else svd3(A + 9 * i, U + 9 * i, S + 3 * i, V + 9 * i);
+  }
+}
+void h_axis_weights(float t, float r, float* W, float* G) { axis_weights(t, r, W, G); }
+void h_within(int dim, const float* F, float lo, float hi, int* out, int n) {
+  for (int i = 0; i < n; ++i)
+    out[i] = dim == 2 ? singular_values_within<2>(F + 4 * i, lo, hi) : singular_values_within<3>(F + 9 * i, lo, hi);
+}
+}
