@@ -18,14 +18,16 @@ using namespace agimp;
 
 struct agimp_sim {
   Ctx c;
+  Particles buf[2];  // particle state ping-pongs between the two buffers
+  int par = 0;       // buf[par] holds the current state
   agimp_params p;
   int device = 0;
   std::string err;
   std::vector<void*> allocs;
   bool graphs = true;
-  cudaGraphExec_t gexec = nullptr;
-  float g_dt = NAN;
-  cudaStream_t g_stream = nullptr;
+  cudaGraphExec_t gexec[2] = {nullptr, nullptr};  // one captured substep per parity
+  float g_dt[2] = {NAN, NAN};
+  cudaStream_t g_stream[2] = {nullptr, nullptr};
   cudaStream_t internal = nullptr;
   cudaEvent_t ev_in = nullptr, ev_out = nullptr;
   float* staging = nullptr;
@@ -35,6 +37,21 @@ struct agimp_sim {
 };
 
 namespace {
+
+// the simulator's kernel context with P = current state, Q = the other buffer
+Ctx& cur(agimp_sim* s) {
+  s->c.P = s->buf[s->par];
+  s->c.Q = s->buf[1 - s->par];
+  return s->c;
+}
+
+void drop_graphs(agimp_sim* s) {
+  for (int k = 0; k < 2; ++k)
+    if (s->gexec[k]) {
+      cudaGraphExecDestroy(s->gexec[k]);
+      s->gexec[k] = nullptr;
+    }
+}
 
 agimp_status fail(agimp_sim* s, agimp_status st, const std::string& msg) {
   if (s) s->err = msg;
@@ -82,22 +99,43 @@ struct StreamUse {
   }
 };
 
-__global__ void k_aos_to_soa(const float* __restrict__ aos, float* __restrict__ soa, long long n, int comps) {
+// Caller arrays are in the caller's particle order; storage slot i holds
+// particle id[i].
+__global__ void k_aos_to_soa(const float* __restrict__ aos, const int32_t* __restrict__ id, float* __restrict__ soa,
+                             long long n, int comps) {
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n * comps;
        i += (long long)gridDim.x * blockDim.x) {
-    const long long p = i / comps;
+    const long long slot = i / comps;
     const int c = (int)(i % comps);
-    soa[c * n + p] = aos[i];
+    soa[c * n + slot] = aos[(long long)id[slot] * comps + c];
   }
 }
 
-__global__ void k_soa_to_aos(const float* __restrict__ soa, float* __restrict__ aos, long long n, int comps) {
+__global__ void k_soa_to_aos(const float* __restrict__ soa, const int32_t* __restrict__ id, float* __restrict__ aos,
+                             long long n, int comps) {
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n * comps;
        i += (long long)gridDim.x * blockDim.x) {
-    const long long p = i / comps;
+    const long long slot = i / comps;
     const int c = (int)(i % comps);
-    aos[i] = soa[c * n + p];
+    aos[(long long)id[slot] * comps + c] = soa[c * n + slot];
   }
+}
+
+__global__ void k_i32_in(const int32_t* __restrict__ src, const int32_t* __restrict__ id, int32_t* __restrict__ dst,
+                         long long n) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    dst[i] = src[id[i]];
+}
+
+__global__ void k_i32_out(const int32_t* __restrict__ src, const int32_t* __restrict__ id, int32_t* __restrict__ dst,
+                          long long n) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    dst[id[i]] = src[i];
+}
+
+__global__ void k_iota(int32_t* __restrict__ id, long long n) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    id[i] = (int32_t)i;
 }
 
 template <int D>
@@ -269,35 +307,40 @@ agimp_status agimp_create(const agimp_params* p, int32_t device, agimp_sim** out
   AL(c.touch_flag, Vf.nblocks);
   AL(c.touch_list, Vf.nblocks);
   cudaMemset(c.touch_flag, 0, Vf.nblocks * sizeof(uint32_t));
-  AL(c.bin_count, tot_blocks);
-  AL(c.bin_start, tot_blocks);
-  cudaMemset(c.bin_count, 0, tot_blocks * sizeof(int32_t));
+  AL(c.bin_count, tot_blocks + 1);  // + the bin of particles without a level
+  AL(c.bin_start, tot_blocks + 1);
+  cudaMemset(c.bin_count, 0, (tot_blocks + 1) * sizeof(int32_t));
   const long long N = c.N;
-  AL(c.chunks, N / CHUNK + tot_blocks + 1);
+  AL(c.chunks, N / CHUNK + tot_blocks + 2);
   AL(c.bin_of, N + 1);
   AL(c.rank_of, N + 1);
   AL(c.perm, N + 1);
-  AL(c.x, D * N + 1);
-  AL(c.v, D * N + 1);
-  AL(c.F, D * D * N + 1);
-  AL(c.C, D * D * N + 1);
-  AL(c.m, N + 1);
-  AL(c.Jp, N + 1);
-  AL(c.g, N + 1);
-  AL(c.fl, N + 1);
-  cudaMemset(c.x, 0, (D * N + 1) * sizeof(float));
-  cudaMemset(c.v, 0, (D * N + 1) * sizeof(float));
-  cudaMemset(c.F, 0, (D * D * N + 1) * sizeof(float));
-  cudaMemset(c.C, 0, (D * D * N + 1) * sizeof(float));
-  cudaMemset(c.m, 0, (N + 1) * sizeof(float));
-  cudaMemset(c.g, 0, (N + 1) * sizeof(int32_t));
-  cudaMemset(c.fl, 0xff, (N + 1) * sizeof(int32_t));
+  for (int k = 0; k < 2; ++k) {
+    Particles& P = s->buf[k];
+    AL(P.x, D * N + 1);
+    AL(P.v, D * N + 1);
+    AL(P.F, D * D * N + 1);
+    AL(P.C, D * D * N + 1);
+    AL(P.m, N + 1);
+    AL(P.Jp, N + 1);
+    AL(P.g, N + 1);
+    AL(P.fl, N + 1);
+    AL(P.id, N + 1);
+    cudaMemset(P.x, 0, (D * N + 1) * sizeof(float));
+    cudaMemset(P.v, 0, (D * N + 1) * sizeof(float));
+    cudaMemset(P.F, 0, (D * D * N + 1) * sizeof(float));
+    cudaMemset(P.C, 0, (D * D * N + 1) * sizeof(float));
+    cudaMemset(P.m, 0, (N + 1) * sizeof(float));
+    cudaMemset(P.g, 0, (N + 1) * sizeof(int32_t));
+    cudaMemset(P.fl, 0xff, (N + 1) * sizeof(int32_t));
+  }
+  if (N) k_iota<<<gs_blocks(N), 256>>>(s->buf[0].id, N);
   s->staging_floats = std::max<size_t>((size_t)1 << 20, (size_t)(D * D * N));
   AL(s->staging, s->staging_floats);
   {
     // Jp starts at 1
     std::vector<float> ones(N + 1, 1.0f);
-    cudaMemcpy(c.Jp, ones.data(), (N + 1) * sizeof(float), cudaMemcpyHostToDevice);
+    cudaMemcpy(s->buf[0].Jp, ones.data(), (N + 1) * sizeof(float), cudaMemcpyHostToDevice);
   }
 #undef AL
   if (cudaStreamCreateWithFlags(&s->internal, cudaStreamNonBlocking) != cudaSuccess ||
@@ -319,7 +362,7 @@ agimp_status agimp_destroy(agimp_sim* s) {
   if (!s) return AGIMP_INVALID_ARG;
   cudaSetDevice(s->device);
   cudaDeviceSynchronize();
-  if (s->gexec) cudaGraphExecDestroy(s->gexec);
+  drop_graphs(s);
   for (void* p : s->allocs) cudaFree(p);
   if (s->map_dev) cudaFree(s->map_dev);
   if (s->internal) cudaStreamDestroy(s->internal);
@@ -337,7 +380,7 @@ static agimp_status upload_soa(agimp_sim* s, const float* src, float* dst, int c
     CK(cudaMemcpyAsync(s->staging, src, N * comps * sizeof(float), cudaMemcpyHostToDevice, st));
     aos = s->staging;
   }
-  k_aos_to_soa<<<gs_blocks(N * comps), 256, 0, st>>>(aos, dst, N, comps);
+  k_aos_to_soa<<<gs_blocks(N * comps), 256, 0, st>>>(aos, s->buf[s->par].id, dst, N, comps);
   CK(cudaGetLastError());
   return AGIMP_OK;
 }
@@ -346,7 +389,7 @@ static agimp_status download_soa(agimp_sim* s, const float* src, float* dst, int
   const long long N = s->c.N;
   if (N == 0) return AGIMP_OK;
   float* aos = (memory == AGIMP_MEM_HOST) ? s->staging : dst;
-  k_soa_to_aos<<<gs_blocks(N * comps), 256, 0, st>>>(src, aos, N, comps);
+  k_soa_to_aos<<<gs_blocks(N * comps), 256, 0, st>>>(src, s->buf[s->par].id, aos, N, comps);
   CK(cudaGetLastError());
   if (memory == AGIMP_MEM_HOST) {
     CK(cudaMemcpyAsync(dst, s->staging, N * comps * sizeof(float), cudaMemcpyDeviceToHost, st));
@@ -358,10 +401,25 @@ static agimp_status download_soa(agimp_sim* s, const float* src, float* dst, int
 static agimp_status copy_i32(agimp_sim* s, const int32_t* src, int32_t* dst, int to_dev, int memory, cudaStream_t st) {
   const long long N = s->c.N;
   if (N == 0) return AGIMP_OK;
-  cudaMemcpyKind k = memory == AGIMP_MEM_HOST ? (to_dev ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToHost)
-                                              : cudaMemcpyDeviceToDevice;
-  CK(cudaMemcpyAsync(dst, src, N * sizeof(int32_t), k, st));
-  if (!to_dev && memory == AGIMP_MEM_HOST) CK(cudaStreamSynchronize(st));
+  const int32_t* id = s->buf[s->par].id;
+  int32_t* tmp = (int32_t*)s->staging;
+  if (to_dev) {
+    const int32_t* from = src;
+    if (memory == AGIMP_MEM_HOST) {
+      CK(cudaMemcpyAsync(tmp, src, N * sizeof(int32_t), cudaMemcpyHostToDevice, st));
+      from = tmp;
+    }
+    k_i32_in<<<gs_blocks(N), 256, 0, st>>>(from, id, dst, N);
+    CK(cudaGetLastError());
+  } else {
+    int32_t* to = memory == AGIMP_MEM_HOST ? tmp : dst;
+    k_i32_out<<<gs_blocks(N), 256, 0, st>>>(src, id, to, N);
+    CK(cudaGetLastError());
+    if (memory == AGIMP_MEM_HOST) {
+      CK(cudaMemcpyAsync(dst, tmp, N * sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+      CK(cudaStreamSynchronize(st));
+    }
+  }
   return AGIMP_OK;
 }
 
@@ -371,14 +429,15 @@ agimp_status agimp_set_particles(agimp_sim* s, const float* x, const float* v, c
   CK(cudaSetDevice(s->device));
   StreamUse su(s, stream);
   const int D = s->c.dim;
+  const Particles& P = s->buf[s->par];
   agimp_status r;
-  if (x && (r = upload_soa(s, x, s->c.x, D, memory, su.use))) return r;
-  if (v && (r = upload_soa(s, v, s->c.v, D, memory, su.use))) return r;
-  if (F && (r = upload_soa(s, F, s->c.F, D * D, memory, su.use))) return r;
-  if (C && (r = upload_soa(s, C, s->c.C, D * D, memory, su.use))) return r;
-  if (m && (r = upload_soa(s, m, s->c.m, 1, memory, su.use))) return r;
-  if (Jp && (r = upload_soa(s, Jp, s->c.Jp, 1, memory, su.use))) return r;
-  if (g && (r = copy_i32(s, g, s->c.g, 1, memory, su.use))) return r;
+  if (x && (r = upload_soa(s, x, P.x, D, memory, su.use))) return r;
+  if (v && (r = upload_soa(s, v, P.v, D, memory, su.use))) return r;
+  if (F && (r = upload_soa(s, F, P.F, D * D, memory, su.use))) return r;
+  if (C && (r = upload_soa(s, C, P.C, D * D, memory, su.use))) return r;
+  if (m && (r = upload_soa(s, m, P.m, 1, memory, su.use))) return r;
+  if (Jp && (r = upload_soa(s, Jp, P.Jp, 1, memory, su.use))) return r;
+  if (g && (r = copy_i32(s, g, P.g, 1, memory, su.use))) return r;
   if (memory == AGIMP_MEM_HOST) CK(cudaStreamSynchronize(su.use));  // host buffers may be reused on return
   return AGIMP_OK;
 }
@@ -389,15 +448,16 @@ agimp_status agimp_get_particles(agimp_sim* s, float* x, float* v, float* F, flo
   CK(cudaSetDevice(s->device));
   StreamUse su(s, stream);
   const int D = s->c.dim;
+  const Particles& P = s->buf[s->par];
   agimp_status r;
-  if (x && (r = download_soa(s, s->c.x, x, D, memory, su.use))) return r;
-  if (v && (r = download_soa(s, s->c.v, v, D, memory, su.use))) return r;
-  if (F && (r = download_soa(s, s->c.F, F, D * D, memory, su.use))) return r;
-  if (C && (r = download_soa(s, s->c.C, C, D * D, memory, su.use))) return r;
-  if (m && (r = download_soa(s, s->c.m, m, 1, memory, su.use))) return r;
-  if (Jp && (r = download_soa(s, s->c.Jp, Jp, 1, memory, su.use))) return r;
-  if (g && (r = copy_i32(s, s->c.g, g, 0, memory, su.use))) return r;
-  if (fl && (r = copy_i32(s, s->c.fl, fl, 0, memory, su.use))) return r;
+  if (x && (r = download_soa(s, P.x, x, D, memory, su.use))) return r;
+  if (v && (r = download_soa(s, P.v, v, D, memory, su.use))) return r;
+  if (F && (r = download_soa(s, P.F, F, D * D, memory, su.use))) return r;
+  if (C && (r = download_soa(s, P.C, C, D * D, memory, su.use))) return r;
+  if (m && (r = download_soa(s, P.m, m, 1, memory, su.use))) return r;
+  if (Jp && (r = download_soa(s, P.Jp, Jp, 1, memory, su.use))) return r;
+  if (g && (r = copy_i32(s, P.g, g, 0, memory, su.use))) return r;
+  if (fl && (r = copy_i32(s, P.fl, fl, 0, memory, su.use))) return r;
   return AGIMP_OK;
 }
 
@@ -428,10 +488,7 @@ agimp_status agimp_set_level_map(agimp_sim* s, const int8_t* table, int32_t halo
   s->c.map_h = halo;
   s->c.map_n = n;
   s->c.is_static = 1;
-  if (s->gexec) {
-    cudaGraphExecDestroy(s->gexec);
-    s->gexec = nullptr;
-  }
+  drop_graphs(s);
   (void)stream;
   return AGIMP_OK;
 }
@@ -439,10 +496,7 @@ agimp_status agimp_set_level_map(agimp_sim* s, const int8_t* table, int32_t halo
 agimp_status agimp_clear_level_map(agimp_sim* s) {
   if (!s) return AGIMP_INVALID_ARG;
   s->c.is_static = 0;
-  if (s->gexec) {
-    cudaGraphExecDestroy(s->gexec);
-    s->gexec = nullptr;
-  }
+  drop_graphs(s);
   return AGIMP_OK;
 }
 
@@ -456,32 +510,35 @@ agimp_status agimp_substep(agimp_sim* s, float dt, int32_t n_steps, void* stream
   if (!s || n_steps < 0 || !std::isfinite(dt)) return fail(s, AGIMP_INVALID_ARG, "bad substep args");
   CK(cudaSetDevice(s->device));
   StreamUse su(s, stream);
-  if (!s->graphs) {
-    s->c.dt = dt;
-    for (int i = 0; i < n_steps; ++i) launch_substep(s->c, su.use);
-    CK(cudaGetLastError());
-    s->substeps += n_steps;
-    return AGIMP_OK;
-  }
-  if (!s->gexec || s->g_dt != dt || s->g_stream != su.use) {
-    if (s->gexec) {
-      cudaGraphExecDestroy(s->gexec);
-      s->gexec = nullptr;
+  for (int i = 0; i < n_steps; ++i) {
+    const int k = s->par;
+    Ctx& c = cur(s);
+    c.dt = dt;
+    if (!s->graphs) {
+      launch_substep(c, su.use);
+      CK(cudaGetLastError());
+    } else {
+      if (!s->gexec[k] || s->g_dt[k] != dt || s->g_stream[k] != su.use) {
+        if (s->gexec[k]) {
+          cudaGraphExecDestroy(s->gexec[k]);
+          s->gexec[k] = nullptr;
+        }
+        cudaGraph_t graph = nullptr;
+        CK(cudaStreamBeginCapture(su.use, cudaStreamCaptureModeThreadLocal));
+        launch_substep(c, su.use);
+        cudaError_t e = cudaStreamEndCapture(su.use, &graph);
+        if (e != cudaSuccess) return cuda_fail(s, e, "capture substep");
+        e = cudaGraphInstantiate(&s->gexec[k], graph, 0);
+        cudaGraphDestroy(graph);
+        if (e != cudaSuccess) return cuda_fail(s, e, "instantiate substep graph");
+        s->g_dt[k] = dt;
+        s->g_stream[k] = su.use;
+      }
+      CK(cudaGraphLaunch(s->gexec[k], su.use));
     }
-    s->c.dt = dt;
-    cudaGraph_t graph = nullptr;
-    CK(cudaStreamBeginCapture(su.use, cudaStreamCaptureModeThreadLocal));
-    launch_substep(s->c, su.use);
-    cudaError_t e = cudaStreamEndCapture(su.use, &graph);
-    if (e != cudaSuccess) return cuda_fail(s, e, "capture substep");
-    e = cudaGraphInstantiate(&s->gexec, graph, 0);
-    cudaGraphDestroy(graph);
-    if (e != cudaSuccess) return cuda_fail(s, e, "instantiate substep graph");
-    s->g_dt = dt;
-    s->g_stream = su.use;
+    s->par ^= 1;  // the new state is in the other buffer
+    s->substeps += 1;
   }
-  for (int i = 0; i < n_steps; ++i) CK(cudaGraphLaunch(s->gexec, su.use));
-  s->substeps += n_steps;
   return AGIMP_OK;
 }
 
@@ -489,7 +546,7 @@ agimp_status agimp_refine_levels(agimp_sim* s, int32_t band, void* stream) {
   if (!s || band < 1 || band > 32) return fail(s, AGIMP_INVALID_ARG, "band must be in [1, 32]");
   CK(cudaSetDevice(s->device));
   StreamUse su(s, stream);
-  launch_refine(s->c, band, su.use);
+  launch_refine(cur(s), band, su.use);
   CK(cudaGetLastError());
   return AGIMP_OK;
 }
@@ -575,7 +632,7 @@ agimp_status agimp_get_stats(agimp_sim* s, agimp_stats* out) {
   CK(cudaMemcpy(h, s->c.ctr, sizeof(h), cudaMemcpyDeviceToHost));
   std::memset(out, 0, sizeof(*out));
   for (int l = 0; l < MAXL; ++l) out->active_blocks[l] = l < s->c.L ? h[CTR_LEVEL + l] : 0;
-  out->n_binned = h[CTR_BINCUR];
+  out->n_binned = h[CTR_BINCUR] - h[CTR_UNBIN];
   out->n_chunks = h[CTR_CHUNKS];
   out->substeps = s->substeps;
   return AGIMP_OK;
@@ -589,8 +646,10 @@ agimp_status agimp_profile_substep(agimp_sim* s, float dt, float* ms, int32_t n,
   StreamUse su(s, stream);
   cudaEvent_t ev[PHASES + 1];
   for (int i = 0; i <= PHASES; ++i) CK(cudaEventCreate(&ev[i]));
-  s->c.dt = dt;
-  launch_substep(s->c, su.use, ev);
+  Ctx& c = cur(s);
+  c.dt = dt;
+  launch_substep(c, su.use, ev);
+  s->par ^= 1;
   cudaError_t e = cudaEventSynchronize(ev[PHASES]);
   for (int i = 0; i < PHASES && e == cudaSuccess; ++i) e = cudaEventElapsedTime(&ms[i], ev[i], ev[i + 1]);
   for (int i = 0; i <= PHASES; ++i) cudaEventDestroy(ev[i]);

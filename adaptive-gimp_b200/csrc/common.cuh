@@ -39,6 +39,7 @@ enum {
   CTR_BINCUR = 9,  // particles placed by the bin allocator
   CTR_CHUNKS = 10, // P2G/G2P work items
   CTR_ERR = 11,    // error bits
+  CTR_UNBIN = 12,  // particles without a level (fl_p = -1) in the last substep
   // [16, 22): particle bounding box used by the refinement rule
   CTR_COUNT = 24
 };
@@ -51,6 +52,18 @@ struct LevelDev {
   float4* node;
   int32_t* bmap;
   int32_t* blist;
+};
+
+struct Particles {
+  float* x;    // [dim][N]
+  float* v;    // [dim][N]
+  float* F;    // [dim*dim][N]
+  float* C;    // [dim*dim][N]
+  float* m;    // [N]
+  float* Jp;   // [N]
+  int32_t* g;  // [N] prescribed level
+  int32_t* fl; // [N] level used by the last substep
+  int32_t* id; // [N] the particle's index in the caller's arrays
 };
 
 struct Ctx {
@@ -72,14 +85,10 @@ struct Ctx {
   int32_t* bin_of;
   int32_t* rank_of;
   int32_t* perm;
-  float* x;
-  float* v;
-  float* F;
-  float* C;
-  float* m;
-  float* Jp;
-  int32_t* g;
-  int32_t* fl;
+  // Particle state, SoA.  P holds the state the substep starts from, in the
+  // bin order of the previous substep; G2P writes the new state into Q in this
+  // substep's bin order (the host swaps P and Q between substeps).
+  Particles P, Q;
   const int8_t* map;
   uint8_t* occ;  // refinement scratch over the finest cells
 };

@@ -29,7 +29,7 @@ __device__ __forceinline__ bool particle_cell(const Ctx& c, int p, int* cell) {
   bool ok = true;
 #pragma unroll
   for (int d = 0; d < D; ++d) {
-    const float x = c.x[(long long)d * c.N + p];
+    const float x = c.P.x[(long long)d * c.N + p];
     if (!(x >= 0.f && x < 1.f)) ok = false;
     cell[d] = ok ? (int)floorf(x * (float)c.sz) : 0;
   }
@@ -146,7 +146,7 @@ __global__ void k_assign(Ctx c, int band) {
       break;
     }
   }
-  c.g[p] = lv;
+  c.P.g[p] = lv;
 }
 
 template <int D>

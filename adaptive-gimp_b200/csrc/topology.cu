@@ -49,6 +49,7 @@ __global__ void k_clear(Ctx c) {
     c.ctr[CTR_TOUCH] = 0;
     c.ctr[CTR_BINCUR] = 0;
     c.ctr[CTR_CHUNKS] = 0;
+    c.ctr[CTR_UNBIN] = 0;
   }
   const long long tot = total_elems(c, 0, c.L, D);
   GS_LOOP(e, tot) {
@@ -112,7 +113,7 @@ __global__ void k_touch_activate(Ctx c) {
   bool esc = !valid;
 #pragma unroll
   for (int d = 0; d < D; ++d) {
-    xp[d] = valid ? c.x[(long long)d * c.N + p] : 0.f;
+    xp[d] = valid ? c.P.x[(long long)d * c.N + p] : 0.f;
     if (!(xp[d] >= 0.f && xp[d] < 1.f)) esc = true;
   }
   if (valid && esc) set_err(c, ERR_ESCAPED);
@@ -133,7 +134,7 @@ __global__ void k_touch_activate(Ctx c) {
   }
   if (esc) return;
   if (!c.is_static) {
-    const int gl = c.g[p];
+    const int gl = c.P.g[p];
     if (gl < 0 || gl >= c.L) return;
     const float inv = (float)(c.coarsest << gl);
     int base[D];
@@ -392,7 +393,9 @@ __global__ void k_ghost_tj(Ctx c) {
 // ---------------------------------------------------------------------------
 // level_mapping (adaptive_gimp.py:189-216): fl_p = finest level with an
 // ACTIVATED cell among the 2^d cells around the particle; bin = (fl_p, block
-// of base).  The rank inside the bin comes from a warp-aggregated atomic.
+// of base).  Particles without a level go to one extra bin after all block
+// bins, so that every particle gets a slot in the new order.  The rank inside
+// the bin comes from a warp-aggregated atomic.
 template <int D>
 __global__ void k_bin(Ctx c) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
@@ -403,10 +406,12 @@ __global__ void k_bin(Ctx c) {
     bool esc = false;
 #pragma unroll
     for (int d = 0; d < D; ++d) {
-      xp[d] = c.x[(long long)d * c.N + p];
+      xp[d] = c.P.x[(long long)d * c.N + p];
       if (!(xp[d] >= 0.f && xp[d] < 1.f)) esc = true;
     }
     int fl = -1;
+    int nbins = 0;
+    for (int q = 0; q < c.L; ++q) nbins += c.ctr[CTR_LEVEL + q];
     if (!esc) {
       for (int l = 0; l < c.L; ++l) {
         const float inv = (float)(c.coarsest << l);
@@ -443,7 +448,8 @@ __global__ void k_bin(Ctx c) {
         }
       }
     }
-    c.fl[p] = fl;
+    if (fl < 0) bin = nbins;  // the extra bin
+    c.P.fl[p] = fl;
   }
   const unsigned grp = __match_any_sync(0xffffffffu, bin);
   const int leader = __ffs(grp) - 1;
@@ -500,8 +506,9 @@ __device__ __forceinline__ int2 block_incl_scan2(int a, int b, int2* warp_sums) 
 __global__ void __launch_bounds__(1024) k_offsets(Ctx c) {
   __shared__ int2 warp_sums[32];
   __shared__ int2 s_base;
-  long long nb = 0;
-  for (int q = 0; q < c.L; ++q) nb += c.ctr[CTR_LEVEL + q];
+  long long nblk = 0;
+  for (int q = 0; q < c.L; ++q) nblk += c.ctr[CTR_LEVEL + q];
+  const long long nb = nblk + 1;  // block bins + the extra bin of particles without a level
   for (long long t0 = (long long)blockIdx.x * blockDim.x; t0 < nb; t0 += (long long)gridDim.x * blockDim.x) {
     const long long b = t0 + threadIdx.x;
     int cnt = 0;
@@ -520,13 +527,18 @@ __global__ void __launch_bounds__(1024) k_offsets(Ctx c) {
       const int start = s_base.x + inc.x - cnt;
       c.bin_start[b] = start;
       const int ch0 = s_base.y + inc.y - nch;
-      int l = 0;
-      long long r = b;
-      while (l < c.L - 1 && r >= c.ctr[CTR_LEVEL + l]) {
-        r -= c.ctr[CTR_LEVEL + l];
-        ++l;
+      int l = -1, blk = 0;  // level -1 marks the extra bin
+      if (b < nblk) {
+        l = 0;
+        long long r = b;
+        while (l < c.L - 1 && r >= c.ctr[CTR_LEVEL + l]) {
+          r -= c.ctr[CTR_LEVEL + l];
+          ++l;
+        }
+        blk = c.lev[l].blist[r];
+      } else {
+        c.ctr[CTR_UNBIN] = cnt;
       }
-      const int blk = c.lev[l].blist[r];
       for (int j = 0; j < nch; ++j) c.chunks[ch0 + j] = make_int4(l, blk, start + j * CHUNK, min(CHUNK, cnt - j * CHUNK));
     }
     __syncthreads();
@@ -535,7 +547,7 @@ __global__ void __launch_bounds__(1024) k_offsets(Ctx c) {
 
 __global__ void k_scatter(Ctx c) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >= c.N || c.fl[p] < 0) return;
+  if (p >= c.N) return;
   c.perm[c.bin_start[c.bin_of[p]] + c.rank_of[p]] = p;
 }
 

@@ -87,14 +87,13 @@ struct P2GLayout {
   static constexpr int G3 = (D == 2) ? 9 : 27;  // stencil nodes
   static constexpr int NGROUP = 32 / G3;        // lane groups per warp
   static constexpr int TN = (D == 2) ? 36 : 216;
-  static constexpr int OFF_W = 0;               // W[d][3]
-  static constexpr int OFF_G = 3 * D;           // G[d][3]
-  static constexpr int OFF_M = 6 * D;           // m
-  static constexpr int OFF_A = OFF_M + 1;       // a[d]
-  static constexpr int OFF_B = OFF_A + D;       // B[d][d]
-  static constexpr int OFF_S = OFF_B + D * D;   // S[d][d]
-  static constexpr int NF = OFF_S + D * D;
-  static constexpr int STRIDE = NF | 1;         // odd: conflict-free per-particle columns
+  // per-particle record, read by every lane of a task:
+  //   float4 [0]          (m, a_0, a_1, a_2)      a = m (v - C (tc + 1))
+  //   float4 [1 .. D]     rows of B = m C         (4th lane unused)
+  //   float4 [1+D .. 2D]  rows of the scaled stress S
+  //   float  [4(1+2D) ..] W[d][3], G[d][3]        per-axis weights / gradients
+  static constexpr int OFF_WG = 4 * (1 + 2 * D);
+  static constexpr int STRIDE = OFF_WG + ((6 * D + 3) & ~3);  // multiple of 4 floats
   static constexpr int MAXTASK = NC + CHUNK / 32;
   static constexpr size_t bytes() {
     return sizeof(float) * ((size_t)CHUNK * STRIDE + 4 * TN) +
@@ -127,6 +126,7 @@ __global__ void __launch_bounds__(CHUNK) k_p2g(Ctx c) {
   for (int ch = blockIdx.x; ch < nch; ch += gridDim.x) {
     const int4 wd = c.chunks[ch];
     const int l = wd.x;
+    if (l < 0) continue;  // particles without a level: no transfer (uniform over the CTA)
     const LevelDev& V = c.lev[l];
     for (int i = threadIdx.x; i < 4 * Y::TN; i += blockDim.x) tile[i] = 0.f;
     for (int i = threadIdx.x; i < Y::NC; i += blockDim.x) s_cnt[i] = 0;
@@ -136,7 +136,7 @@ __global__ void __launch_bounds__(CHUNK) k_p2g(Ctx c) {
     // -- 1. per-particle quantities ------------------------------------------
     const int i = threadIdx.x;
     int cell = -1;
-    if (i < wd.w) {
+    if (l >= 0 && i < wd.w) {
       const int p = c.perm[wd.z + i];
       const long long N = c.N;
       const float inv = (float)(c.coarsest << l);
@@ -144,15 +144,16 @@ __global__ void __launch_bounds__(CHUNK) k_p2g(Ctx c) {
       float xp[D], vp[D], F[D * D], Cm[D * D];
 #pragma unroll
       for (int d = 0; d < D; ++d) {
-        xp[d] = c.x[d * N + p];
-        vp[d] = c.v[d * N + p];
+        xp[d] = c.P.x[d * N + p];
+        vp[d] = c.P.v[d * N + p];
       }
 #pragma unroll
       for (int k = 0; k < D * D; ++k) {
-        F[k] = c.F[k * N + p];
-        Cm[k] = c.C[k * N + p];
+        F[k] = c.P.F[k * N + p];
+        Cm[k] = c.P.C[k * N + p];
       }
-      const float mp = c.m[p];
+      const float mp = c.P.m[p];
+      const float jp = c.plast == 1 ? c.P.Jp[p] : 1.f;
       float tc[D];
       cell = 0;
 #pragma unroll
@@ -164,7 +165,7 @@ __global__ void __launch_bounds__(CHUNK) k_p2g(Ctx c) {
       }
       float mu = c.mu, la = c.la;
       if (c.plast == 1) {
-        const float h = expf(c.xi * (1.f - c.Jp[p]));
+        const float h = expf(c.xi * (1.f - jp));
         mu *= h;
         la *= h;
       }
@@ -175,28 +176,32 @@ __global__ void __launch_bounds__(CHUNK) k_p2g(Ctx c) {
       const float diag = la * J * (J - 1.f);
       const float sc = (-c.dt * pw) / (rd * dx);
       float* P = pd + i * Y::STRIDE;
+      float4* P4 = (float4*)P;
+      float a[D];
 #pragma unroll
-      for (int a = 0; a < D; ++a)
-#pragma unroll
-        for (int b = 0; b < D; ++b) {
-          float s = 0.f;
-#pragma unroll
-          for (int k = 0; k < D; ++k) s += (tmu * (F[a * D + k] - Rm[a * D + k])) * F[b * D + k];
-          P[Y::OFF_S + a * D + b] = sc * (s + (a == b ? diag : 0.f));
-        }
-#pragma unroll
-      for (int d = 0; d < D; ++d) axis_weights(tc[d], c.radius, P + Y::OFF_W + 3 * d, P + Y::OFF_G + 3 * d);
-      P[Y::OFF_M] = mp;
-#pragma unroll
-      for (int a = 0; a < D; ++a) {
+      for (int r = 0; r < D; ++r) {
         float cd = 0.f;
 #pragma unroll
-        for (int b = 0; b < D; ++b) {
-          cd += Cm[a * D + b] * (tc[b] + 1.f);
-          P[Y::OFF_B + a * D + b] = mp * Cm[a * D + b];
-        }
-        P[Y::OFF_A + a] = mp * (vp[a] - cd);
+        for (int b = 0; b < D; ++b) cd += Cm[r * D + b] * (tc[b] + 1.f);
+        a[r] = mp * (vp[r] - cd);
       }
+      P4[0] = make_float4(mp, a[0], a[1], D == 3 ? a[D - 1] : 0.f);
+#pragma unroll
+      for (int r = 0; r < D; ++r) {
+        float s[3] = {0.f, 0.f, 0.f};
+#pragma unroll
+        for (int b = 0; b < D; ++b) {
+          float acc = 0.f;
+#pragma unroll
+          for (int k = 0; k < D; ++k) acc += (tmu * (F[r * D + k] - Rm[r * D + k])) * F[b * D + k];
+          s[b] = sc * (acc + (r == b ? diag : 0.f));
+        }
+        P4[1 + r] = make_float4(mp * Cm[r * D], mp * Cm[r * D + 1], D == 3 ? mp * Cm[r * D + D - 1] : 0.f, 0.f);
+        P4[1 + D + r] = make_float4(s[0], s[1], s[2], 0.f);
+      }
+#pragma unroll
+      for (int d = 0; d < D; ++d)
+        axis_weights(tc[d], c.radius, P + Y::OFF_WG + 3 * d, P + Y::OFF_WG + 3 * D + 3 * d);
     }
     // rank inside the cell (warp-aggregated shared atomics)
     int rank = 0;
@@ -267,29 +272,39 @@ __global__ void __launch_bounds__(CHUNK) k_p2g(Ctx c) {
         if (on) {
           for (int j = g; j < len; j += Y::NGROUP) {
             const float* P = pd + s_sorted[s0 + j] * Y::STRIDE;
+            const float4* P4 = (const float4*)P;
+            const float* W = P + Y::OFF_WG;
+            const float* G = W + 3 * D;
             float w, gw[D];
             if (D == 2) {
-              const float wx = P[Y::OFF_W + n[0]], wy = P[Y::OFF_W + 3 + n[1]];
+              const float wx = W[n[0]], wy = W[3 + n[1]];
               w = wx * wy * kw;
-              gw[0] = P[Y::OFF_G + n[0]] * wy * kg;
-              gw[1] = wx * P[Y::OFF_G + 3 + n[1]] * kg;
+              gw[0] = G[n[0]] * wy * kg;
+              gw[1] = wx * G[3 + n[1]] * kg;
             } else {
-              const float wx = P[Y::OFF_W + n[0]], wy = P[Y::OFF_W + 3 + n[1]], wz = P[Y::OFF_W + 6 + n[2]];
-              w = wx * wy * wz * kw;
-              gw[0] = P[Y::OFF_G + n[0]] * wy * wz * kg;
-              gw[1] = wx * P[Y::OFF_G + 3 + n[1]] * wz * kg;
-              gw[2] = wx * wy * P[Y::OFF_G + 6 + n[2]] * kg;
+              const float wx = W[n[0]], wy = W[3 + n[1]], wz = W[6 + n[2]];
+              const float wyz = wy * wz;
+              w = wx * wyz * kw;
+              gw[0] = G[n[0]] * wyz * kg;
+              gw[1] = wx * G[3 + n[1]] * wz * kg;
+              gw[2] = wx * wy * G[6 + n[2]] * kg;
             }
-            am += w * P[Y::OFF_M];
+            const float4 ma = P4[0];
+            am += w * ma.x;
+            const float av[3] = {ma.y, ma.z, ma.w};
 #pragma unroll
-            for (int a = 0; a < D; ++a) {
-              float u = P[Y::OFF_A + a];
+            for (int r = 0; r < D; ++r) {
+              const float4 Br = P4[1 + r];
+              const float4 Sr = P4[1 + D + r];
+              const float bb[3] = {Br.x, Br.y, Br.z};
+              const float ss[3] = {Sr.x, Sr.y, Sr.z};
+              float u = av[r];
 #pragma unroll
-              for (int b = 0; b < D; ++b) u += P[Y::OFF_B + a * D + b] * (float)n[b];
+              for (int b = 0; b < D; ++b) u += bb[b] * (float)n[b];
               float s = 0.f;
 #pragma unroll
-              for (int b = 0; b < D; ++b) s += P[Y::OFF_S + a * D + b] * gw[b];
-              ap[a] += w * u + s;
+              for (int b = 0; b < D; ++b) s += ss[b] * gw[b];
+              ap[r] += w * u + s;
             }
           }
         }
@@ -524,7 +539,7 @@ __global__ void k_prolong(Ctx c, int l) {
 // ---------------------------------------------------------------------------
 // g2p (adaptive_gimp.py:252-275), plus the snow return map (extension).
 template <int D>
-__device__ __forceinline__ void snow_project(const Ctx& c, float* F, int p) {
+__device__ __forceinline__ void snow_project(const Ctx& c, float* F, float& jp) {
   // Stomakhin et al. 2013: clamp the singular values to [1-theta_c, 1+theta_s].
   // When they are provably inside already, F and Jp are unchanged.
   if (singular_values_within<D>(F, 1.f - c.theta_c, 1.f + c.theta_s)) return;
@@ -541,7 +556,7 @@ __device__ __forceinline__ void snow_project(const Ctx& c, float* F, int p) {
     Jn *= cl;
     sc[d] = cl;
   }
-  c.Jp[p] = c.Jp[p] * Jo / Jn;
+  jp = jp * Jo / Jn;
 #pragma unroll
   for (int i = 0; i < D; ++i)
 #pragma unroll
@@ -553,6 +568,30 @@ __device__ __forceinline__ void snow_project(const Ctx& c, float* F, int p) {
     }
 }
 
+// G2P writes the updated particles into Q in this substep's bin order, so the
+// next substep reads every particle array with contiguous loads.  m, g and id
+// travel with the particle; fl records the level used; particles without a
+// level (the extra bin, level -1) are copied unchanged.
+template <int D>
+__device__ __forceinline__ void copy_particle(const Ctx& c, int p, int j) {
+  const long long N = c.N;
+#pragma unroll
+  for (int d = 0; d < D; ++d) {
+    c.Q.x[d * N + j] = c.P.x[d * N + p];
+    c.Q.v[d * N + j] = c.P.v[d * N + p];
+  }
+#pragma unroll
+  for (int k = 0; k < D * D; ++k) {
+    c.Q.F[k * N + j] = c.P.F[k * N + p];
+    c.Q.C[k * N + j] = c.P.C[k * N + p];
+  }
+  c.Q.m[j] = c.P.m[p];
+  c.Q.Jp[j] = c.P.Jp[p];
+  c.Q.g[j] = c.P.g[p];
+  c.Q.id[j] = c.P.id[p];
+  c.Q.fl[j] = -1;
+}
+
 template <int D>
 __global__ void __launch_bounds__(CHUNK) k_g2p(Ctx c) {
   constexpr int TN = (D == 2) ? 36 : 216;
@@ -560,10 +599,32 @@ __global__ void __launch_bounds__(CHUNK) k_g2p(Ctx c) {
   const int nch = c.ctr[CTR_CHUNKS];
   const float pw = (D == 2) ? 0.25f : 0.125f;
   const float rd = (D == 2) ? c.radius * c.radius : c.radius * c.radius * c.radius;
+  const long long N = c.N;
   for (int ch = blockIdx.x; ch < nch; ch += gridDim.x) {
     const int4 wd = c.chunks[ch];
     const int l = wd.x;
+    const int j = wd.z + threadIdx.x;
+    const bool mine = (int)threadIdx.x < wd.w;
+    if (l < 0) {  // uniform over the CTA
+      if (mine) copy_particle<D>(c, c.perm[j], j);
+      continue;
+    }
     const LevelDev& V = c.lev[l];
+    // issue the particle loads before the tile load so that they overlap
+    int p = 0;
+    float xp[D], F[D * D], jp = 1.f, mp = 0.f;
+    int gp = 0, idp = 0;
+    if (mine) {
+      p = c.perm[j];
+#pragma unroll
+      for (int d = 0; d < D; ++d) xp[d] = c.P.x[d * N + p];
+#pragma unroll
+      for (int k = 0; k < D * D; ++k) F[k] = c.P.F[k * N + p];
+      mp = c.P.m[p];
+      gp = c.P.g[p];
+      idp = c.P.id[p];
+      if (c.plast == 1) jp = c.P.Jp[p];
+    }
     int O[D];
     chunk_origin<D>(V, wd.y, O);
     for (int t = threadIdx.x; t < TN; t += blockDim.x) {
@@ -581,22 +642,17 @@ __global__ void __launch_bounds__(CHUNK) k_g2p(Ctx c) {
       if (D == 3) sv[D - 1][t] = nd.z;
     }
     __syncthreads();
-    if ((int)threadIdx.x < wd.w) {
-      const int p = c.perm[wd.z + threadIdx.x];
-      const long long N = c.N;
+    if (mine) {
       const float inv = (float)(c.coarsest << l);
       const float dx = 1.f / inv;
-      float xp[D];
-#pragma unroll
-      for (int d = 0; d < D; ++d) xp[d] = c.x[d * N + p];
-      int base[D], rb[D];
+      int rb[D];
       float tc[D];
 #pragma unroll
       for (int d = 0; d < D; ++d) {
         const float xs = xp[d] * inv;
-        base[d] = (int)(xs + 0.5f) - 1;
-        tc[d] = xs - (float)(base[d] + 1);
-        rb[d] = base[d] - O[d];
+        const int base = (int)(xs + 0.5f) - 1;
+        tc[d] = xs - (float)(base + 1);
+        rb[d] = base - O[d];
       }
       Stencil<D> st;
       make_stencil<D>(tc, c.radius, st);
@@ -626,33 +682,35 @@ __global__ void __launch_bounds__(CHUNK) k_g2p(Ctx c) {
         for (int i = 0; i < D; ++i) {
           nv[i] += gv[i] * w;
 #pragma unroll
-          for (int j = 0; j < D; ++j) G[i * D + j] += gv[i] * gw[j];
+          for (int q = 0; q < D; ++q) G[i * D + q] += gv[i] * gw[q];
         }
       }
-      float F[D * D];
-#pragma unroll
-      for (int i = 0; i < D * D; ++i) F[i] = c.F[i * N + p];
 #pragma unroll
       for (int d = 0; d < D; ++d) {
-        c.v[d * N + p] = nv[d];
-        c.x[d * N + p] = xp[d] + c.dt * nv[d];
+        c.Q.v[d * N + j] = nv[d];
+        c.Q.x[d * N + j] = xp[d] + c.dt * nv[d];
       }
 #pragma unroll
-      for (int i = 0; i < D * D; ++i) c.C[i * N + p] = G[i];
+      for (int i = 0; i < D * D; ++i) c.Q.C[i * N + j] = G[i];
       const float s = (c.dt * pw) / (rd * dx);
       float Fn[D * D];
 #pragma unroll
       for (int i = 0; i < D; ++i)
 #pragma unroll
-        for (int j = 0; j < D; ++j) {
+        for (int q = 0; q < D; ++q) {
           float a = 0.f;
 #pragma unroll
-          for (int k = 0; k < D; ++k) a += ((i == k ? 1.f : 0.f) + s * G[i * D + k]) * F[k * D + j];
-          Fn[i * D + j] = a;
+          for (int k = 0; k < D; ++k) a += ((i == k ? 1.f : 0.f) + s * G[i * D + k]) * F[k * D + q];
+          Fn[i * D + q] = a;
         }
-      if (c.plast == 1) snow_project<D>(c, Fn, p);
+      if (c.plast == 1) snow_project<D>(c, Fn, jp);
 #pragma unroll
-      for (int i = 0; i < D * D; ++i) c.F[i * N + p] = Fn[i];
+      for (int i = 0; i < D * D; ++i) c.Q.F[i * N + j] = Fn[i];
+      c.Q.m[j] = mp;
+      c.Q.Jp[j] = jp;
+      c.Q.g[j] = gp;
+      c.Q.id[j] = idp;
+      c.Q.fl[j] = l;
     }
     __syncthreads();
   }
