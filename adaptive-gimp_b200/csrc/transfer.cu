@@ -101,8 +101,48 @@ struct P2GLayout {
   }
 };
 
+// One particle's contribution to the node at offset n of its base cell:
+// mass w m and momentum w (a + B n) + S grad w (adaptive_gimp.py:249-250).
+template <int D, class Y>
+__device__ __forceinline__ void p2g_node_term(const float* P, const int* n, float kw, float kg, float& am, float* ap) {
+  const float4* P4 = (const float4*)P;
+  const float* W = P + Y::OFF_WG;
+  const float* G = W + 3 * D;
+  float w, gw[D];
+  if (D == 2) {
+    const float wx = W[n[0]], wy = W[3 + n[1]];
+    w = wx * wy * kw;
+    gw[0] = G[n[0]] * wy * kg;
+    gw[1] = wx * G[3 + n[1]] * kg;
+  } else {
+    const float wx = W[n[0]], wy = W[3 + n[1]], wz = W[6 + n[2]];
+    const float wyz = wy * wz;
+    w = wx * wyz * kw;
+    gw[0] = G[n[0]] * wyz * kg;
+    gw[1] = wx * G[3 + n[1]] * wz * kg;
+    gw[2] = wx * wy * G[6 + n[2]] * kg;
+  }
+  const float4 ma = P4[0];
+  am += w * ma.x;
+  const float av[3] = {ma.y, ma.z, ma.w};
+#pragma unroll
+  for (int r = 0; r < D; ++r) {
+    const float4 Br = P4[1 + r];
+    const float4 Sr = P4[1 + D + r];
+    const float bb[3] = {Br.x, Br.y, Br.z};
+    const float ss[3] = {Sr.x, Sr.y, Sr.z};
+    float u = av[r];
+#pragma unroll
+    for (int b = 0; b < D; ++b) u += bb[b] * (float)n[b];
+    float s = 0.f;
+#pragma unroll
+    for (int b = 0; b < D; ++b) s += ss[b] * gw[b];
+    ap[r] += w * u + s;
+  }
+}
+
 template <int D>
-__global__ void __launch_bounds__(CHUNK) k_p2g(Ctx c) {
+__global__ void __launch_bounds__(CHUNK, 4) k_p2g(Ctx c) {
   using Y = P2GLayout<D>;
   extern __shared__ float dsm[];
   float* pd = dsm;                              // [CHUNK][STRIDE]
@@ -270,43 +310,19 @@ __global__ void __launch_bounds__(CHUNK) k_p2g(Ctx c) {
 #pragma unroll
         for (int d = 0; d < D; ++d) ap[d] = 0.f;
         if (on) {
-          for (int j = g; j < len; j += Y::NGROUP) {
-            const float* P = pd + s_sorted[s0 + j] * Y::STRIDE;
-            const float4* P4 = (const float4*)P;
-            const float* W = P + Y::OFF_WG;
-            const float* G = W + 3 * D;
-            float w, gw[D];
-            if (D == 2) {
-              const float wx = W[n[0]], wy = W[3 + n[1]];
-              w = wx * wy * kw;
-              gw[0] = G[n[0]] * wy * kg;
-              gw[1] = wx * G[3 + n[1]] * kg;
-            } else {
-              const float wx = W[n[0]], wy = W[3 + n[1]], wz = W[6 + n[2]];
-              const float wyz = wy * wz;
-              w = wx * wyz * kw;
-              gw[0] = G[n[0]] * wyz * kg;
-              gw[1] = wx * G[3 + n[1]] * wz * kg;
-              gw[2] = wx * wy * G[6 + n[2]] * kg;
-            }
-            const float4 ma = P4[0];
-            am += w * ma.x;
-            const float av[3] = {ma.y, ma.z, ma.w};
+          // two particles per step: independent accumulators hide shared-memory latency
+          float am2 = 0.f, ap2[D];
 #pragma unroll
-            for (int r = 0; r < D; ++r) {
-              const float4 Br = P4[1 + r];
-              const float4 Sr = P4[1 + D + r];
-              const float bb[3] = {Br.x, Br.y, Br.z};
-              const float ss[3] = {Sr.x, Sr.y, Sr.z};
-              float u = av[r];
-#pragma unroll
-              for (int b = 0; b < D; ++b) u += bb[b] * (float)n[b];
-              float s = 0.f;
-#pragma unroll
-              for (int b = 0; b < D; ++b) s += ss[b] * gw[b];
-              ap[r] += w * u + s;
-            }
+          for (int d = 0; d < D; ++d) ap2[d] = 0.f;
+          int j = g;
+          for (; j + Y::NGROUP < len; j += 2 * Y::NGROUP) {
+            p2g_node_term<D, Y>(pd + s_sorted[s0 + j] * Y::STRIDE, n, kw, kg, am, ap);
+            p2g_node_term<D, Y>(pd + s_sorted[s0 + j + Y::NGROUP] * Y::STRIDE, n, kw, kg, am2, ap2);
           }
+          if (j < len) p2g_node_term<D, Y>(pd + s_sorted[s0 + j] * Y::STRIDE, n, kw, kg, am, ap);
+          am += am2;
+#pragma unroll
+          for (int d = 0; d < D; ++d) ap[d] += ap2[d];
         }
         if (Y::NGROUP > 1) {  // 2D: fold lane groups 1.. onto group 0 (sources read before any add)
           __syncwarp();
@@ -593,127 +609,96 @@ __device__ __forceinline__ void copy_particle(const Ctx& c, int p, int j) {
 }
 
 template <int D>
-__global__ void __launch_bounds__(CHUNK) k_g2p(Ctx c) {
-  constexpr int TN = (D == 2) ? 36 : 216;
-  __shared__ float sv[D][TN];
-  const int nch = c.ctr[CTR_CHUNKS];
+__global__ void __launch_bounds__(256, 3) k_g2p(Ctx c) {
+  // one thread per particle in bin order; the 3^d nodes come through L1
+  // (particles of a bin share a (4+2)^d node tile)
   const float pw = (D == 2) ? 0.25f : 0.125f;
   const float rd = (D == 2) ? c.radius * c.radius : c.radius * c.radius * c.radius;
   const long long N = c.N;
-  for (int ch = blockIdx.x; ch < nch; ch += gridDim.x) {
-    const int4 wd = c.chunks[ch];
-    const int l = wd.x;
-    const int j = wd.z + threadIdx.x;
-    const bool mine = (int)threadIdx.x < wd.w;
-    if (l < 0) {  // uniform over the CTA
-      if (mine) copy_particle<D>(c, c.perm[j], j);
-      continue;
-    }
-    const LevelDev& V = c.lev[l];
-    // issue the particle loads before the tile load so that they overlap
-    int p = 0;
-    float xp[D], F[D * D], jp = 1.f, mp = 0.f;
-    int gp = 0, idp = 0;
-    if (mine) {
-      p = c.perm[j];
-#pragma unroll
-      for (int d = 0; d < D; ++d) xp[d] = c.P.x[d * N + p];
-#pragma unroll
-      for (int k = 0; k < D * D; ++k) F[k] = c.P.F[k * N + p];
-      mp = c.P.m[p];
-      gp = c.P.g[p];
-      idp = c.P.id[p];
-      if (c.plast == 1) jp = c.P.Jp[p];
-    }
-    int O[D];
-    chunk_origin<D>(V, wd.y, O);
-    for (int t = threadIdx.x; t < TN; t += blockDim.x) {
-      int I[D];
-      int tt = t;
-#pragma unroll
-      for (int d = D - 1; d >= 0; --d) {
-        I[d] = O[d] + tt % 6;
-        tt /= 6;
-      }
-      float4 nd = make_float4(0.f, 0.f, 0.f, 0.f);
-      if (in_store<D>(V, I)) nd = V.node[elem_of<D>(V, I)];
-      sv[0][t] = nd.x;
-      sv[1][t] = nd.y;
-      if (D == 3) sv[D - 1][t] = nd.z;
-    }
-    __syncthreads();
-    if (mine) {
-      const float inv = (float)(c.coarsest << l);
-      const float dx = 1.f / inv;
-      int rb[D];
-      float tc[D];
-#pragma unroll
-      for (int d = 0; d < D; ++d) {
-        const float xs = xp[d] * inv;
-        const int base = (int)(xs + 0.5f) - 1;
-        tc[d] = xs - (float)(base + 1);
-        rb[d] = base - O[d];
-      }
-      Stencil<D> st;
-      make_stencil<D>(tc, c.radius, st);
-      float nv[D], G[D * D];
-#pragma unroll
-      for (int i = 0; i < D; ++i) nv[i] = 0.f;
-#pragma unroll
-      for (int i = 0; i < D * D; ++i) G[i] = 0.f;
-#pragma unroll
-      for (int k = 0; k < ((D == 2) ? 9 : 27); ++k) {
-        int n[D];
-        int t = k;
-#pragma unroll
-        for (int d = D - 1; d >= 0; --d) {
-          n[d] = t % 3;
-          t /= 3;
-        }
-        float w, gw[D];
-        node_weight<D>(st, n, w, gw);
-        int ti = 0;
-#pragma unroll
-        for (int d = 0; d < D; ++d) ti = ti * 6 + rb[d] + n[d];
-        float gv[D];
-#pragma unroll
-        for (int i = 0; i < D; ++i) gv[i] = sv[i][ti];
-#pragma unroll
-        for (int i = 0; i < D; ++i) {
-          nv[i] += gv[i] * w;
-#pragma unroll
-          for (int q = 0; q < D; ++q) G[i * D + q] += gv[i] * gw[q];
-        }
-      }
-#pragma unroll
-      for (int d = 0; d < D; ++d) {
-        c.Q.v[d * N + j] = nv[d];
-        c.Q.x[d * N + j] = xp[d] + c.dt * nv[d];
-      }
-#pragma unroll
-      for (int i = 0; i < D * D; ++i) c.Q.C[i * N + j] = G[i];
-      const float s = (c.dt * pw) / (rd * dx);
-      float Fn[D * D];
-#pragma unroll
-      for (int i = 0; i < D; ++i)
-#pragma unroll
-        for (int q = 0; q < D; ++q) {
-          float a = 0.f;
-#pragma unroll
-          for (int k = 0; k < D; ++k) a += ((i == k ? 1.f : 0.f) + s * G[i * D + k]) * F[k * D + q];
-          Fn[i * D + q] = a;
-        }
-      if (c.plast == 1) snow_project<D>(c, Fn, jp);
-#pragma unroll
-      for (int i = 0; i < D * D; ++i) c.Q.F[i * N + j] = Fn[i];
-      c.Q.m[j] = mp;
-      c.Q.Jp[j] = jp;
-      c.Q.g[j] = gp;
-      c.Q.id[j] = idp;
-      c.Q.fl[j] = l;
-    }
-    __syncthreads();
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= c.N) return;
+  const int p = c.perm[j];
+  const int l = c.P.fl[p];
+  if (l < 0) {
+    copy_particle<D>(c, p, j);
+    return;
   }
+  float xp[D], F[D * D];
+#pragma unroll
+  for (int d = 0; d < D; ++d) xp[d] = c.P.x[d * N + p];
+#pragma unroll
+  for (int k = 0; k < D * D; ++k) F[k] = c.P.F[k * N + p];
+  const float mp = c.P.m[p];
+  const int gp = c.P.g[p];
+  const int idp = c.P.id[p];
+  float jp = c.plast == 1 ? c.P.Jp[p] : 1.f;
+  const LevelDev& V = c.lev[l];
+  const float inv = (float)(c.coarsest << l);
+  const float dx = 1.f / inv;
+  int base[D];
+  float tc[D];
+#pragma unroll
+  for (int d = 0; d < D; ++d) {
+    const float xs = xp[d] * inv;
+    base[d] = (int)(xs + 0.5f) - 1;
+    tc[d] = xs - (float)(base[d] + 1);
+  }
+  Stencil<D> st;
+  make_stencil<D>(tc, c.radius, st);
+  float nv[D], G[D * D];
+#pragma unroll
+  for (int i = 0; i < D; ++i) nv[i] = 0.f;
+#pragma unroll
+  for (int i = 0; i < D * D; ++i) G[i] = 0.f;
+#pragma unroll
+  for (int k = 0; k < ((D == 2) ? 9 : 27); ++k) {
+    int n[D], I[D];
+    int t = k;
+#pragma unroll
+    for (int d = D - 1; d >= 0; --d) {
+      n[d] = t % 3;
+      t /= 3;
+    }
+#pragma unroll
+    for (int d = 0; d < D; ++d) I[d] = base[d] + n[d];
+    // base lies in [-1, size-1] for an in-domain particle: always in store
+    const float4 nd = __ldg(&V.node[elem_of<D>(V, I)]);
+    const float gv[3] = {nd.x, nd.y, nd.z};
+    float w, gw[D];
+    node_weight<D>(st, n, w, gw);
+#pragma unroll
+    for (int i = 0; i < D; ++i) {
+      nv[i] += gv[i] * w;
+#pragma unroll
+      for (int q = 0; q < D; ++q) G[i * D + q] += gv[i] * gw[q];
+    }
+  }
+#pragma unroll
+  for (int d = 0; d < D; ++d) {
+    c.Q.v[d * N + j] = nv[d];
+    c.Q.x[d * N + j] = xp[d] + c.dt * nv[d];
+  }
+#pragma unroll
+  for (int i = 0; i < D * D; ++i) c.Q.C[i * N + j] = G[i];
+  const float s = (c.dt * pw) / (rd * dx);
+  float Fn[D * D];
+#pragma unroll
+  for (int i = 0; i < D; ++i)
+#pragma unroll
+    for (int q = 0; q < D; ++q) {
+      float a = 0.f;
+#pragma unroll
+      for (int k = 0; k < D; ++k) a += ((i == k ? 1.f : 0.f) + s * G[i * D + k]) * F[k * D + q];
+      Fn[i * D + q] = a;
+    }
+  if (c.plast == 1) snow_project<D>(c, Fn, jp);
+#pragma unroll
+  for (int i = 0; i < D * D; ++i) c.Q.F[i * N + j] = Fn[i];
+  c.Q.m[j] = mp;
+  c.Q.Jp[j] = jp;
+  c.Q.g[j] = gp;
+  c.Q.id[j] = idp;
+  c.Q.fl[j] = l;
 }
 
 // ---------------------------------------------------------------------------
@@ -733,7 +718,7 @@ void launch_transfer(const Ctx& c, cudaStream_t s, cudaEvent_t* ev) {
   if (ev) cudaEventRecord(ev[6], s);
   for (int l = 1; l < c.L; ++l) k_prolong<D><<<G, 256, 0, s>>>(c, l);
   if (ev) cudaEventRecord(ev[7], s);
-  k_g2p<D><<<G, CHUNK, 0, s>>>(c);
+  if (c.N) k_g2p<D><<<(c.N + 255) / 256, 256, 0, s>>>(c);
   if (ev) cudaEventRecord(ev[8], s);
 }
 
