@@ -26,6 +26,8 @@ EXPORTS = (
     "agimp_clear_level_map", "agimp_substep", "agimp_set_graphs", "agimp_refine_levels", "agimp_get_grid",
     "agimp_get_node_mask", "agimp_errors", "agimp_get_stats", "agimp_kernels_per_substep",
     "agimp_profile_substep", "agimp_refine_levels_noalloc",
+    "agimp_mlp_num_params", "agimp_mlp_create", "agimp_mlp_destroy", "agimp_mlp_set_params", "agimp_mlp_get_params",
+    "agimp_mlp_forward", "agimp_mlp_errors",
 )
 PHASES = ("blocks", "topology", "binning", "p2g", "restrict", "gridop", "prolong", "g2p")
 
@@ -89,6 +91,13 @@ def load(path: str | None = None):
     L.agimp_profile_substep.argtypes = [vp, ctypes.c_float, fp, ctypes.c_int32, vp]
     L.agimp_refine_levels_noalloc.argtypes = [vp, ctypes.c_int64, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
                                               ctypes.c_int32, vp, vp]
+    L.agimp_mlp_num_params.restype = ctypes.c_int32
+    L.agimp_mlp_create.argtypes = [ctypes.c_int32, ctypes.POINTER(vp)]
+    L.agimp_mlp_destroy.argtypes = [vp]
+    L.agimp_mlp_set_params.argtypes = [vp, vp, ctypes.c_int32, vp]
+    L.agimp_mlp_get_params.argtypes = [vp, vp, ctypes.c_int32, vp]
+    L.agimp_mlp_forward.argtypes = [vp, vp, vp, ctypes.c_int64, vp]
+    L.agimp_mlp_errors.argtypes = [vp, ctypes.POINTER(ctypes.c_uint32), ctypes.c_int32]
     _lib = L
     return L
 

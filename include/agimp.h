@@ -181,6 +181,22 @@ agimp_status agimp_profile_substep(agimp_sim* s, float dt, float* ms, int32_t n,
 agimp_status agimp_refine_levels_noalloc(const float* x, int64_t n, int32_t dim, int32_t level, int32_t coarsest_size,
                                          int32_t band, int32_t* g, void* stream);
 
+/* ---- Surrogate return-map MLP (extension; the reference has no plasticity) ----
+ * 7 inputs -> 64 -> 64 -> 4 outputs, SiLU after both hidden layers, bf16
+ * weights and activations with f32 accumulation on the tensor cores
+ * (tcgen05).  Parameters are one f32 vector of agimp_mlp_num_params() values:
+ * W1[7][64], b1[64], W2[64][64], b2[64], W3[64][4], b3[4] (row-major, y = x W + b).
+ * X [n][7] and Y [n][4] are device arrays. */
+typedef struct agimp_mlp agimp_mlp;
+int32_t agimp_mlp_num_params(void);
+agimp_status agimp_mlp_create(int32_t device, agimp_mlp** out);
+agimp_status agimp_mlp_destroy(agimp_mlp* m);
+agimp_status agimp_mlp_set_params(agimp_mlp* m, const float* params, int32_t memory, void* stream);
+agimp_status agimp_mlp_get_params(agimp_mlp* m, float* params, int32_t memory, void* stream);
+agimp_status agimp_mlp_forward(agimp_mlp* m, const float* X, float* Y, int64_t n, void* stream);
+/* bit 0: a tensor-core completion wait timed out.  Synchronizes the device. */
+agimp_status agimp_mlp_errors(agimp_mlp* m, uint32_t* bits, int32_t clear);
+
 #ifdef __cplusplus
 }
 #endif
