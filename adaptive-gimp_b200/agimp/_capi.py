@@ -27,7 +27,7 @@ EXPORTS = (
     "agimp_get_node_mask", "agimp_errors", "agimp_get_stats", "agimp_kernels_per_substep",
     "agimp_profile_substep", "agimp_refine_levels_noalloc",
     "agimp_mlp_num_params", "agimp_mlp_create", "agimp_mlp_destroy", "agimp_mlp_set_params", "agimp_mlp_get_params",
-    "agimp_mlp_forward", "agimp_mlp_errors",
+    "agimp_mlp_forward", "agimp_mlp_errors", "agimp_mlp_grad", "agimp_mlp_train_step", "agimp_mlp_reset_optimizer",
 )
 PHASES = ("blocks", "topology", "binning", "p2g", "restrict", "gridop", "prolong", "g2p")
 
@@ -98,6 +98,9 @@ def load(path: str | None = None):
     L.agimp_mlp_get_params.argtypes = [vp, vp, ctypes.c_int32, vp]
     L.agimp_mlp_forward.argtypes = [vp, vp, vp, ctypes.c_int64, vp]
     L.agimp_mlp_errors.argtypes = [vp, ctypes.POINTER(ctypes.c_uint32), ctypes.c_int32]
+    L.agimp_mlp_grad.argtypes = [vp, vp, vp, ctypes.c_int64, vp, vp, vp]
+    L.agimp_mlp_train_step.argtypes = [vp, vp, vp, ctypes.c_int64, ctypes.c_float, vp, vp]
+    L.agimp_mlp_reset_optimizer.argtypes = [vp]
     _lib = L
     return L
 

@@ -194,6 +194,17 @@ agimp_status agimp_mlp_destroy(agimp_mlp* m);
 agimp_status agimp_mlp_set_params(agimp_mlp* m, const float* params, int32_t memory, void* stream);
 agimp_status agimp_mlp_get_params(agimp_mlp* m, float* params, int32_t memory, void* stream);
 agimp_status agimp_mlp_forward(agimp_mlp* m, const float* X, float* Y, int64_t n, void* stream);
+/* Loss (mean over the n samples of the squared error summed over the 4
+ * outputs) and its gradient with respect to the parameters, both computed on
+ * the tensor cores; grad [num_params] and loss [1] are device arrays (either
+ * may be NULL).  T [n][4] holds the targets. */
+agimp_status agimp_mlp_grad(agimp_mlp* m, const float* X, const float* T, int64_t n, float* grad, float* loss,
+                            void* stream);
+/* One Adam step (beta1 0.9, beta2 0.999, eps 1e-8) on the full batch; loss
+ * (device, may be NULL) receives the loss before the step. */
+agimp_status agimp_mlp_train_step(agimp_mlp* m, const float* X, const float* T, int64_t n, float lr, float* loss,
+                                  void* stream);
+agimp_status agimp_mlp_reset_optimizer(agimp_mlp* m);
 /* bit 0: a tensor-core completion wait timed out.  Synchronizes the device. */
 agimp_status agimp_mlp_errors(agimp_mlp* m, uint32_t* bits, int32_t clear);
 

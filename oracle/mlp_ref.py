@@ -57,21 +57,25 @@ def forward(P, X, emulate_bf16=True):
 
 def loss_and_grad(P, X, T, emulate_bf16=True):
     """Mean squared error over the batch (sum over outputs, mean over samples)
-    and its gradient with respect to the f32 parameters."""
+    and its gradient with respect to the f32 parameters.  With emulate_bf16 the
+    backward pass rounds dy, dz2 and dz1 to bf16 where the kernels feed them to
+    the tensor cores (the bias gradients are column sums of the rounded values,
+    as the kernels obtain them from a row of ones in the transposed operands)."""
     y, c = forward(P, X, emulate_bf16)
     n = len(X)
     r = bf16 if emulate_bf16 else (lambda a: np.asarray(a, np.float32))
     dy = 2.0 * (y - T) / n
+    dyr = r(dy).astype(np.float64)
     g = {}
-    g["W3"] = c["a2"].T @ dy
-    g["b3"] = dy.sum(0)
-    da2 = r(dy).astype(np.float64) @ c["W3"].T if emulate_bf16 else dy @ c["W3"].T
-    dz2 = da2 * dsilu(c["z2"])
-    g["W2"] = c["a1"].T @ (r(dz2).astype(np.float64) if emulate_bf16 else dz2)
+    g["W3"] = c["a2"].T @ dyr
+    g["b3"] = dyr.sum(0)
+    da2 = dyr @ c["W3"].T
+    dz2 = r(da2 * dsilu(c["z2"])).astype(np.float64)
+    g["W2"] = c["a1"].T @ dz2
     g["b2"] = dz2.sum(0)
-    da1 = (r(dz2).astype(np.float64) if emulate_bf16 else dz2) @ c["W2"].T
-    dz1 = da1 * dsilu(c["z1"])
-    g["W1"] = c["x"].T @ (r(dz1).astype(np.float64) if emulate_bf16 else dz1)
+    da1 = dz2 @ c["W2"].T
+    dz1 = r(da1 * dsilu(c["z1"])).astype(np.float64)
+    g["W1"] = c["x"].T @ dz1
     g["b1"] = dz1.sum(0)
     loss = float(((y - T) ** 2).sum() / n)
     return loss, pack(g)
