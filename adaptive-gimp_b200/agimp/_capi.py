@@ -28,6 +28,7 @@ EXPORTS = (
     "agimp_profile_substep", "agimp_refine_levels_noalloc",
     "agimp_mlp_num_params", "agimp_mlp_create", "agimp_mlp_destroy", "agimp_mlp_set_params", "agimp_mlp_get_params",
     "agimp_mlp_forward", "agimp_mlp_errors", "agimp_mlp_grad", "agimp_mlp_train_step", "agimp_mlp_reset_optimizer",
+    "agimp_set_surrogate", "agimp_set_recorder", "agimp_recorded",
 )
 PHASES = ("blocks", "topology", "binning", "p2g", "restrict", "gridop", "prolong", "g2p")
 
@@ -39,13 +40,13 @@ class Params(ctypes.Structure):
         ("n_particles", ctypes.c_int64), ("radius", ctypes.c_double), ("gravity", ctypes.c_double * 3),
         ("E", ctypes.c_double), ("nu", ctypes.c_double), ("theta_c", ctypes.c_double),
         ("theta_s", ctypes.c_double), ("hardening", ctypes.c_double), ("n_colliders", ctypes.c_int32),
-        ("colliders", (ctypes.c_double * 6) * 4),
+        ("colliders", (ctypes.c_double * 6) * 4), ("invalid_nodes", ctypes.c_int32),
     ]
 
 
 class Stats(ctypes.Structure):
     _fields_ = [("active_blocks", ctypes.c_int32 * 8), ("n_binned", ctypes.c_int32), ("n_chunks", ctypes.c_int32),
-                ("substeps", ctypes.c_int64)]
+                ("substeps", ctypes.c_int64), ("n_surrogate", ctypes.c_int32), ("n_fallback", ctypes.c_int32)]
 
 
 class AgimpError(RuntimeError):
@@ -101,6 +102,9 @@ def load(path: str | None = None):
     L.agimp_mlp_grad.argtypes = [vp, vp, vp, ctypes.c_int64, vp, vp, vp]
     L.agimp_mlp_train_step.argtypes = [vp, vp, vp, ctypes.c_int64, ctypes.c_float, vp, vp]
     L.agimp_mlp_reset_optimizer.argtypes = [vp]
+    L.agimp_set_surrogate.argtypes = [vp, vp, ctypes.POINTER(ctypes.c_float), ctypes.c_float]
+    L.agimp_set_recorder.argtypes = [vp, vp, vp, ctypes.c_int64, ctypes.c_int32]
+    L.agimp_recorded.argtypes = [vp, ctypes.POINTER(ctypes.c_int64), ctypes.c_int32]
     _lib = L
     return L
 

@@ -214,7 +214,7 @@ class AdaptiveGIMP:
     def __init__(self, dim, level, coarsest_size, n_particles, particle_initializer, grid_initializer=None, *,
                  device=0, radius=0.5, p_mass=1.0, gravity=None, E=5e3, nu=0.2, boundary_gap=4,
                  boundary_mode="ref_slip", plasticity=None, theta_c=2.5e-2, theta_s=7.5e-3, hardening=10.0,
-                 colliders=(), graphs=True):
+                 colliders=(), invalid_nodes="raw", graphs=True):
         self._L = _capi.load()
         self.dim = dim
         self.level = level
@@ -242,6 +242,9 @@ class AdaptiveGIMP:
         p.boundary_mode = {"ref_slip": 0, "sticky": 1}[boundary_mode]
         p.plasticity = {None: 0, "none": 0, "snow": 1}[plasticity]
         p.theta_c, p.theta_s, p.hardening = theta_c, theta_s, hardening
+        # "raw": the reference's grid update (unactivated nodes keep raw P2G
+        # momentum); "normalize": extension that divides them by their mass
+        p.invalid_nodes = {"raw": 0, "normalize": 1}[invalid_nodes]
         p.n_colliders = len(colliders)
         for k, box in enumerate(colliders):
             for j in range(6):
@@ -338,7 +341,31 @@ class AdaptiveGIMP:
         st = _capi.Stats()
         _capi.check(self._L.agimp_get_stats(self._h, ctypes.byref(st)), self._h, "stats")
         return dict(active_blocks=list(st.active_blocks)[: self.level], n_binned=st.n_binned, n_chunks=st.n_chunks,
-                    substeps=st.substeps)
+                    substeps=st.substeps, n_surrogate=st.n_surrogate, n_fallback=st.n_fallback)
+
+    # -- surrogate return map (extension) ---------------------------------------
+    def set_surrogate(self, mlp, xmax=None, tol=0.02):
+        """Use `mlp` (agimp.surrogate.MLP) for the snow return map; None switches it off."""
+        if mlp is None:
+            _capi.check(self._L.agimp_set_surrogate(self._h, None, None, 0.0), self._h, "set surrogate")
+            return
+        xm = (ctypes.c_float * 7)(*[float(v) for v in xmax])
+        _capi.check(self._L.agimp_set_surrogate(self._h, mlp._h, xm, float(tol)), self._h, "set surrogate")
+        self._surrogate = mlp
+
+    def set_recorder(self, X=None, T=None, stride=1):
+        """Record (features, projected state) pairs into CUDA tensors X [cap, 7], T [cap, 4]."""
+        if X is None:
+            _capi.check(self._L.agimp_set_recorder(self._h, None, None, 0, 1), self._h, "set recorder")
+            return
+        _capi.check(self._L.agimp_set_recorder(self._h, ctypes.c_void_p(X.data_ptr()), ctypes.c_void_p(T.data_ptr()),
+                                               X.shape[0], int(stride)), self._h, "set recorder")
+        self._rec = (X, T)
+
+    def recorded(self, reset=False):
+        n = ctypes.c_int64()
+        _capi.check(self._L.agimp_recorded(self._h, ctypes.byref(n), 1 if reset else 0), self._h, "recorded")
+        return n.value
 
     def profile_substep(self, dt0, stream=None):
         """One substep with per-phase CUDA-event timing; returns {phase: ms}."""

@@ -1,8 +1,10 @@
 """Surrogate return-map MLP on the tensor cores (libagimp.so agimp_mlp_*).
 
 The network maps 7 normalised features of a particle's trial elastic state to
-4 normalised outputs (projected singular values and the new log Jp); the
-feature definitions live with the simulator integration.
+4 normalised outputs (the return map's change of the singular values and of
+log Jp, which decode to the projected singular values and the new log Jp);
+the feature definitions live with the simulator integration
+(csrc/common.cuh snow_features).
 """
 from __future__ import annotations
 
@@ -69,3 +71,75 @@ class MLP:
         b = ctypes.c_uint32()
         _capi.check(self._L.agimp_mlp_errors(self._h, ctypes.byref(b), 1 if clear else 0), None, "mlp errors")
         return b.value
+
+
+# ---------------------------------------------------------------------------
+# training pipeline
+SIG, LJ, HSC = 0.05, 0.5, 5.0  # input scales (csrc/common.cuh snow_features)
+DSIG, DLJ = 0.02, 0.02  # output scales: changes of sig and log Jp
+
+
+def record_pairs(scene, capacity, stride=1, max_substeps=400, device=0, **sim_over):
+    """Run the plain (SVD) return map on `scene` and record up to `capacity`
+    (features, projected state) pairs; returns CUDA tensors X [n, 7], T [n, 4]."""
+    import torch
+    sim = scene.build(device=device, **sim_over)
+    X = torch.empty((capacity, IN), dtype=torch.float32, device="cuda:%d" % device)
+    T = torch.empty((capacity, OUT), dtype=torch.float32, device="cuda:%d" % device)
+    sim.set_recorder(X, T, stride)
+    for i in range(max_substeps):
+        if scene.refine_every and i % scene.refine_every == 0:
+            sim.refine_levels(scene.refine_band)
+        sim.substep(scene.dt)
+        if i % 20 == 19 and sim.recorded() >= capacity:
+            break
+    n = min(sim.recorded(), capacity)
+    sim.close()
+    return X[:n], T[:n]
+
+
+def trained_range(X, margin=1.05, floor=1e-3):
+    """Per-feature bound |x_k| <= xmax_k of the training inputs."""
+    import torch
+    m = X.abs().amax(dim=0).float().cpu().numpy()
+    return np.maximum(m * margin, floor).astype(np.float32)
+
+
+def train(mlp, X, T, steps=2000, batch=65536, lr=3e-3, lr_final=3e-4, seed=0, log_every=0):
+    """Adam on random minibatches (tensor-core gradients); returns the loss history."""
+    import torch
+    g = torch.Generator(device=X.device)
+    g.manual_seed(seed)
+    loss = torch.zeros(1, dtype=torch.float32, device=X.device)
+    st = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    L = mlp._L
+    L.agimp_mlp_reset_optimizer(mlp._h)
+    hist = []
+    n = X.shape[0]
+    for it in range(steps):
+        idx = torch.randint(0, n, (min(batch, n),), generator=g, device=X.device)
+        xb, tb = X[idx].contiguous(), T[idx].contiguous()
+        a = it / max(steps - 1, 1)
+        rate = lr * (lr_final / lr) ** a  # geometric decay
+        _capi.check(L.agimp_mlp_train_step(mlp._h, ctypes.c_void_p(xb.data_ptr()), ctypes.c_void_p(tb.data_ptr()),
+                                           xb.shape[0], ctypes.c_float(rate), ctypes.c_void_p(loss.data_ptr()), st),
+                    None, "train step")
+        if log_every and (it % log_every == 0 or it == steps - 1):
+            hist.append((it, float(loss.item())))
+    return hist
+
+
+def evaluate(mlp, X, T):
+    """Mean squared error and max abs error of the MLP on (X, T)."""
+    Y = mlp.forward(X)
+    d = (Y - T).abs()
+    return float((d ** 2).sum(1).mean().item()), float(d.max().item())
+
+
+def save(path, mlp, xmax, meta=None):
+    np.savez(path, params=mlp.params(), xmax=np.asarray(xmax, np.float32), **(meta or {}))
+
+
+def load(path, device=0):
+    z = np.load(path)
+    return MLP(device=device, params=z["params"]), z["xmax"]

@@ -16,6 +16,10 @@
 
 using namespace agimp;
 
+namespace agimp {
+void mlp_buffers(const agimp_mlp* m, const void** packed, const float** P);
+}
+
 struct agimp_sim {
   Ctx c;
   Particles buf[2];  // particle state ping-pongs between the two buffers
@@ -216,6 +220,7 @@ void agimp_default_params(agimp_params* p, int32_t dim, int32_t level, int32_t c
   p->boundary_gap = 4;
   p->boundary_mode = 0;
   p->plasticity = 0;
+  p->invalid_nodes = 0;
   p->n_particles = n;
   p->radius = 0.5;
   p->gravity[1] = -100.0;
@@ -234,7 +239,8 @@ agimp_status agimp_create(const agimp_params* p, int32_t device, agimp_sim** out
   if ((p->dim != 2 && p->dim != 3) || p->level < 1 || p->level > MAXL || p->coarsest_size < 4 ||
       (p->coarsest_size & (p->coarsest_size - 1)) || p->n_particles < 0 || p->n_particles > (int64_t)1 << 30 ||
       p->n_colliders < 0 || p->n_colliders > 4 || !(p->radius > 0.0 && p->radius <= 0.5) ||
-      (p->coarsest_size << (p->level - 1)) > (1 << 13) || p->plasticity < 0 || p->plasticity > 1)
+      (p->coarsest_size << (p->level - 1)) > (1 << 13) || p->plasticity < 0 || p->plasticity > 1 ||
+      p->invalid_nodes < 0 || p->invalid_nodes > 1)
     return AGIMP_INVALID_ARG;
   agimp_sim* s = new agimp_sim();
   s->p = *p;
@@ -259,6 +265,7 @@ agimp_status agimp_create(const agimp_params* p, int32_t device, agimp_sim** out
   c.gap = p->boundary_gap;
   c.bmode = p->boundary_mode;
   c.plast = p->plasticity;
+  c.inv_norm = p->invalid_nodes;
   c.radius = (float)p->radius;
   const double mu = p->E / (2.0 * (1.0 + p->nu)), la = p->E * p->nu / ((1.0 + p->nu) * (1.0 - 2.0 * p->nu));
   c.mu = (float)mu;
@@ -633,12 +640,65 @@ agimp_status agimp_get_stats(agimp_sim* s, agimp_stats* out) {
   std::memset(out, 0, sizeof(*out));
   for (int l = 0; l < MAXL; ++l) out->active_blocks[l] = l < s->c.L ? h[CTR_LEVEL + l] : 0;
   out->n_binned = h[CTR_BINCUR] - h[CTR_UNBIN];
+  out->n_surrogate = h[CTR_SUR];
+  out->n_fallback = h[CTR_SURFB];
   out->n_chunks = h[CTR_CHUNKS];
   out->substeps = s->substeps;
   return AGIMP_OK;
 }
 
-int32_t agimp_kernels_per_substep(const agimp_sim* s) { return s ? kernels_per_substep(s->c) : 0; }
+int32_t agimp_kernels_per_substep(const agimp_sim* s) {
+  if (!s) return 0;
+  return kernels_per_substep(s->c) + ((s->c.sur && s->c.plast == 1 && s->c.N) ? 2 : 0);
+}
+
+agimp_status agimp_set_surrogate(agimp_sim* s, const agimp_mlp* m, const float* xmax, float tol) {
+  if (!s) return AGIMP_INVALID_ARG;
+  CK(cudaSetDevice(s->device));
+  CK(cudaDeviceSynchronize());
+  drop_graphs(s);
+  if (!m) {
+    s->c.sur = 0;
+    return AGIMP_OK;
+  }
+  if (s->c.plast != 1) return fail(s, AGIMP_INVALID_ARG, "the surrogate replaces the snow return map: plasticity must be snow");
+  if (!xmax || !(tol > 0.f)) return fail(s, AGIMP_INVALID_ARG, "surrogate needs xmax[7] and tol > 0");
+  const long long N = s->c.N;
+  if (!s->c.sur_X) {
+    CK(dalloc(s, &s->c.sur_X, (size_t)N * 7 + 8));
+    CK(dalloc(s, &s->c.sur_Y, (size_t)N * 4 + 8));
+    CK(dalloc(s, &s->c.sur_meta, (size_t)N * SUR_META + 8));
+  }
+  mlp_buffers(m, &s->c.mlp_packed, &s->c.mlp_P);
+  for (int k = 0; k < 8; ++k) s->c.sur_xmax[k] = k < 7 ? xmax[k] : 0.f;
+  s->c.sur_tol = tol;
+  s->c.sur = 1;
+  return AGIMP_OK;
+}
+
+agimp_status agimp_set_recorder(agimp_sim* s, float* X, float* T, int64_t capacity, int32_t stride) {
+  if (!s || (X && (!T || capacity <= 0 || stride < 1))) return fail(s, AGIMP_INVALID_ARG, "bad recorder args");
+  CK(cudaSetDevice(s->device));
+  CK(cudaDeviceSynchronize());
+  drop_graphs(s);
+  s->c.rec_X = X;
+  s->c.rec_T = T;
+  s->c.rec_cap = X ? capacity : 0;
+  s->c.rec_stride = X ? stride : 1;
+  CK(cudaMemset(s->c.ctr + CTR_REC, 0, sizeof(int32_t)));
+  return AGIMP_OK;
+}
+
+agimp_status agimp_recorded(agimp_sim* s, int64_t* count, int32_t reset) {
+  if (!s || !count) return AGIMP_INVALID_ARG;
+  CK(cudaSetDevice(s->device));
+  CK(cudaDeviceSynchronize());
+  int32_t v = 0;
+  CK(cudaMemcpy(&v, s->c.ctr + CTR_REC, sizeof(v), cudaMemcpyDeviceToHost));
+  *count = v;
+  if (reset) CK(cudaMemset(s->c.ctr + CTR_REC, 0, sizeof(int32_t)));
+  return AGIMP_OK;
+}
 
 agimp_status agimp_profile_substep(agimp_sim* s, float dt, float* ms, int32_t n, void* stream) {
   if (!s || !ms || n < PHASES || !std::isfinite(dt)) return fail(s, AGIMP_INVALID_ARG, "bad profile args");

@@ -30,7 +30,7 @@ constexpr int CHUNK = 256;  // particles per P2G/G2P work item (= CTA size)
 constexpr int HALO = 4;
 
 enum : uint32_t { ACT = 1u, GHO = 2u, TJ = 4u, CUL = 8u };
-enum : uint32_t { ERR_OOB = 1u, ERR_ESCAPED = 2u, ERR_MAP_OOB = 4u, ERR_NOBIN = 8u };
+enum : uint32_t { ERR_OOB = 1u, ERR_ESCAPED = 2u, ERR_MAP_OOB = 4u, ERR_NOBIN = 8u, ERR_MLP = 16u };
 
 // device counters
 enum {
@@ -40,6 +40,9 @@ enum {
   CTR_CHUNKS = 10, // P2G/G2P work items
   CTR_ERR = 11,    // error bits
   CTR_UNBIN = 12,  // particles without a level (fl_p = -1) in the last substep
+  CTR_SUR = 13,    // particles handed to the surrogate MLP in the last substep
+  CTR_REC = 14,    // recorded (features, projected state) pairs since the recorder was armed
+  CTR_SURFB = 15,  // surrogate predictions rejected (exact return map used instead)
   // [16, 22): particle bounding box used by the refinement rule
   CTR_COUNT = 24
 };
@@ -71,6 +74,7 @@ struct Ctx {
   int N;
   int sms;  // multiprocessors of the device (grid-stride launch width)
   int is_static, gap, bmode, plast, ncol, map_h, map_n;
+  int inv_norm;  // 1: normalise nodes that are not activated (extension)
   float radius, mu, la, theta_c, theta_s, xi, dt;
   float grav[3];
   double col[4][6];  // collider boxes, compared in double like the oracle
@@ -91,7 +95,44 @@ struct Ctx {
   Particles P, Q;
   const int8_t* map;
   uint8_t* occ;  // refinement scratch over the finest cells
+  // surrogate return map and training-pair recorder (extension)
+  int sur;                   // 1: G2P hands particles that need a projection to the MLP
+  int rec_stride;            // recorder: particles whose new slot is a multiple of this
+  long long rec_cap;         // recorder capacity (pairs)
+  float sur_tol;             // accepted residual of a prediction
+  float sur_xmax[8];         // trained range of each feature
+  float* sur_X;              // [N][7]
+  float* sur_Y;              // [N][4]
+  float* sur_meta;           // [N][SUR_META]
+  float* rec_X;              // [rec_cap][7]
+  float* rec_T;              // [rec_cap][4]
+  const void* mlp_packed;    // bf16 operand tiles of the MLP
+  const float* mlp_P;        // f32 parameters of the MLP
 };
+
+// Surrogate features of a trial elastic state with singular values sig and
+// plastic volume ratio jp (snow, Stomakhin et al. 2013): 7 inputs
+//   (sig_i - 1) / 0.05 (i < 3; 0 for the missing one in 2D), log(jp) / 0.5,
+//   xi (1 - jp) / 5 (the log of the hardening scale), theta_c / 0.025 - 1,
+//   theta_s / 0.0075 - 1,
+// and 4 outputs, the return map's change of those quantities:
+//   (projected sig_i - sig_i) / 0.02, (log(new jp) - log(jp)) / 0.02.
+// Outputs as changes are exactly 0 along elastic directions, so the network's
+// bf16 resolution only limits the plastic part of the map.
+constexpr float SUR_SIG = 0.05f, SUR_LJ = 0.5f, SUR_H = 5.f;
+constexpr float SUR_DSIG = 0.02f, SUR_DLJ = 0.02f;
+constexpr int SUR_META = 24;  // slot, U[9], V[9], sig[3], jp (padded)
+
+template <int D>
+__host__ __device__ __forceinline__ void snow_features(const float* sig, float jp, float xi, float tc, float ts,
+                                                       float* x) {
+#pragma unroll
+  for (int d = 0; d < 3; ++d) x[d] = d < D ? (sig[d] - 1.f) / SUR_SIG : 0.f;
+  x[3] = logf(jp) / SUR_LJ;
+  x[4] = xi * (1.f - jp) / SUR_H;
+  x[5] = tc / 0.025f - 1.f;
+  x[6] = ts / 0.0075f - 1.f;
+}
 
 // ---------------------------------------------------------------------------
 // index helpers
@@ -515,6 +556,9 @@ constexpr int PHASES = 8;  // blocks, topology, binning, p2g, restrict, gridop, 
 void launch_substep(const Ctx& c, cudaStream_t s, cudaEvent_t* ev = nullptr);
 void launch_refine(const Ctx& c, int band, cudaStream_t s);
 void prepare_transfer_kernels();  // kernel attributes (shared-memory opt-in); once per device
+// surrogate MLP forward over a device-side sample count (mlp.cu)
+void launch_mlp_forward_dev(const void* packed, const float* P, const float* X, float* Y, const int32_t* n_dev,
+                            long long cap, int32_t* err, int sms, cudaStream_t s);
 int kernels_per_substep(const Ctx& c);
 
 }  // namespace agimp

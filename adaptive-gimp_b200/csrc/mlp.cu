@@ -79,7 +79,9 @@ struct FwdSmem {
 // Y[n][4] = MLP(X[n][7]) for n < N.
 __global__ void __launch_bounds__(TILE) k_forward(const float* __restrict__ X, float* __restrict__ Y, long long N,
                                                   const __nv_bfloat16* __restrict__ packed,
-                                                  const float* __restrict__ P, int32_t* __restrict__ err) {
+                                                  const float* __restrict__ P, int32_t* __restrict__ err,
+                                                  const int32_t* __restrict__ n_dev, uint32_t err_bit) {
+  if (n_dev) N = min((long long)*n_dev, N);  // device-side sample count, capped by the buffer size
   extern __shared__ __align__(128) unsigned char sm[];
   __nv_bfloat16* sB = (__nv_bfloat16*)(sm + FwdSmem::B1);
   __nv_bfloat16* sA1 = (__nv_bfloat16*)(sm + FwdSmem::A1);
@@ -194,7 +196,7 @@ __global__ void __launch_bounds__(TILE) k_forward(const float* __restrict__ X, f
   __syncthreads();
   umma::fence_after_sync();
   if (warp == 0) umma::tmem_dealloc(tmem, 128);
-  if (!ok && tid == 0) atomicOr((unsigned*)err, 1u);
+  if (!ok && tid == 0) atomicOr((unsigned*)err, err_bit);
 }
 
 
@@ -499,6 +501,20 @@ __global__ void k_adam(float* __restrict__ P, const float* __restrict__ g, float
 }
 
 }  // namespace mlp
+
+void launch_mlp_forward_dev(const void* packed, const float* P, const float* X, float* Y, const int32_t* n_dev,
+                            long long cap, int32_t* err, int sms, cudaStream_t s) {
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(mlp::k_forward, cudaFuncAttributeMaxDynamicSharedMemorySize, mlp::FwdSmem::BYTES);
+    attr = true;
+  }
+  const long long ntiles = (cap + mlp::TILE - 1) / mlp::TILE;
+  const int grid = (int)std::min<long long>(ntiles, (long long)sms * 4);
+  mlp::k_forward<<<grid, mlp::TILE, mlp::FwdSmem::BYTES, s>>>(X, Y, cap, (const __nv_bfloat16*)packed, P, err, n_dev,
+                                                             ERR_MLP);
+}
+
 }  // namespace agimp
 
 using namespace agimp;
@@ -516,6 +532,13 @@ struct agimp_mlp {
   int sms = 148;
   std::string msg;
 };
+
+namespace agimp {
+void mlp_buffers(const agimp_mlp* m, const void** packed, const float** P) {
+  *packed = m->packed;
+  *P = m->P;
+}
+}  // namespace agimp
 
 extern "C" {
 
@@ -601,7 +624,8 @@ agimp_status agimp_mlp_forward(agimp_mlp* m, const float* X, float* Y, int64_t n
   if (cudaSetDevice(m->device) != cudaSuccess) return AGIMP_CUDA_ERROR;
   const long long ntiles = (n + mlp::TILE - 1) / mlp::TILE;
   const int grid = (int)std::min<long long>(ntiles, (long long)m->sms * 4);
-  mlp::k_forward<<<grid, mlp::TILE, mlp::FwdSmem::BYTES, (cudaStream_t)stream>>>(X, Y, n, m->packed, m->P, m->err);
+  mlp::k_forward<<<grid, mlp::TILE, mlp::FwdSmem::BYTES, (cudaStream_t)stream>>>(X, Y, n, m->packed, m->P, m->err,
+                                                                                 nullptr, 1u);
   return cudaGetLastError() == cudaSuccess ? AGIMP_OK : AGIMP_CUDA_ERROR;
 }
 

@@ -50,6 +50,8 @@ __global__ void k_clear(Ctx c) {
     c.ctr[CTR_BINCUR] = 0;
     c.ctr[CTR_CHUNKS] = 0;
     c.ctr[CTR_UNBIN] = 0;
+    c.ctr[CTR_SUR] = 0;
+    c.ctr[CTR_SURFB] = 0;
   }
   const long long tot = total_elems(c, 0, c.L, D);
   GS_LOOP(e, tot) {

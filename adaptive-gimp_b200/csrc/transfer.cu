@@ -445,7 +445,10 @@ __global__ void k_gridop(Ctx c) {
     const long long idx = (blk << (2 * D)) | loc;
     const float4 nd = V.node[idx];
     if (!(nd.w > 0.f)) continue;
-    if (!is_activated(nm_get<D>(c, l, I))) continue;
+    if (!is_activated(nm_get<D>(c, l, I))) {
+      if (c.inv_norm) V.node[idx] = make_float4(nd.x / nd.w, nd.y / nd.w, D == 3 ? nd.z / nd.w : nd.z, nd.w);
+      continue;
+    }
     float vv[3] = {nd.x, nd.y, nd.z};
     const int s = c.L - 1 - l;
     bool band = false;
@@ -555,33 +558,185 @@ __global__ void k_prolong(Ctx c, int l) {
 // ---------------------------------------------------------------------------
 // g2p (adaptive_gimp.py:252-275), plus the snow return map (extension).
 template <int D>
-__device__ __forceinline__ void snow_project(const Ctx& c, float* F, float& jp) {
-  // Stomakhin et al. 2013: clamp the singular values to [1-theta_c, 1+theta_s].
-  // When they are provably inside already, F and Jp are unchanged.
-  if (singular_values_within<D>(F, 1.f - c.theta_c, 1.f + c.theta_s)) return;
-  float U[D * D], sg[D], V[D * D];
+__device__ __forceinline__ void svd_d(const float* F, float* U, float* sg, float* V) {
   if (D == 2)
     svd2(F, U, sg, V);
   else
     svd3(F, U, sg, V);
+}
+
+// Exact snow return map (Stomakhin et al. 2013) on an SVD: clamp the singular
+// values to [1-theta_c, 1+theta_s], update Jp, rebuild F.  Written with
+// explicitly rounded operations (no contraction choices left to the compiler)
+// so that every inlined copy, in G2P and in the surrogate's finishing kernel,
+// gives the same bits for the same SVD.
+template <int D>
+__device__ __forceinline__ void snow_clamp_rebuild(const Ctx& c, const float* U, const float* sg, const float* V,
+                                                   float* F, float& jp) {
+  const float lo = 1.f - c.theta_c, hi = 1.f + c.theta_s;
   float Jo = 1.f, Jn = 1.f, sc[D];
 #pragma unroll
   for (int d = 0; d < D; ++d) {
-    const float cl = fminf(fmaxf(sg[d], 1.f - c.theta_c), 1.f + c.theta_s);
-    Jo *= sg[d];
-    Jn *= cl;
+    const float cl = fminf(fmaxf(sg[d], lo), hi);
+    Jo = __fmul_rn(Jo, sg[d]);
+    Jn = __fmul_rn(Jn, cl);
     sc[d] = cl;
   }
-  jp = jp * Jo / Jn;
+  jp = __fdiv_rn(__fmul_rn(jp, Jo), Jn);
 #pragma unroll
   for (int i = 0; i < D; ++i)
 #pragma unroll
     for (int j = 0; j < D; ++j) {
       float a = 0.f;
 #pragma unroll
-      for (int k = 0; k < D; ++k) a += U[i * D + k] * sc[k] * V[j * D + k];
+      for (int k = 0; k < D; ++k) a = __fmaf_rn(__fmul_rn(U[i * D + k], sc[k]), V[j * D + k], a);
       F[i * D + j] = a;
     }
+}
+
+// warp-aggregated slot reservation for the lanes that call it together
+__device__ __forceinline__ int reserve_slot(int32_t* counter) {
+  const unsigned mask = __activemask();
+  const int lane = threadIdx.x & 31;
+  const int leader = __ffs(mask) - 1;
+  int base = 0;
+  if (lane == leader) base = atomicAdd(counter, __popc(mask));
+  base = __shfl_sync(mask, base, leader);
+  return base + __popc(mask & ((1u << lane) - 1u));
+}
+
+// The surrogate's domain: a non-inverted trial state with positive singular
+// values and plastic ratio.
+template <int D>
+__device__ __forceinline__ bool sur_domain(const float* F, const float* sg, float jp) {
+  bool ok = jp > 0.f && det<D>(F) > 0.f;
+#pragma unroll
+  for (int d = 0; d < D; ++d) ok = ok && sg[d] > 0.f;
+  return ok;
+}
+
+// Recorder: the surrogate's training pair (features, exact projected state)
+// of a trial state with singular values sg and plastic ratio jp.
+template <int D>
+__device__ __forceinline__ void record_pair(const Ctx& c, const float* sg, float jp) {
+  float x[7], y[4];
+  snow_features<D>(sg, jp, c.xi, c.theta_c, c.theta_s, x);
+  float Jo = 1.f, Jn = 1.f;
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    if (d < D) {
+      const float cl = fminf(fmaxf(sg[d], 1.f - c.theta_c), 1.f + c.theta_s);
+      Jo *= sg[d];
+      Jn *= cl;
+      y[d] = (cl - sg[d]) / SUR_DSIG;
+    } else {
+      y[d] = 0.f;
+    }
+  }
+  y[3] = logf(Jo / Jn) / SUR_DLJ;
+  const int slot = reserve_slot(&c.ctr[CTR_REC]);
+  if ((long long)slot >= c.rec_cap) return;
+#pragma unroll
+  for (int k = 0; k < 7; ++k) c.rec_X[(long long)slot * 7 + k] = x[k];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) c.rec_T[(long long)slot * 4 + k] = y[k];
+}
+
+// Surrogate hand-off of a trial state with SVD (U, sg, V): its features go to
+// the MLP's input buffer and U, V, sig, jp to the metadata buffer, and
+// k_sur_finish writes F and Jp.  Returns false when the features leave the
+// trained range (the caller then applies the exact return map).
+template <int D>
+__device__ __forceinline__ bool sur_handoff(const Ctx& c, const float* U, const float* sg, const float* V, float jp,
+                                            int j) {
+  float x[7];
+  snow_features<D>(sg, jp, c.xi, c.theta_c, c.theta_s, x);
+  bool ok = true;
+#pragma unroll
+  for (int k = 0; k < 7; ++k) ok = ok && fabsf(x[k]) <= c.sur_xmax[k];
+  if (!ok) return false;
+  const int slot = reserve_slot(&c.ctr[CTR_SUR]);
+  float* meta = c.sur_meta + (long long)slot * SUR_META;
+  meta[0] = __int_as_float(j);
+#pragma unroll
+  for (int k = 0; k < D * D; ++k) {
+    meta[1 + k] = U[k];
+    meta[10 + k] = V[k];
+  }
+#pragma unroll
+  for (int d = 0; d < D; ++d) meta[19 + d] = sg[d];
+  meta[22] = jp;
+#pragma unroll
+  for (int k = 0; k < 7; ++k) c.sur_X[(long long)slot * 7 + k] = x[k];
+  return true;
+}
+
+// Snow return map of G2P's trial state F (in place): states whose singular
+// values are provably inside the clamp interval are unchanged; the others get
+// an SVD, are recorded when the recorder samples this particle, and are
+// projected exactly or handed to the surrogate.
+template <int D>
+__device__ __forceinline__ void snow_return_map(const Ctx& c, float* F, float& jp, int j) {
+  if (singular_values_within<D>(F, 1.f - c.theta_c, 1.f + c.theta_s)) return;
+  float U[D * D], sg[D], V[D * D];
+  svd_d<D>(F, U, sg, V);
+  const bool dom = (c.rec_X || c.sur) && sur_domain<D>(F, sg, jp);
+  if (c.rec_X && dom && j % c.rec_stride == 0) record_pair<D>(c, sg, jp);
+  if (c.sur && dom && sur_handoff<D>(c, U, sg, V, jp, j)) return;
+  snow_clamp_rebuild<D>(c, U, sg, V, F, jp);
+}
+
+// Apply the MLP's predictions: decode the projected singular values sig' and
+// the change of log Jp, reject them when sig' leaves the clamp interval (the
+// yield surface) or the change breaks the plastic-volume balance
+// log Jp' - log Jp = sum log sig - sum log sig' by more than sur_tol (then the
+// exact return map is used), and write F and Jp.
+template <int D>
+__global__ void k_sur_finish(Ctx c) {
+  const int n = c.ctr[CTR_SUR];
+  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < n; s += gridDim.x * blockDim.x) {
+    const float* meta = c.sur_meta + (long long)s * SUR_META;
+    const int j = __float_as_int(meta[0]);
+    float U[D * D], V[D * D], sg[D];
+#pragma unroll
+    for (int k = 0; k < D * D; ++k) {
+      U[k] = meta[1 + k];
+      V[k] = meta[10 + k];
+    }
+#pragma unroll
+    for (int d = 0; d < D; ++d) sg[d] = meta[19 + d];
+    float jp = meta[22];
+    const float* y = c.sur_Y + (long long)s * 4;
+    float sp[D], r = 0.f, lsum = 0.f;
+#pragma unroll
+    for (int d = 0; d < D; ++d) {
+      sp[d] = sg[d] + SUR_DSIG * y[d];
+      r = fmaxf(r, fmaxf(sp[d] - (1.f + c.theta_s), (1.f - c.theta_c) - sp[d]));
+      lsum += logf(sg[d]) - logf(fmaxf(sp[d], 1e-6f));
+    }
+    const float dljp = SUR_DLJ * y[3];
+    r = fmaxf(r, fabsf(dljp - lsum));
+    float F[D * D];
+    if (!(r <= c.sur_tol)) {
+      snow_clamp_rebuild<D>(c, U, sg, V, F, jp);
+      atomicAdd(&c.ctr[CTR_SURFB], 1);
+    } else {
+      jp = jp * expf(dljp);
+#pragma unroll
+      for (int a = 0; a < D; ++a)
+#pragma unroll
+        for (int b = 0; b < D; ++b) {
+          float acc = 0.f;
+#pragma unroll
+          for (int k = 0; k < D; ++k) acc += U[a * D + k] * sp[k] * V[b * D + k];
+          F[a * D + b] = acc;
+        }
+    }
+    const long long N = c.N;
+#pragma unroll
+    for (int k = 0; k < D * D; ++k) c.Q.F[k * N + j] = F[k];
+    c.Q.Jp[j] = jp;
+  }
 }
 
 // G2P writes the updated particles into Q in this substep's bin order, so the
@@ -691,7 +846,7 @@ __global__ void __launch_bounds__(256, 3) k_g2p(Ctx c) {
       for (int k = 0; k < D; ++k) a += ((i == k ? 1.f : 0.f) + s * G[i * D + k]) * F[k * D + q];
       Fn[i * D + q] = a;
     }
-  if (c.plast == 1) snow_project<D>(c, Fn, jp);
+  if (c.plast == 1) snow_return_map<D>(c, Fn, jp, j);
 #pragma unroll
   for (int i = 0; i < D * D; ++i) c.Q.F[i * N + j] = Fn[i];
   c.Q.m[j] = mp;
@@ -719,6 +874,10 @@ void launch_transfer(const Ctx& c, cudaStream_t s, cudaEvent_t* ev) {
   for (int l = 1; l < c.L; ++l) k_prolong<D><<<G, 256, 0, s>>>(c, l);
   if (ev) cudaEventRecord(ev[7], s);
   if (c.N) k_g2p<D><<<(c.N + 255) / 256, 256, 0, s>>>(c);
+  if (c.sur && c.plast == 1 && c.N) {
+    launch_mlp_forward_dev(c.mlp_packed, c.mlp_P, c.sur_X, c.sur_Y, c.ctr + CTR_SUR, c.N, c.ctr + CTR_ERR, c.sms, s);
+    k_sur_finish<D><<<c.sms * 8, 256, 0, s>>>(c);
+  }
   if (ev) cudaEventRecord(ev[8], s);
 }
 

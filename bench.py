@@ -14,6 +14,9 @@ whole scene; the refinement every 10th step is inside the timed region.
   `e2e` is the same metric through the public Python API with host buffers:
   the scene is uploaded from pinned host memory and x_p is read back to
   pinned host memory after every substep, all inside the timed region.
+--surrogate NPZ: the snow return map goes through the trained surrogate MLP
+  (tensor-core inference, exact fallback); the line adds the plain path's
+  throughput on the same scene and the position error against it.
 --impl reference: the reference's algorithm on the host cores (the CPU
   oracle restatement, OpenMP on all host threads) on the same scene; rank 0
   only.
@@ -56,6 +59,10 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=20.0, help="budget of the CPU baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--surrogate", default=None, metavar="NPZ",
+                    help="snow return map through this trained surrogate (agimp.train_surrogate output); the line "
+                         "then also reports the plain path's throughput and the position error against it")
+    ap.add_argument("--sur-tol", type=float, default=1e-3, help="surrogate residual tolerance")
     return ap.parse_args()
 
 
@@ -168,6 +175,7 @@ def cpu_oracle_run(scene, seconds, threads, steps_cap=None, warmup=1):
     kw["boundary_mode"] = {"ref_slip": 0, "sticky": 1}[sk.get("boundary_mode", "ref_slip")]
     kw["plasticity"] = {None: 0, "snow": 1}[sk.get("plasticity")]
     kw["colliders"] = tuple(sk.get("colliders", ()))
+    kw["invalid_nodes"] = {"raw": 0, "normalize": 1}[sk.get("invalid_nodes", "raw")]
     o = O.Oracle(d, scene.level, scene.coarsest, n, **kw)
     o.set_particles(scene.x, scene.v, np.tile(np.eye(d), (n, 1, 1)), np.zeros((n, d, d)), scene.m, scene.g)
     if scene.grid_initializer is not None:
@@ -218,6 +226,50 @@ def run_reference(a):
     print(json.dumps(out))
 
 
+def timed_steps(sim, scene, a, stream, dist=None, clocks=None):
+    """Warm-up, then K timed substeps between CUDA events on `stream`; returns ms."""
+    import contextlib
+
+    import torch
+    st = __import__("ctypes").c_void_p(stream.cuda_stream)
+    run_steps(sim, scene, 0, a.warmup, st)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    with (clocks or contextlib.nullcontext()):
+        e0.record(stream)
+        run_steps(sim, scene, a.warmup, a.steps, st)
+        e1.record(stream)
+        torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    return e0.elapsed_time(e1)
+
+
+def surrogate_report(a, scene, sim, ms, local):
+    """Plain (SVD return map) run of the same scene for comparison: its
+    throughput and the surrogate run's position error against it."""
+    import numpy as np
+    import torch
+    st = sim.stats()
+    plain = scene.build(device=local)
+    stream = torch.cuda.Stream()
+    with torch.cuda.stream(stream):
+        ms_plain = timed_steps(plain, scene, a, stream)
+    xs, xp = sim.x_p.to_numpy(), plain.x_p.to_numpy()
+    plain.close()
+    d = np.abs(xs.astype(np.float64) - xp)
+    return {"weights": os.path.relpath(a.surrogate, REPO) if os.path.isabs(a.surrogate) else a.surrogate,
+            "tol": a.sur_tol, "ms_per_step": ms / a.steps, "plain_ms_per_step": ms_plain / a.steps,
+            "plain_value": scene.n * a.steps / (ms_plain / 1e3), "speedup_vs_plain": ms_plain / ms,
+            "substeps_compared": a.warmup + a.steps,
+            "position_error_vs_plain": {"max": float(d.max()), "mean": float(d.mean()), "unit": "domain lengths"},
+            "last_substep": {"handed_off": st["n_surrogate"], "rejected": st["n_fallback"]}}
+
+
 def run_agimp(a):
     import numpy as np
     import torch
@@ -235,25 +287,17 @@ def run_agimp(a):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     scene = scenes.make_config(a.config, seed=rank, scale=a.scale)
     sim = scene.build(device=local)
+    mlp = None
+    if a.surrogate:
+        from agimp.surrogate import load
+        mlp, xmax = load(a.surrogate, device=local)
+        sim.set_surrogate(mlp, xmax, a.sur_tol)
     import ctypes
     stream = torch.cuda.Stream()
     st = ctypes.c_void_p(stream.cuda_stream)
     with torch.cuda.stream(stream):
-        run_steps(sim, scene, 0, a.warmup, st)
-        torch.cuda.synchronize()
-        if dist:
-            dist.barrier()
-        torch.cuda.synchronize()
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
-        with Clocks(local) as clk:
-            e0.record(stream)
-            run_steps(sim, scene, a.warmup, a.steps, st)
-            e1.record(stream)
-            torch.cuda.synchronize()
-        if dist:
-            dist.barrier()
-        ms = e0.elapsed_time(e1)
+        clk = Clocks(local)
+        ms = timed_steps(sim, scene, a, stream, dist, clk)
         errors = sim.errors()
         stats = sim.stats()
         # per-phase timing of single substeps (direct launches, CUDA events)
@@ -294,8 +338,16 @@ def run_agimp(a):
         "clocks": clk.summary(),
         "device_errors": errors,
     }
+    if mlp is not None:
+        # the per-phase profile above ran extra substeps: rebuild for the comparison
+        sim.close()
+        sim = scene.build(device=local)
+        sim.set_surrogate(mlp, xmax, a.sur_tol)
+        with torch.cuda.stream(stream):
+            timed_steps(sim, scene, a, stream)
+        out["surrogate"] = surrogate_report(a, scene, sim, ms, local)
     if not a.no_e2e:
-        out["e2e"] = e2e_run(a, scene, local)
+        out["e2e"] = e2e_run(a, scene, local, a.surrogate and (mlp, xmax, a.sur_tol))
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         threads = os.cpu_count() or 1
         val, done, el = cpu_oracle_run(scene, a.cpu_seconds, threads)
@@ -310,7 +362,7 @@ def run_agimp(a):
         print(json.dumps(out))
 
 
-def e2e_run(a, scene, local):
+def e2e_run(a, scene, local, sur=None):
     """Same metric through the public API with host buffers: upload the scene
     from pinned host memory, then per substep call substep() and read x_p back
     into pinned host memory."""
@@ -332,6 +384,8 @@ def e2e_run(a, scene, local):
     hJ[:] = 1
     out = pinned((n, d))
     sim = scene.build(device=local)
+    if sur:
+        sim.set_surrogate(*sur)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     sim.set_particles(x=hx, v=hv, F=hF, C=hC, m=hm, g=hg, Jp=hJ)

@@ -34,7 +34,7 @@
 extern "C" {
 #endif
 
-#define AGIMP_ABI_VERSION 1
+#define AGIMP_ABI_VERSION 2
 
 typedef enum {
   AGIMP_OK = 0,
@@ -79,6 +79,12 @@ typedef struct agimp_params {
   double theta_c, theta_s, hardening; /* snow parameters (extension) */
   int32_t n_colliders;    /* sticky box colliders, extension, <= 4 */
   double colliders[4][6]; /* lo[3], hi[3] in domain units */
+  /* Grid nodes that receive P2G mass but are neither activated, ghost nor
+   * T-junction nodes.  0 (reference, adaptive_gimp.py:280): the grid update
+   * skips them, so G2P reads their unnormalised momentum.  1 (extension):
+   * their momentum is divided by their mass (no gravity, no walls), which
+   * keeps dense particle regions on coarse levels stable. */
+  int32_t invalid_nodes;
 } agimp_params;
 
 typedef struct agimp_stats {
@@ -86,6 +92,8 @@ typedef struct agimp_stats {
   int32_t n_binned;         /* particles with fl_p >= 0 in the last substep */
   int32_t n_chunks;         /* P2G/G2P work items in the last substep */
   int64_t substeps;         /* substeps run since creation */
+  int32_t n_surrogate;      /* particles whose return map went to the surrogate MLP (last substep) */
+  int32_t n_fallback;       /* of those, predictions rejected for the exact return map */
 } agimp_stats;
 
 typedef struct agimp_sim agimp_sim;
@@ -205,6 +213,24 @@ agimp_status agimp_mlp_grad(agimp_mlp* m, const float* X, const float* T, int64_
 agimp_status agimp_mlp_train_step(agimp_mlp* m, const float* X, const float* T, int64_t n, float lr, float* loss,
                                   void* stream);
 agimp_status agimp_mlp_reset_optimizer(agimp_mlp* m);
+
+/* Surrogate return map in the substep (snow plasticity only).  Particles whose
+ * trial singular values leave the clamp interval get an SVD as before; their
+ * features (see snow_features in csrc/common.cuh) go through the MLP, whose
+ * prediction is used unless a feature lies outside the trained range
+ * |x_k| <= xmax[k] (k < 7, host array) or the prediction's residual (distance
+ * from the clamp interval, or the plastic-volume balance error in log Jp)
+ * exceeds tol; those particles take the exact return map.  m must outlive its
+ * use; m == NULL switches the surrogate off.  Allocates its buffers (N x 35
+ * floats) on first use. */
+agimp_status agimp_set_surrogate(agimp_sim* s, const agimp_mlp* m, const float* xmax, float tol);
+/* Training-pair recorder (snow plasticity): every substep, particles whose new
+ * slot is a multiple of `stride` append (features [7], exact projected state
+ * [4]) to the device arrays X [capacity][7], T [capacity][4]; X == NULL
+ * switches it off.  agimp_recorded returns the number appended (it may exceed
+ * capacity; only the first capacity are stored). */
+agimp_status agimp_set_recorder(agimp_sim* s, float* X, float* T, int64_t capacity, int32_t stride);
+agimp_status agimp_recorded(agimp_sim* s, int64_t* count, int32_t reset);
 /* bit 0: a tensor-core completion wait timed out.  Synchronizes the device. */
 agimp_status agimp_mlp_errors(agimp_mlp* m, uint32_t* bits, int32_t clear);
 

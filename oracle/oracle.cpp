@@ -229,6 +229,7 @@ typedef struct {
   double theta_c, theta_s, hardening;
   int32_t n_colliders;
   double colliders[4][6];  // sticky boxes: lo[3], hi[3] in domain units
+  int32_t invalid_nodes;   // 0: reference (raw momentum kept), 1: normalised
 } orc_params;
 }
 
@@ -248,7 +249,7 @@ template <int D, typename R> struct Sim : SimBase {
     std::vector<R> m, v;
     std::vector<uint8_t> blk;
   };
-  int L, coarsest, sz, gap, bmode, plast;
+  int L, coarsest, sz, gap, bmode, plast, inv_norm;
   double coarsest_dx;
   R radius, grav[3], mu, la, theta_c, theta_s, xi;
   int ncol; double col[4][6];
@@ -269,6 +270,7 @@ template <int D, typename R> struct Sim : SimBase {
   Sim(const orc_params* p, int64_t n) {
     L = p->level; coarsest = p->coarsest_size; sz = coarsest << (L - 1);
     gap = p->boundary_gap; bmode = p->boundary_mode; plast = p->plasticity;
+    inv_norm = p->invalid_nodes;
     coarsest_dx = 1.0 / coarsest;
     radius = (R)p->radius;
     for (int d = 0; d < 3; ++d) grav[d] = (R)p->gravity[d];
@@ -743,7 +745,12 @@ template <int D, typename R> struct Sim : SimBase {
       int64_t o, b; Lev& A = lev[l];
       if (!lidx(A, I, o, b)) return;
       if (!(A.m[o] > 0)) return;
-      if (!is_activated(l, I)) return;
+      if (!is_activated(l, I)) {
+        // extension (invalid_nodes = 1): normalise the momentum the
+        // reference leaves raw on nodes it does not update
+        if (inv_norm) for (int c = 0; c < D; ++c) A.v[o * D + c] /= A.m[o];
+        return;
+      }
       R* vv = &A.v[o * D];
       for (int c = 0; c < D; ++c) vv[c] /= A.m[o];
       for (int c = 0; c < D; ++c) vv[c] += grav[c] * dt;

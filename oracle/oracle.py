@@ -34,7 +34,7 @@ class OrcParams(ctypes.Structure):
         ("boundary_gap", ctypes.c_int32), ("boundary_mode", ctypes.c_int32), ("plasticity", ctypes.c_int32),
         ("radius", ctypes.c_double), ("gravity", ctypes.c_double * 3), ("E", ctypes.c_double), ("nu", ctypes.c_double),
         ("theta_c", ctypes.c_double), ("theta_s", ctypes.c_double), ("hardening", ctypes.c_double),
-        ("n_colliders", ctypes.c_int32), ("colliders", (ctypes.c_double * 6) * 4),
+        ("n_colliders", ctypes.c_int32), ("colliders", (ctypes.c_double * 6) * 4), ("invalid_nodes", ctypes.c_int32),
     ]
 
 
@@ -79,7 +79,8 @@ def _p(a, t=ctypes.c_double):
 
 
 REF_DEFAULTS = dict(radius=0.5, gravity=(0.0, -100.0, 0.0), E=5e3, nu=0.2, boundary_gap=4, boundary_mode=0,
-                    plasticity=0, theta_c=2.5e-2, theta_s=7.5e-3, hardening=10.0, colliders=())
+                    plasticity=0, theta_c=2.5e-2, theta_s=7.5e-3, hardening=10.0, colliders=(),
+                    invalid_nodes=0)
 
 
 class Oracle:
@@ -98,6 +99,7 @@ class Oracle:
         p.E, p.nu = cfg["E"], cfg["nu"]
         p.theta_c, p.theta_s, p.hardening = cfg["theta_c"], cfg["theta_s"], cfg["hardening"]
         cols = list(cfg["colliders"])
+        p.invalid_nodes = int(cfg["invalid_nodes"])
         p.n_colliders = len(cols)
         for k, c in enumerate(cols):
             for j in range(6):

@@ -37,6 +37,8 @@ def oracle_kwargs(kw, dim):
         out["plasticity"] = {None: 0, "none": 0, "snow": 1}[kw["plasticity"]]
     if "colliders" in kw:
         out["colliders"] = tuple(kw["colliders"])
+    if "invalid_nodes" in kw:
+        out["invalid_nodes"] = {"raw": 0, "normalize": 1}[kw["invalid_nodes"]]
     return out
 
 

@@ -31,7 +31,7 @@ def test_library_exports_every_declared_symbol():
 def test_abi_version_and_status_strings():
     from agimp import _capi
     lib = _capi.load()
-    assert lib.agimp_abi_version() == 1
+    assert lib.agimp_abi_version() == 2
     assert lib.agimp_status_string(0) == b"ok"
     assert lib.agimp_status_string(1) == b"invalid argument"
 
@@ -45,11 +45,13 @@ def test_default_params_are_reference_constants():
     assert p.radius == 0.5 and p.boundary_gap == 4 and p.boundary_mode == 0 and p.plasticity == 0
     assert tuple(p.gravity) == (0.0, -100.0, 0.0)
     assert p.E == 5e3 and p.nu == 0.2
+    assert p.invalid_nodes == 0  # the reference's grid update (adaptive_gimp.py:280)
 
 
 @pytest.mark.parametrize("field,value", [("dim", 4), ("level", 0), ("level", 9), ("coarsest_size", 12),
                                          ("coarsest_size", 2), ("n_particles", -1), ("radius", 0.75),
-                                         ("n_colliders", 5), ("plasticity", 7)])
+                                         ("n_colliders", 5), ("plasticity", 7),
+                                         ("invalid_nodes", 2)])
 def test_create_rejects_invalid_params(field, value):
     from agimp import _capi
     lib = _capi.load()
