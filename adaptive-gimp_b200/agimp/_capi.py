@@ -29,6 +29,10 @@ EXPORTS = (
     "agimp_mlp_num_params", "agimp_mlp_create", "agimp_mlp_destroy", "agimp_mlp_set_params", "agimp_mlp_get_params",
     "agimp_mlp_forward", "agimp_mlp_errors", "agimp_mlp_grad", "agimp_mlp_train_step", "agimp_mlp_reset_optimizer",
     "agimp_set_surrogate", "agimp_set_recorder", "agimp_recorded",
+    "agimp_set_tuning", "agimp_get_tuning", "agimp_autotune",
+    "agimp_batch_create", "agimp_batch_destroy", "agimp_batch_last_error", "agimp_batch_substep",
+    "agimp_batch_set_graphs", "agimp_batch_set_tuning", "agimp_batch_get_tuning", "agimp_batch_autotune",
+    "agimp_batch_kernels_per_substep", "agimp_batch_profile_substep",
 )
 PHASES = ("blocks", "topology", "binning", "p2g", "restrict", "gridop", "prolong", "g2p")
 
@@ -47,6 +51,13 @@ class Params(ctypes.Structure):
 class Stats(ctypes.Structure):
     _fields_ = [("active_blocks", ctypes.c_int32 * 8), ("n_binned", ctypes.c_int32), ("n_chunks", ctypes.c_int32),
                 ("substeps", ctypes.c_int64), ("n_surrogate", ctypes.c_int32), ("n_fallback", ctypes.c_int32)]
+
+
+class Tuning(ctypes.Structure):
+    _fields_ = [("chunk", ctypes.c_int32), ("ctas_per_sm", ctypes.c_int32), ("ms_per_substep", ctypes.c_float)]
+
+    def as_dict(self):
+        return dict(chunk=self.chunk, ctas_per_sm=self.ctas_per_sm, ms_per_substep=self.ms_per_substep)
 
 
 class AgimpError(RuntimeError):
@@ -105,16 +116,32 @@ def load(path: str | None = None):
     L.agimp_set_surrogate.argtypes = [vp, vp, ctypes.POINTER(ctypes.c_float), ctypes.c_float]
     L.agimp_set_recorder.argtypes = [vp, vp, vp, ctypes.c_int64, ctypes.c_int32]
     L.agimp_recorded.argtypes = [vp, ctypes.POINTER(ctypes.c_int64), ctypes.c_int32]
+    tp = ctypes.POINTER(Tuning)
+    L.agimp_set_tuning.argtypes = [vp, tp]
+    L.agimp_get_tuning.argtypes = [vp, tp]
+    L.agimp_autotune.argtypes = [vp, ctypes.c_float, ctypes.c_int32, tp, vp]
+    L.agimp_batch_create.argtypes = [ctypes.POINTER(vp), ctypes.c_int32, ctypes.POINTER(vp)]
+    L.agimp_batch_destroy.argtypes = [vp]
+    L.agimp_batch_last_error.restype = ctypes.c_char_p
+    L.agimp_batch_last_error.argtypes = [vp]
+    L.agimp_batch_substep.argtypes = [vp, ctypes.c_float, ctypes.c_int32, vp]
+    L.agimp_batch_set_graphs.argtypes = [vp, ctypes.c_int32]
+    L.agimp_batch_set_tuning.argtypes = [vp, tp]
+    L.agimp_batch_get_tuning.argtypes = [vp, tp]
+    L.agimp_batch_autotune.argtypes = [vp, ctypes.c_float, ctypes.c_int32, tp, vp]
+    L.agimp_batch_kernels_per_substep.argtypes = [vp]
+    L.agimp_batch_kernels_per_substep.restype = ctypes.c_int32
+    L.agimp_batch_profile_substep.argtypes = [vp, ctypes.c_float, fp, ctypes.c_int32, vp]
     _lib = L
     return L
 
 
-def check(status: int, handle=None, what: str = ""):
+def check(status: int, handle=None, what: str = "", batch=False):
     if status != 0:
         L = load()
         msg = L.agimp_status_string(status).decode()
         if handle:
-            detail = L.agimp_last_error(handle).decode()
+            detail = (L.agimp_batch_last_error if batch else L.agimp_last_error)(handle).decode()
             if detail:
                 msg += ": " + detail
         raise AgimpError("%s failed (%d): %s" % (what or "agimp call", status, msg))

@@ -1,0 +1,77 @@
+"""Batches of independent scenes stepped by shared launches (libagimp.so
+agimp_batch_*).  No counterpart in the reference: it runs one AdaptiveGIMP at a
+time.
+
+    sims = [scene.build() for scene in scenes]
+    batch = SceneBatch(sims)
+    batch.autotune(dt)          # optional: pick launch sizes by measurement
+    batch.substep(dt, 100)      # every simulator advances 100 substeps
+    x0 = sims[0].x_p.to_numpy() # readback stays per simulator
+"""
+from __future__ import annotations
+
+import ctypes
+
+from . import _capi
+from .simulator import _torch_stream
+
+
+class SceneBatch:
+    def __init__(self, sims, graphs=True):
+        self._L = _capi.load()
+        self.sims = list(sims)
+        arr = (ctypes.c_void_p * len(self.sims))(*[s._h for s in self.sims])
+        h = ctypes.c_void_p()
+        _capi.check(self._L.agimp_batch_create(arr, len(self.sims), ctypes.byref(h)), None, "agimp_batch_create")
+        self._h = h
+        self._L.agimp_batch_set_graphs(self._h, 1 if graphs else 0)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._L.agimp_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __len__(self):
+        return len(self.sims)
+
+    @property
+    def n_particles(self):
+        return sum(s.n_particles for s in self.sims)
+
+    def substep(self, dt0, n=1, stream=None):
+        st = stream if stream is not None else _torch_stream()
+        _capi.check(self._L.agimp_batch_substep(self._h, float(dt0), int(n), st), self._h, "batch substep", batch=True)
+
+    @property
+    def tuning(self):
+        t = _capi.Tuning()
+        _capi.check(self._L.agimp_batch_get_tuning(self._h, ctypes.byref(t)), self._h, "get tuning", batch=True)
+        return t.as_dict()
+
+    def set_tuning(self, chunk=256, ctas_per_sm=8):
+        t = _capi.Tuning(int(chunk), int(ctas_per_sm), 0.0)
+        _capi.check(self._L.agimp_batch_set_tuning(self._h, ctypes.byref(t)), self._h, "set tuning", batch=True)
+
+    def autotune(self, dt0, trials=5, stream=None):
+        t = _capi.Tuning()
+        st = stream if stream is not None else _torch_stream()
+        _capi.check(self._L.agimp_batch_autotune(self._h, float(dt0), int(trials), ctypes.byref(t), st), self._h,
+                    "batch autotune", batch=True)
+        return t.as_dict()
+
+    def profile_substep(self, dt0, stream=None):
+        """One substep of the whole batch with per-phase CUDA-event timing; {phase: ms}."""
+        ms = (ctypes.c_float * len(_capi.PHASES))()
+        st = stream if stream is not None else _torch_stream()
+        _capi.check(self._L.agimp_batch_profile_substep(self._h, float(dt0), ms, len(ms), st), self._h,
+                    "batch profile", batch=True)
+        return dict(zip(_capi.PHASES, list(ms)))
+
+    def kernels_per_substep(self):
+        return int(self._L.agimp_batch_kernels_per_substep(self._h))

@@ -14,8 +14,8 @@ ROOT = os.path.dirname(PKG)
 CSRC = os.path.join(ROOT, "csrc")
 INCLUDE = os.path.join(os.path.dirname(ROOT), "include")
 LIB = os.path.join(PKG, "libagimp.so")
-SOURCES = ["capi.cu", "topology.cu", "transfer.cu", "refine.cu", "noalloc.cu", "mlp.cu"]
-HEADERS = ["common.cuh", "umma.cuh"]
+SOURCES = ["capi.cu", "batch.cu", "topology.cu", "transfer.cu", "refine.cu", "noalloc.cu", "mlp.cu"]
+HEADERS = ["common.cuh", "umma.cuh", "sim.h"]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-O3", "--expt-relaxed-constexpr"]

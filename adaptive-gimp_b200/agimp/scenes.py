@@ -84,16 +84,13 @@ def band_level_map(boxes, dim, level, coarsest_size, near=2, mid=4, floor_y=0.25
     for lo, hi in boxes:
         sl = tuple(slice(int(np.floor(a * nc)), int(np.ceil(b * nc))) for a, b in zip(lo, hi))
         cov[sl] = True
-    dist = np.full(cov.shape, 1 << 20)
-    idx = np.argwhere(cov)
-    grid = np.stack(np.meshgrid(*[np.arange(nc)] * dim, indexing="ij"), -1)
-    for chunk in np.array_split(idx, max(1, len(idx) // 256)):
-        if len(chunk):
-            d = np.abs(grid[..., None, :] - chunk[None]).max(-1).min(-1)
-            dist = np.minimum(dist, d)
+    # Chebyshev distance <= k from a covered cell <=> inside a (2k+1)^dim box
+    from scipy.ndimage import maximum_filter
+    within_near = maximum_filter(cov, size=2 * near + 1, mode="constant", cval=False)
+    within_mid = maximum_filter(cov, size=2 * mid + 1, mode="constant", cval=False)
     y_center = (np.arange(nc) + 0.5) / nc
     ylow = np.broadcast_to(y_center.reshape((1, nc) + (1,) * (dim - 2)), cov.shape) < floor_y
-    coarse_lv = np.where((dist <= near) | ylow, level - 1, np.where(dist <= mid, max(level - 2, 0), 0))
+    coarse_lv = np.where(within_near | ylow, level - 1, np.where(within_mid, max(level - 2, 0), 0))
     sz = nc << (level - 1)
     s = level - 1
 
@@ -262,4 +259,57 @@ def make_config(k, seed=0, scale=1.0):
                           invalid_nodes="normalize"),
                      refine_every=10, refine_band=3,
                      description="3D 4 levels 64^3..512^3, two colliding snow spheres r=0.12 at +-2, E=1.4e5 rho=400")
+    if k == 4:
+        raise ValueError("config 4 is a batch of scenes: use make_batch_config()")
     raise ValueError("unknown config %r" % k)
+
+
+def _place_boxes(rng, sides, tries=200):
+    """Non-overlapping axis-aligned 2D boxes with the given (w, h) sides inside
+    [0.1, 0.9]^2 (rejection sampling; later boxes shrink if they do not fit)."""
+    placed = []
+    for w, h in sides:
+        for t in range(tries):
+            f = 1.0 if t < tries // 2 else 0.7
+            ww, hh = w * f, h * f
+            lo = rng.uniform([0.1, 0.1], [0.9 - ww, 0.9 - hh])
+            hi = lo + [ww, hh]
+            if all(np.any(hi <= a) or np.any(lo >= b) for a, b in placed):
+                placed.append((lo, hi))
+                break
+    return placed
+
+
+def make_batch_config(seed=0, n_scenes=256, scale=1.0):
+    """Config 4: independent 2D scenes for one batch.  Each scene draws its
+    level count from {2, 3, 4}, its finest resolution from {256, 512}, 1-3
+    boxes and a particle count from a lognormal clipped to [2k, 60k] (times
+    `scale`); the boxes share that count at 4 particles per finest cell.
+    Material, time step and level maps are config 1's (elastic, E=1e4 with
+    rho=100, sticky walls, dt=1e-4, static map: the finest level within 2
+    coarsest cells of a box or below y = 0.25)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(n_scenes):
+        L = int(rng.integers(2, 5))
+        fin = int(rng.choice([256, 512]))
+        c = fin >> (L - 1)
+        nbox = int(rng.integers(1, 4))
+        target = float(np.clip(rng.lognormal(np.log(12000.0), 0.8), 2000, 60000)) * scale
+        area = target / (4.0 * fin * fin)  # 4 particles per finest cell
+        shares = rng.dirichlet(np.ones(nbox)) * area
+        sides = []
+        for a in shares:
+            r = rng.uniform(0.5, 2.0)
+            w = float(np.sqrt(a * r))
+            sides.append((min(w, 0.7), min(a / w, 0.7)))
+        boxes = _place_boxes(rng, sides)
+        xs = [fill_lattice(rng, 2, fin, *box_region(lo, hi)) for lo, hi in boxes]
+        x = np.concatenate(xs) if xs else np.zeros((0, 2), np.float32)
+        n = len(x)
+        out.append(Scene("config4_scene%03d" % i, 2, L, c, x, np.zeros((n, 2), np.float32),
+                         np.full(n, L - 1, np.int32), _unit_mass(n), 1e-4, 1000,
+                         dict(E=1e4 / RHO[1], nu=0.2, gravity=(0.0, -9.8), boundary_mode="sticky"),
+                         grid_initializer=band_level_map([(tuple(lo), tuple(hi)) for lo, hi in boxes], 2, L, c),
+                         description="%d levels %d^2..%d^2, %d boxes, %d particles" % (L, c, fin, len(boxes), n)))
+    return out

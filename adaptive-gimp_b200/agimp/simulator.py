@@ -367,6 +367,27 @@ class AdaptiveGIMP:
         _capi.check(self._L.agimp_recorded(self._h, ctypes.byref(n), 1 if reset else 0), self._h, "recorded")
         return n.value
 
+    # -- launch tuning -----------------------------------------------------------
+    @property
+    def tuning(self):
+        t = _capi.Tuning()
+        _capi.check(self._L.agimp_get_tuning(self._h, ctypes.byref(t)), self._h, "get tuning")
+        return t.as_dict()
+
+    def set_tuning(self, chunk=256, ctas_per_sm=8):
+        """P2G work-item size (64, 128, 256) and grid-stride CTAs per SM."""
+        t = _capi.Tuning(int(chunk), int(ctas_per_sm), 0.0)
+        _capi.check(self._L.agimp_set_tuning(self._h, ctypes.byref(t)), self._h, "set tuning")
+
+    def autotune(self, dt0, trials=5, stream=None):
+        """Time every launch choice on the current state (restored afterwards),
+        keep the fastest and return it."""
+        t = _capi.Tuning()
+        st = stream if stream is not None else _torch_stream()
+        _capi.check(self._L.agimp_autotune(self._h, float(dt0), int(trials), ctypes.byref(t), st), self._h,
+                    "autotune")
+        return t.as_dict()
+
     def profile_substep(self, dt0, stream=None):
         """One substep with per-phase CUDA-event timing; returns {phase: ms}."""
         ms = (ctypes.c_float * len(_capi.PHASES))()

@@ -1,0 +1,342 @@
+// Batches of scenes: one launch per kernel for all scenes of a batch, under a
+// CUDA graph per step phase, with launch sizes chosen by a measuring
+// autotuner.  A single simulator steps through this same path as a batch of
+// one.
+//
+// Launch layout.  Each launch kind (grid-stride kernels, the bin allocator)
+// gives every scene a consecutive range of CTAs:
+//   grid-stride kernels (over particles, active blocks or work items):
+//     sms * ctas_per_sm CTAs shared in proportion to the scenes' particle
+//     counts (at least one each);
+//   bin allocator: a quarter of the scene's grid-stride CTAs (at least one).
+// The kernels find their scene by binary search over the range starts.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+#include "sim.h"
+
+namespace agimp {
+
+#define BCK(call)                                                            \
+  do {                                                                       \
+    cudaError_t e_ = (call);                                                 \
+    if (e_ != cudaSuccess) {                                                 \
+      b->err = std::string(#call) + ": " + cudaGetErrorString(e_);           \
+      return AGIMP_CUDA_ERROR;                                               \
+    }                                                                        \
+  } while (0)
+
+Ctx& sim_ctx(agimp_sim* s) {
+  s->c.P = s->buf[s->par];
+  s->c.Q = s->buf[1 - s->par];
+  return s->c;
+}
+
+agimp_status batch_init(agimp_batch* b) {
+  const int n = (int)b->sims.size();
+  b->device = b->sims[0]->device;
+  b->dim = b->sims[0]->c.dim;
+  b->sms = b->sims[0]->c.sms;
+  for (int k = 0; k < 2; ++k) {
+    BCK(cudaMalloc(&b->dctx[k], sizeof(Ctx) * n));
+    b->hctx[k].resize(n);
+    std::memset(b->hctx[k].data(), 0, sizeof(Ctx) * n);
+    b->hvalid[k].assign(n, 0);
+  }
+  BCK(cudaMalloc(&b->dofs, sizeof(int) * NMAP * (n + 1)));
+  b->hofs.assign(NMAP * (n + 1), 0);
+  if (!b->single) {
+    BCK(cudaStreamCreateWithFlags(&b->internal, cudaStreamNonBlocking));
+    BCK(cudaEventCreateWithFlags(&b->ev_in, cudaEventDisableTiming));
+    BCK(cudaEventCreateWithFlags(&b->ev_out, cudaEventDisableTiming));
+  }
+  return AGIMP_OK;
+}
+
+void batch_drop_graphs(agimp_batch* b) {
+  for (int k = 0; k < 2; ++k)
+    if (b->gexec[k]) {
+      cudaGraphExecDestroy(b->gexec[k]);
+      b->gexec[k] = nullptr;
+    }
+}
+
+void batch_free(agimp_batch* b) {
+  batch_drop_graphs(b);
+  for (int k = 0; k < 2; ++k)
+    if (b->dctx[k]) cudaFree(b->dctx[k]);
+  if (b->dofs) cudaFree(b->dofs);
+  if (b->internal) cudaStreamDestroy(b->internal);
+  if (b->ev_in) cudaEventDestroy(b->ev_in);
+  if (b->ev_out) cudaEventDestroy(b->ev_out);
+  b->dctx[0] = b->dctx[1] = nullptr;
+  b->dofs = nullptr;
+  b->internal = nullptr;
+  b->ev_in = b->ev_out = nullptr;
+}
+
+// CTA ranges of every launch kind (host copy in b->hofs, uploaded on `use`).
+static agimp_status build_maps(agimp_batch* b, cudaStream_t use) {
+  const int n = (int)b->sims.size();
+  long long sumN = 0;
+  for (agimp_sim* s : b->sims) sumN += s->c.N;
+  const long long G = (long long)b->sms * b->tune.ctas_per_sm;
+  int* Gm = b->hofs.data() + MAP_G * (n + 1);
+  int* O = b->hofs.data() + MAP_O * (n + 1);
+  Gm[0] = O[0] = 0;
+  for (int i = 0; i < n; ++i) {
+    const long long N = b->sims[i]->c.N;
+    const int cg = n == 1 ? (int)std::max<long long>(1, G)
+                          : (int)std::max<long long>(1, sumN ? (long long)std::llround((double)G * N / sumN) : 1);
+    Gm[i + 1] = Gm[i] + cg;
+    O[i + 1] = O[i] + std::max(1, cg / 4);
+  }
+  b->nct[MAP_G] = Gm[n];
+  b->nct[MAP_O] = O[n];
+  BCK(cudaMemcpyAsync(b->dofs, b->hofs.data(), sizeof(int) * b->hofs.size(), cudaMemcpyHostToDevice, use));
+  b->maps_valid = true;
+  return AGIMP_OK;
+}
+
+// Bring the device contexts of phase `ph` up to date with the scenes' state.
+static agimp_status sync_contexts(agimp_batch* b, int ph, float dt, cudaStream_t use) {
+  const int n = (int)b->sims.size();
+  int lo = n, hi = -1;
+  for (int i = 0; i < n; ++i) {
+    Ctx& c = sim_ctx(b->sims[i]);
+    c.dt = dt;
+    c.chunk = b->tune.chunk;
+    Ctx& h = b->hctx[ph][i];
+    if (!b->hvalid[ph][i] || std::memcmp(&h, &c, sizeof(Ctx)) != 0) {
+      std::memcpy(&h, &c, sizeof(Ctx));
+      b->hvalid[ph][i] = 1;
+      lo = std::min(lo, i);
+      hi = std::max(hi, i);
+    }
+  }
+  if (hi >= lo)
+    BCK(cudaMemcpyAsync(b->dctx[ph] + lo, b->hctx[ph].data() + lo, sizeof(Ctx) * (hi - lo + 1),
+                        cudaMemcpyHostToDevice, use));
+  return AGIMP_OK;
+}
+
+static BatchLaunch make_launch(agimp_batch* b, int ph) {
+  BatchLaunch bl;
+  const int n = (int)b->sims.size();
+  bl.b.ctx = b->dctx[ph];
+  bl.b.ofs = b->dofs;
+  bl.b.n = n;
+  bl.dim = b->dim;
+  bl.maxL = 1;
+  bl.any_dynamic = 0;
+  for (agimp_sim* s : b->sims) {
+    bl.maxL = std::max(bl.maxL, s->c.L);
+    if (!s->c.is_static) bl.any_dynamic = 1;
+  }
+  for (int k = 0; k < NMAP; ++k) bl.nct[k] = b->nct[k];
+  bl.chunk = b->tune.chunk;
+  bl.single = b->single ? &b->hctx[ph][0] : nullptr;
+  return bl;
+}
+
+static agimp_batch::Key launch_key(const BatchLaunch& bl, cudaStream_t use) {
+  agimp_batch::Key k;
+  std::memset(&k, 0, sizeof(k));
+  k.maxL = bl.maxL;
+  k.any_dynamic = bl.any_dynamic;
+  k.chunk = bl.chunk;
+  k.sur = bl.single && bl.single->sur && bl.single->plast == 1 && bl.single->N;
+  for (int i = 0; i < NMAP; ++i) k.nct[i] = bl.nct[i];
+  k.stream = use;
+  return k;
+}
+
+agimp_status batch_step(agimp_batch* b, float dt, int n, cudaStream_t use, cudaEvent_t* ev) {
+  BCK(cudaSetDevice(b->device));
+  if (!b->single)
+    for (agimp_sim* s : b->sims)
+      if (s->c.sur) {
+        b->err = "a batch of several scenes cannot use the surrogate return map";
+        return AGIMP_INVALID_ARG;
+      }
+  if (!b->maps_valid) {
+    const agimp_status st = build_maps(b, use);
+    if (st != AGIMP_OK) return st;
+  }
+  for (int i = 0; i < n; ++i) {
+    const int ph = b->single ? b->sims[0]->par : (int)(b->steps & 1);
+    agimp_status st = sync_contexts(b, ph, dt, use);
+    if (st != AGIMP_OK) return st;
+    const BatchLaunch bl = make_launch(b, ph);
+    if (ev || !b->graphs) {
+      launch_substep(bl, use, ev);
+      BCK(cudaGetLastError());
+    } else {
+      const agimp_batch::Key key = launch_key(bl, use);
+      if (!b->gexec[ph] || std::memcmp(&key, &b->gkey[ph], sizeof(key)) != 0) {
+        if (b->gexec[ph]) {
+          cudaGraphExecDestroy(b->gexec[ph]);
+          b->gexec[ph] = nullptr;
+        }
+        cudaGraph_t graph = nullptr;
+        BCK(cudaStreamBeginCapture(use, cudaStreamCaptureModeThreadLocal));
+        launch_substep(bl, use, nullptr);
+        BCK(cudaStreamEndCapture(use, &graph));
+        const cudaError_t e = cudaGraphInstantiate(&b->gexec[ph], graph, 0);
+        cudaGraphDestroy(graph);
+        BCK(e);
+        std::memcpy(&b->gkey[ph], &key, sizeof(key));
+      }
+      BCK(cudaGraphLaunch(b->gexec[ph], use));
+    }
+    for (agimp_sim* s : b->sims) {
+      s->par ^= 1;  // the new state is in the other buffer
+      s->substeps += 1;
+    }
+    b->steps += 1;
+  }
+  return AGIMP_OK;
+}
+
+int batch_kernels(agimp_batch* b) {
+  const BatchLaunch bl = make_launch(b, 0);
+  const Ctx& c = b->sims[0]->c;
+  return kernels_per_substep(bl) + ((b->single && c.sur && c.plast == 1 && c.N) ? 2 : 0);
+}
+
+agimp_status batch_set_tuning(agimp_batch* b, const agimp_tuning* t) {
+  if (!t || (t->chunk != 64 && t->chunk != 128 && t->chunk != 256) || t->ctas_per_sm < 1 || t->ctas_per_sm > 32) {
+    b->err = "tuning: chunk must be 64, 128 or 256 and ctas_per_sm in [1, 32]";
+    return AGIMP_INVALID_ARG;
+  }
+  b->tune.chunk = t->chunk;
+  b->tune.ctas_per_sm = t->ctas_per_sm;
+  b->tune.ms_per_substep = t->ms_per_substep;
+  b->maps_valid = false;
+  batch_drop_graphs(b);
+  return AGIMP_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Autotuner.  Every candidate (P2G work-item size x grid-stride CTAs per SM)
+// runs `trials` timed substeps after two warm-up substeps (which capture its
+// graphs) from the same saved particle state; the fastest is kept.  The saved
+// state is put back after each candidate, so tuning leaves the simulation
+// where it was.  The grid itself needs no restoring: every substep clears the
+// blocks the previous substep activated, whichever they were.
+namespace {
+
+struct Saved {
+  agimp_sim* s;
+  int par;
+  long long substeps;
+  int32_t err, rec;
+  char* data;  // particle arrays of buf[par]
+};
+
+size_t state_bytes(const agimp_sim* s) {
+  const size_t N = s->c.N, D = s->c.dim;
+  return (2 * D + 2 * D * D + 5) * N * 4;
+}
+
+template <class F>
+void for_each_array(agimp_sim* s, const Particles& P, F f) {
+  const size_t N = s->c.N, D = s->c.dim;
+  f(P.x, D * N * 4);
+  f(P.v, D * N * 4);
+  f(P.F, D * D * N * 4);
+  f(P.C, D * D * N * 4);
+  f(P.m, N * 4);
+  f(P.Jp, N * 4);
+  f(P.g, N * 4);
+  f(P.fl, N * 4);
+  f(P.id, N * 4);
+}
+
+}  // namespace
+
+agimp_status batch_autotune(agimp_batch* b, float dt, int trials, agimp_tuning* best, cudaStream_t use) {
+  BCK(cudaSetDevice(b->device));
+  if (trials < 1 || trials > 1000) {
+    b->err = "trials must be in [1, 1000]";
+    return AGIMP_INVALID_ARG;
+  }
+  size_t total = 0;
+  for (agimp_sim* s : b->sims) total += state_bytes(s);
+  char* scratch = nullptr;
+  BCK(cudaMalloc(&scratch, std::max<size_t>(total, 16)));
+  std::vector<Saved> saved;
+  size_t off = 0;
+  for (agimp_sim* s : b->sims) {
+    Saved v{s, s->par, s->substeps, 0, 0, scratch + off};
+    int32_t h[2];
+    cudaMemcpyAsync(&h[0], s->c.ctr + CTR_ERR, 4, cudaMemcpyDeviceToHost, use);
+    cudaMemcpyAsync(&h[1], s->c.ctr + CTR_REC, 4, cudaMemcpyDeviceToHost, use);
+    cudaStreamSynchronize(use);
+    v.err = h[0];
+    v.rec = h[1];
+    size_t o = 0;
+    for_each_array(s, s->buf[s->par], [&](const void* p, size_t nb) {
+      cudaMemcpyAsync(v.data + o, p, nb, cudaMemcpyDeviceToDevice, use);
+      o += nb;
+    });
+    off += state_bytes(s);
+    saved.push_back(v);
+  }
+  auto restore = [&]() {
+    for (Saved& v : saved) {
+      agimp_sim* s = v.s;
+      s->par = v.par;
+      s->substeps = v.substeps;
+      size_t o = 0;
+      for_each_array(s, s->buf[v.par], [&](void* p, size_t nb) {
+        cudaMemcpyAsync(p, v.data + o, nb, cudaMemcpyDeviceToDevice, use);
+        o += nb;
+      });
+      cudaMemcpyAsync(s->c.ctr + CTR_ERR, &v.err, 4, cudaMemcpyHostToDevice, use);
+      cudaMemcpyAsync(s->c.ctr + CTR_REC, &v.rec, 4, cudaMemcpyHostToDevice, use);
+    }
+    return cudaStreamSynchronize(use);
+  };
+  const agimp_tuning old = b->tune;
+  agimp_tuning top{0, 0, INFINITY};
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  agimp_status st = AGIMP_OK;
+  const int chunks[3] = {64, 128, 256};
+  const int cps[4] = {2, 4, 8, 16};
+  for (int ci = 0; ci < 3 && st == AGIMP_OK; ++ci)
+    for (int gi = 0; gi < 4 && st == AGIMP_OK; ++gi) {
+      agimp_tuning t{chunks[ci], cps[gi], 0.f};
+      st = batch_set_tuning(b, &t);
+      if (st == AGIMP_OK) st = batch_step(b, dt, 2, use, nullptr);
+      if (st != AGIMP_OK) break;
+      cudaEventRecord(e0, use);
+      st = batch_step(b, dt, trials, use, nullptr);
+      cudaEventRecord(e1, use);
+      const cudaError_t e = cudaEventSynchronize(e1);
+      float ms = 0.f;
+      if (e == cudaSuccess) cudaEventElapsedTime(&ms, e0, e1);
+      const cudaError_t r = restore();
+      if (st == AGIMP_OK && (e != cudaSuccess || r != cudaSuccess)) {
+        b->err = std::string("autotune: ") + cudaGetErrorString(e != cudaSuccess ? e : r);
+        st = AGIMP_CUDA_ERROR;
+      }
+      t.ms_per_substep = ms / trials;
+      if (st == AGIMP_OK && t.ms_per_substep < top.ms_per_substep) top = t;
+    }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(scratch);
+  if (st != AGIMP_OK) {
+    batch_set_tuning(b, &old);
+    return st;
+  }
+  st = batch_set_tuning(b, &top);
+  if (best) *best = top;
+  return st;
+}
+
+}  // namespace agimp

@@ -11,8 +11,7 @@
 #include <string>
 #include <vector>
 
-#include "../../include/agimp.h"
-#include "common.cuh"
+#include "sim.h"
 
 using namespace agimp;
 
@@ -20,41 +19,20 @@ namespace agimp {
 void mlp_buffers(const agimp_mlp* m, const void** packed, const float** P);
 }
 
-struct agimp_sim {
-  Ctx c;
-  Particles buf[2];  // particle state ping-pongs between the two buffers
-  int par = 0;       // buf[par] holds the current state
-  agimp_params p;
-  int device = 0;
-  std::string err;
-  std::vector<void*> allocs;
-  bool graphs = true;
-  cudaGraphExec_t gexec[2] = {nullptr, nullptr};  // one captured substep per parity
-  float g_dt[2] = {NAN, NAN};
-  cudaStream_t g_stream[2] = {nullptr, nullptr};
-  cudaStream_t internal = nullptr;
-  cudaEvent_t ev_in = nullptr, ev_out = nullptr;
-  float* staging = nullptr;
-  size_t staging_floats = 0;
-  int8_t* map_dev = nullptr;
-  long long substeps = 0;
-};
-
 namespace {
 
 // the simulator's kernel context with P = current state, Q = the other buffer
-Ctx& cur(agimp_sim* s) {
-  s->c.P = s->buf[s->par];
-  s->c.Q = s->buf[1 - s->par];
-  return s->c;
+Ctx& cur(agimp_sim* s) { return sim_ctx(s); }
+
+// captured substeps depend on the launch structure and the surrogate settings
+void drop_graphs(agimp_sim* s) {
+  if (s->self) batch_drop_graphs(s->self);
 }
 
-void drop_graphs(agimp_sim* s) {
-  for (int k = 0; k < 2; ++k)
-    if (s->gexec[k]) {
-      cudaGraphExecDestroy(s->gexec[k]);
-      s->gexec[k] = nullptr;
-    }
+// status of a batch call on the simulator's own batch, with its message
+agimp_status from_batch(agimp_sim* s, agimp_status st) {
+  if (st != AGIMP_OK) s->err = s->self->err;
+  return st;
 }
 
 agimp_status fail(agimp_sim* s, agimp_status st, const std::string& msg) {
@@ -318,7 +296,8 @@ agimp_status agimp_create(const agimp_params* p, int32_t device, agimp_sim** out
   AL(c.bin_start, tot_blocks + 1);
   cudaMemset(c.bin_count, 0, (tot_blocks + 1) * sizeof(int32_t));
   const long long N = c.N;
-  AL(c.chunks, N / CHUNK + tot_blocks + 2);
+  AL(c.chunks, N / MIN_CHUNK + tot_blocks + 2);
+  c.chunk = CHUNK;
   AL(c.bin_of, N + 1);
   AL(c.rank_of, N + 1);
   AL(c.perm, N + 1);
@@ -356,6 +335,13 @@ agimp_status agimp_create(const agimp_params* p, int32_t device, agimp_sim** out
     agimp_destroy(s);
     return AGIMP_CUDA_ERROR;
   }
+  s->self = new agimp_batch();
+  s->self->sims.push_back(s);
+  s->self->single = true;
+  if (batch_init(s->self) != AGIMP_OK) {
+    agimp_destroy(s);
+    return AGIMP_CUDA_ERROR;
+  }
   e = cudaDeviceSynchronize();
   if (e != cudaSuccess) {
     agimp_destroy(s);
@@ -369,7 +355,11 @@ agimp_status agimp_destroy(agimp_sim* s) {
   if (!s) return AGIMP_INVALID_ARG;
   cudaSetDevice(s->device);
   cudaDeviceSynchronize();
-  drop_graphs(s);
+  if (s->self) {
+    batch_free(s->self);
+    delete s->self;
+    s->self = nullptr;
+  }
   for (void* p : s->allocs) cudaFree(p);
   if (s->map_dev) cudaFree(s->map_dev);
   if (s->internal) cudaStreamDestroy(s->internal);
@@ -509,7 +499,8 @@ agimp_status agimp_clear_level_map(agimp_sim* s) {
 
 agimp_status agimp_set_graphs(agimp_sim* s, int32_t enable) {
   if (!s) return AGIMP_INVALID_ARG;
-  s->graphs = enable != 0;
+  s->self->graphs = enable != 0;
+  if (!s->self->graphs) drop_graphs(s);
   return AGIMP_OK;
 }
 
@@ -517,36 +508,7 @@ agimp_status agimp_substep(agimp_sim* s, float dt, int32_t n_steps, void* stream
   if (!s || n_steps < 0 || !std::isfinite(dt)) return fail(s, AGIMP_INVALID_ARG, "bad substep args");
   CK(cudaSetDevice(s->device));
   StreamUse su(s, stream);
-  for (int i = 0; i < n_steps; ++i) {
-    const int k = s->par;
-    Ctx& c = cur(s);
-    c.dt = dt;
-    if (!s->graphs) {
-      launch_substep(c, su.use);
-      CK(cudaGetLastError());
-    } else {
-      if (!s->gexec[k] || s->g_dt[k] != dt || s->g_stream[k] != su.use) {
-        if (s->gexec[k]) {
-          cudaGraphExecDestroy(s->gexec[k]);
-          s->gexec[k] = nullptr;
-        }
-        cudaGraph_t graph = nullptr;
-        CK(cudaStreamBeginCapture(su.use, cudaStreamCaptureModeThreadLocal));
-        launch_substep(c, su.use);
-        cudaError_t e = cudaStreamEndCapture(su.use, &graph);
-        if (e != cudaSuccess) return cuda_fail(s, e, "capture substep");
-        e = cudaGraphInstantiate(&s->gexec[k], graph, 0);
-        cudaGraphDestroy(graph);
-        if (e != cudaSuccess) return cuda_fail(s, e, "instantiate substep graph");
-        s->g_dt[k] = dt;
-        s->g_stream[k] = su.use;
-      }
-      CK(cudaGraphLaunch(s->gexec[k], su.use));
-    }
-    s->par ^= 1;  // the new state is in the other buffer
-    s->substeps += 1;
-  }
-  return AGIMP_OK;
+  return from_batch(s, batch_step(s->self, dt, n_steps, su.use, nullptr));
 }
 
 agimp_status agimp_refine_levels(agimp_sim* s, int32_t band, void* stream) {
@@ -649,7 +611,7 @@ agimp_status agimp_get_stats(agimp_sim* s, agimp_stats* out) {
 
 int32_t agimp_kernels_per_substep(const agimp_sim* s) {
   if (!s) return 0;
-  return kernels_per_substep(s->c) + ((s->c.sur && s->c.plast == 1 && s->c.N) ? 2 : 0);
+  return batch_kernels(s->self);
 }
 
 agimp_status agimp_set_surrogate(agimp_sim* s, const agimp_mlp* m, const float* xmax, float tol) {
@@ -706,16 +668,147 @@ agimp_status agimp_profile_substep(agimp_sim* s, float dt, float* ms, int32_t n,
   StreamUse su(s, stream);
   cudaEvent_t ev[PHASES + 1];
   for (int i = 0; i <= PHASES; ++i) CK(cudaEventCreate(&ev[i]));
-  Ctx& c = cur(s);
-  c.dt = dt;
-  launch_substep(c, su.use, ev);
-  s->par ^= 1;
-  cudaError_t e = cudaEventSynchronize(ev[PHASES]);
-  for (int i = 0; i < PHASES && e == cudaSuccess; ++i) e = cudaEventElapsedTime(&ms[i], ev[i], ev[i + 1]);
+  const agimp_status st = batch_step(s->self, dt, 1, su.use, ev);
+  cudaError_t e = st == AGIMP_OK ? cudaEventSynchronize(ev[PHASES]) : cudaSuccess;
+  for (int i = 0; i < PHASES && e == cudaSuccess && st == AGIMP_OK; ++i)
+    e = cudaEventElapsedTime(&ms[i], ev[i], ev[i + 1]);
   for (int i = 0; i <= PHASES; ++i) cudaEventDestroy(ev[i]);
+  if (st != AGIMP_OK) return from_batch(s, st);
   if (e != cudaSuccess) return cuda_fail(s, e, "profile substep");
-  s->substeps += 1;
   return AGIMP_OK;
+}
+
+// ---------------------------------------------------------------------------
+// launch tuning of one simulator
+agimp_status agimp_set_tuning(agimp_sim* s, const agimp_tuning* t) {
+  if (!s) return AGIMP_INVALID_ARG;
+  return from_batch(s, batch_set_tuning(s->self, t));
+}
+
+agimp_status agimp_get_tuning(const agimp_sim* s, agimp_tuning* t) {
+  if (!s || !t) return AGIMP_INVALID_ARG;
+  *t = s->self->tune;
+  return AGIMP_OK;
+}
+
+agimp_status agimp_autotune(agimp_sim* s, float dt, int32_t trials, agimp_tuning* best, void* stream) {
+  if (!s || !std::isfinite(dt)) return fail(s, AGIMP_INVALID_ARG, "bad autotune args");
+  CK(cudaSetDevice(s->device));
+  StreamUse su(s, stream);
+  return from_batch(s, batch_autotune(s->self, dt, trials, best, su.use));
+}
+
+// ---------------------------------------------------------------------------
+// batches of simulators
+static agimp_status bfail(agimp_batch* b, agimp_status st, const char* msg) {
+  if (b) b->err = msg;
+  return st;
+}
+
+// library work of a batch on the caller's stream, or on the batch's internal
+// stream ordered after / before the legacy default stream
+struct BatchStream {
+  agimp_batch* b;
+  cudaStream_t user, use;
+  BatchStream(agimp_batch* b_, void* stream) : b(b_), user((cudaStream_t)stream) {
+    use = user ? user : b->internal;
+    if (!user) {
+      cudaEventRecord(b->ev_in, 0);
+      cudaStreamWaitEvent(b->internal, b->ev_in, 0);
+    }
+  }
+  ~BatchStream() {
+    if (!user) {
+      cudaEventRecord(b->ev_out, b->internal);
+      cudaStreamWaitEvent(0, b->ev_out, 0);
+    }
+  }
+};
+
+agimp_status agimp_batch_create(agimp_sim* const* sims, int32_t n, agimp_batch** out) {
+  if (!sims || !out || n < 1 || n > (1 << 16)) return AGIMP_INVALID_ARG;
+  *out = nullptr;
+  for (int i = 0; i < n; ++i) {
+    if (!sims[i]) return AGIMP_INVALID_ARG;
+    if (sims[i]->device != sims[0]->device || sims[i]->c.dim != sims[0]->c.dim) return AGIMP_INVALID_ARG;
+    for (int j = 0; j < i; ++j)
+      if (sims[j] == sims[i]) return AGIMP_INVALID_ARG;
+  }
+  if (cudaSetDevice(sims[0]->device) != cudaSuccess) return AGIMP_CUDA_ERROR;
+  agimp_batch* b = new agimp_batch();
+  b->sims.assign(sims, sims + n);
+  b->single = false;
+  if (batch_init(b) != AGIMP_OK) {
+    batch_free(b);
+    delete b;
+    return AGIMP_CUDA_ERROR;
+  }
+  *out = b;
+  return AGIMP_OK;
+}
+
+agimp_status agimp_batch_destroy(agimp_batch* b) {
+  if (!b) return AGIMP_INVALID_ARG;
+  cudaSetDevice(b->device);
+  cudaDeviceSynchronize();
+  batch_free(b);
+  delete b;
+  return AGIMP_OK;
+}
+
+const char* agimp_batch_last_error(const agimp_batch* b) { return b ? b->err.c_str() : "null handle"; }
+
+agimp_status agimp_batch_substep(agimp_batch* b, float dt, int32_t n_steps, void* stream) {
+  if (!b || n_steps < 0 || !std::isfinite(dt)) return bfail(b, AGIMP_INVALID_ARG, "bad substep args");
+  if (cudaSetDevice(b->device) != cudaSuccess) return bfail(b, AGIMP_CUDA_ERROR, "cudaSetDevice failed");
+  BatchStream bs(b, stream);
+  return batch_step(b, dt, n_steps, bs.use, nullptr);
+}
+
+agimp_status agimp_batch_set_graphs(agimp_batch* b, int32_t enable) {
+  if (!b) return AGIMP_INVALID_ARG;
+  b->graphs = enable != 0;
+  if (!b->graphs) batch_drop_graphs(b);
+  return AGIMP_OK;
+}
+
+agimp_status agimp_batch_set_tuning(agimp_batch* b, const agimp_tuning* t) {
+  if (!b) return AGIMP_INVALID_ARG;
+  return batch_set_tuning(b, t);
+}
+
+agimp_status agimp_batch_get_tuning(const agimp_batch* b, agimp_tuning* t) {
+  if (!b || !t) return AGIMP_INVALID_ARG;
+  *t = b->tune;
+  return AGIMP_OK;
+}
+
+agimp_status agimp_batch_autotune(agimp_batch* b, float dt, int32_t trials, agimp_tuning* best, void* stream) {
+  if (!b || !std::isfinite(dt)) return bfail(b, AGIMP_INVALID_ARG, "bad autotune args");
+  if (cudaSetDevice(b->device) != cudaSuccess) return bfail(b, AGIMP_CUDA_ERROR, "cudaSetDevice failed");
+  BatchStream bs(b, stream);
+  return batch_autotune(b, dt, trials, best, bs.use);
+}
+
+agimp_status agimp_batch_profile_substep(agimp_batch* b, float dt, float* ms, int32_t n, void* stream) {
+  if (!b || !ms || n < PHASES || !std::isfinite(dt)) return bfail(b, AGIMP_INVALID_ARG, "bad profile args");
+  if (cudaSetDevice(b->device) != cudaSuccess) return bfail(b, AGIMP_CUDA_ERROR, "cudaSetDevice failed");
+  BatchStream bs(b, stream);
+  cudaEvent_t ev[PHASES + 1];
+  for (int i = 0; i <= PHASES; ++i)
+    if (cudaEventCreate(&ev[i]) != cudaSuccess) return bfail(b, AGIMP_CUDA_ERROR, "cudaEventCreate failed");
+  const agimp_status st = batch_step(b, dt, 1, bs.use, ev);
+  cudaError_t e = st == AGIMP_OK ? cudaEventSynchronize(ev[PHASES]) : cudaSuccess;
+  for (int i = 0; i < PHASES && e == cudaSuccess && st == AGIMP_OK; ++i)
+    e = cudaEventElapsedTime(&ms[i], ev[i], ev[i + 1]);
+  for (int i = 0; i <= PHASES; ++i) cudaEventDestroy(ev[i]);
+  if (st != AGIMP_OK) return st;
+  if (e != cudaSuccess) return bfail(b, AGIMP_CUDA_ERROR, cudaGetErrorString(e));
+  return AGIMP_OK;
+}
+
+int32_t agimp_batch_kernels_per_substep(const agimp_batch* b) {
+  return b ? batch_kernels(const_cast<agimp_batch*>(b)) : 0;
 }
 
 }  // extern "C"

@@ -26,7 +26,8 @@
 namespace agimp {
 
 constexpr int MAXL = 8;
-constexpr int CHUNK = 256;  // particles per P2G/G2P work item (= CTA size)
+constexpr int CHUNK = 256;      // largest P2G work item (particles of one bin) = largest P2G CTA
+constexpr int MIN_CHUNK = 64;   // smallest work item (sizes the work-item buffer)
 constexpr int HALO = 4;
 
 enum : uint32_t { ACT = 1u, GHO = 2u, TJ = 4u, CUL = 8u };
@@ -75,6 +76,7 @@ struct Ctx {
   int sms;  // multiprocessors of the device (grid-stride launch width)
   int is_static, gap, bmode, plast, ncol, map_h, map_n;
   int inv_norm;  // 1: normalise nodes that are not activated (extension)
+  int chunk;     // particles per P2G work item: 64, 128 or 256 (launch tuning)
   float radius, mu, la, theta_c, theta_s, xi, dt;
   float grav[3];
   double col[4][6];  // collider boxes, compared in double like the oracle
@@ -550,15 +552,79 @@ __host__ __device__ __forceinline__ void axis_weights(float t, float r, float* W
 }
 
 // ---------------------------------------------------------------------------
+// Batches.  One launch per kernel serves every scene of a batch (a single
+// simulator is a batch of one).  For each kind of launch the CTAs are cut into
+// consecutive ranges, one per scene; a CTA finds its scene by binary search
+// over the range starts and copies the scene's context into shared memory.
+enum { MAP_G = 0,  // grid-stride kernels over particles, active blocks or work items
+       MAP_O = 1,  // bin allocation (1024-thread CTAs)
+       NMAP = 2 };
+
+struct Batch {
+  const Ctx* ctx;  // [n] scene contexts in device memory
+  const int* ofs;  // [NMAP][n + 1] first CTA of each scene, per launch kind
+  int n;
+};
+
+// What the host needs to launch a batch's substep.
+struct BatchLaunch {
+  Batch b;
+  int dim;
+  int maxL;          // most levels of any scene (per-level launches run to it)
+  int nct[NMAP];     // CTAs of each launch kind
+  int chunk;         // P2G work-item size of every scene
+  int any_dynamic;   // some scene activates cells from g_p (runs k_mark_hier)
+  const Ctx* single; // host context of a single simulator (surrogate step), else null
+};
+
+// The calling CTA's scene: its context (copied to *sc), its rank among the
+// scene's CTAs and their number.  Every thread of the CTA must call it.
+template <int KIND>
+__device__ __forceinline__ const Ctx& scene_slice(const Batch& B, Ctx* sc, int& bid, int& nblk) {
+  const int* o = B.ofs + KIND * (B.n + 1);
+  const int cta = (int)blockIdx.x;
+  int lo = 0, hi = B.n - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (__ldg(&o[mid]) <= cta)
+      lo = mid;
+    else
+      hi = mid - 1;
+  }
+  bid = cta - __ldg(&o[lo]);
+  nblk = __ldg(&o[lo + 1]) - __ldg(&o[lo]);
+  const unsigned* src = (const unsigned*)(B.ctx + lo);
+  unsigned* dst = (unsigned*)sc;
+  for (int i = threadIdx.x; i < (int)(sizeof(Ctx) / 4); i += blockDim.x) dst[i] = __ldg(&src[i]);
+  __syncthreads();
+  return *sc;
+}
+
+// Kernel prologue: binds `c` (this CTA's scene), `bid_` and `nblk_`.
+#define SCENE_CTA(B, KIND)  \
+  __shared__ Ctx s_ctx_;    \
+  int bid_, nblk_;          \
+  const Ctx& c = scene_slice<KIND>(B, &s_ctx_, bid_, nblk_)
+
+// grid-stride loop over [0, n) across the CTAs of this CTA's scene
+#define SCENE_LOOP(i, n) \
+  for (long long i = bid_ * (long long)blockDim.x + threadIdx.x; i < (n); i += (long long)nblk_ * blockDim.x)
+
+// the same over the scene's particle slots, with a trip count uniform across
+// the CTA (for warp-collective bodies): p = p0 + threadIdx.x may be >= c.N
+#define SCENE_PARTICLES(p0) \
+  for (int p0 = bid_ * (int)blockDim.x; p0 < c.N; p0 += nblk_ * (int)blockDim.x)
+
+// ---------------------------------------------------------------------------
 // host-side launchers (defined in topology.cu / transfer.cu)
 // ev (optional): PHASES+1 events recorded at the phase boundaries
 constexpr int PHASES = 8;  // blocks, topology, binning, p2g, restrict, gridop, prolong, g2p
-void launch_substep(const Ctx& c, cudaStream_t s, cudaEvent_t* ev = nullptr);
+void launch_substep(const BatchLaunch& bl, cudaStream_t s, cudaEvent_t* ev = nullptr);
 void launch_refine(const Ctx& c, int band, cudaStream_t s);
 void prepare_transfer_kernels();  // kernel attributes (shared-memory opt-in); once per device
 // surrogate MLP forward over a device-side sample count (mlp.cu)
 void launch_mlp_forward_dev(const void* packed, const float* P, const float* X, float* Y, const int32_t* n_dev,
                             long long cap, int32_t* err, int sms, cudaStream_t s);
-int kernels_per_substep(const Ctx& c);
+int kernels_per_substep(const BatchLaunch& bl);
 
 }  // namespace agimp

@@ -1,0 +1,73 @@
+// Host-side state of a simulator (agimp_sim) and of a batch of simulators
+// stepped by shared launches (agimp_batch).  Internal to libagimp.so.
+#pragma once
+#include <string>
+#include <vector>
+
+#include "../../include/agimp.h"
+#include "common.cuh"
+
+struct agimp_batch;
+
+struct agimp_sim {
+  agimp::Ctx c;
+  agimp::Particles buf[2];  // particle state ping-pongs between the two buffers
+  int par = 0;              // buf[par] holds the current state
+  agimp_params p;
+  int device = 0;
+  std::string err;
+  std::vector<void*> allocs;
+  cudaStream_t internal = nullptr;
+  cudaEvent_t ev_in = nullptr, ev_out = nullptr;
+  float* staging = nullptr;
+  size_t staging_floats = 0;
+  int8_t* map_dev = nullptr;
+  long long substeps = 0;
+  agimp_batch* self = nullptr;  // the simulator as a batch of one (its substep path)
+};
+
+// Several simulators (scenes) stepped together: one launch per kernel serves
+// all of them.  The kernels read each scene's context from device memory, one
+// array per step phase (a scene's particle buffers alternate between steps);
+// the host keeps a copy of what the device holds and uploads only entries
+// that changed.
+struct agimp_batch {
+  struct Key {  // launch structure a captured substep holds
+    int maxL, any_dynamic, chunk, sur;
+    int nct[agimp::NMAP];
+    cudaStream_t stream;
+  };
+  std::vector<agimp_sim*> sims;
+  bool single = false;  // a simulator's own batch of one
+  int device = 0, dim = 2, sms = 148;
+  agimp_tuning tune{agimp::CHUNK, 8, 0.f};
+  bool graphs = true;
+  agimp::Ctx* dctx[2] = {nullptr, nullptr};
+  std::vector<agimp::Ctx> hctx[2];
+  std::vector<char> hvalid[2];
+  int* dofs = nullptr;  // [NMAP][n + 1]
+  std::vector<int> hofs;
+  int nct[agimp::NMAP] = {0, 0};
+  bool maps_valid = false;
+  cudaGraphExec_t gexec[2] = {nullptr, nullptr};
+  Key gkey[2];
+  long long steps = 0;
+  cudaStream_t internal = nullptr;  // used when the caller passes no stream (own batches only)
+  cudaEvent_t ev_in = nullptr, ev_out = nullptr;
+  std::string err;
+};
+
+namespace agimp {
+// The simulator's context with P = its current state, Q = the other buffer.
+Ctx& sim_ctx(agimp_sim* s);
+// Allocate a batch's device arrays for its simulators (b->sims, b->single set).
+agimp_status batch_init(agimp_batch* b);
+void batch_free(agimp_batch* b);
+void batch_drop_graphs(agimp_batch* b);
+// n substeps of every scene on `use`; with ev, one substep with phase events
+// and no graph.
+agimp_status batch_step(agimp_batch* b, float dt, int n, cudaStream_t use, cudaEvent_t* ev);
+int batch_kernels(agimp_batch* b);
+agimp_status batch_autotune(agimp_batch* b, float dt, int trials, agimp_tuning* best, cudaStream_t use);
+agimp_status batch_set_tuning(agimp_batch* b, const agimp_tuning* t);
+}  // namespace agimp

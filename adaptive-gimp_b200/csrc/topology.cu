@@ -19,9 +19,6 @@
 
 namespace agimp {
 
-#define GS_LOOP(i, n) \
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < (n); i += (long long)gridDim.x * blockDim.x)
-
 template <int D>
 __device__ __forceinline__ void cell_or(const Ctx& c, int l, const int* I, uint32_t bits) {
   const LevelDev& V = c.lev[l];
@@ -44,8 +41,9 @@ __device__ __forceinline__ uint32_t cell_get(const Ctx& c, int l, const int* I) 
 // Clear everything the previous substep wrote (its active blocks), reset the
 // per-substep counters.
 template <int D>
-__global__ void k_clear(Ctx c) {
-  if (blockIdx.x == 0 && threadIdx.x == 0) {
+__global__ void k_clear(Batch B) {
+  SCENE_CTA(B, MAP_G);
+  if (bid_ == 0 && threadIdx.x == 0) {
     c.ctr[CTR_TOUCH] = 0;
     c.ctr[CTR_BINCUR] = 0;
     c.ctr[CTR_CHUNKS] = 0;
@@ -54,7 +52,7 @@ __global__ void k_clear(Ctx c) {
     c.ctr[CTR_SURFB] = 0;
   }
   const long long tot = total_elems(c, 0, c.L, D);
-  GS_LOOP(e, tot) {
+  SCENE_LOOP(e, tot) {
     int l, loc;
     long long blk;
     decode_elem<D>(c, 0, c.L, e, l, blk, loc);
@@ -107,9 +105,9 @@ __device__ __forceinline__ int grid_init(const Ctx& c, const int* I) {
   return l;
 }
 
+// one particle slot p (may be >= N: the warp-collective part still runs)
 template <int D>
-__global__ void k_touch_activate(Ctx c) {
-  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void touch_one(const Ctx& c, int p) {
   const bool valid = p < c.N;
   float xp[D];
   bool esc = !valid;
@@ -175,6 +173,14 @@ __global__ void k_touch_activate(Ctx c) {
   }
 }
 
+template <int D>
+__global__ void k_touch_activate(Batch B) {
+  SCENE_CTA(B, MAP_G);
+  // the active-block counts were read by k_clear; k_dilate rebuilds them
+  if (bid_ == 0 && threadIdx.x < MAXL) c.ctr[CTR_LEVEL + threadIdx.x] = 0;
+  SCENE_PARTICLES(p0) touch_one<D>(c, p0 + (int)threadIdx.x);
+}
+
 // ---------------------------------------------------------------------------
 // Active-block lists: level l gets the blocks within R_l blocks of each
 // touched finest block (shifted to that level).  Dynamic activation, culling,
@@ -188,7 +194,8 @@ __device__ __forceinline__ int dilate_radius(const Ctx& c, int l) {
 }
 
 template <int D>
-__global__ void k_dilate(Ctx c) {
+__global__ void k_dilate(Batch B) {
+  SCENE_CTA(B, MAP_G);
   int per_level[MAXL];
   long long W = 0;
   for (int l = 0; l < c.L; ++l) {
@@ -198,7 +205,7 @@ __global__ void k_dilate(Ctx c) {
   }
   const long long tot = (long long)c.ctr[CTR_TOUCH] * W;
   const LevelDev& Vf = c.lev[c.L - 1];
-  GS_LOOP(e, tot) {
+  SCENE_LOOP(e, tot) {
     const int t = (int)(e / W);
     int r = (int)(e % W);
     int l = 0;
@@ -250,9 +257,11 @@ __global__ void k_dilate(Ctx c) {
 // ancestors at levels l0..l-1.  Only ACTIVATED bits are read and only CULLING
 // bits written, so all levels run in one pass.
 template <int D>
-__global__ void k_mark_hier(Ctx c) {
+__global__ void k_mark_hier(Batch B) {
+  SCENE_CTA(B, MAP_G);
+  if (c.is_static) return;  // static mode has no culling (adaptive_gimp.py:335-337)
   const long long tot = total_elems(c, 1, c.L, D);
-  GS_LOOP(e, tot) {
+  SCENE_LOOP(e, tot) {
     int l, loc;
     long long blk;
     decode_elem<D>(c, 1, c.L, e, l, blk, loc);
@@ -286,9 +295,10 @@ __global__ void k_mark_hier(Ctx c) {
 // (_activate_mask, adaptive_gimp.py:142-149).  The CULLING bit itself stays
 // set until the next substep clears the block; readback masks it out.
 template <int D>
-__global__ void k_resolve(Ctx c) {
+__global__ void k_resolve(Batch B) {
+  SCENE_CTA(B, MAP_G);
   const long long tot = total_elems(c, 0, c.L, D);
-  GS_LOOP(e, tot) {
+  SCENE_LOOP(e, tot) {
     int l, loc;
     long long blk;
     decode_elem<D>(c, 0, c.L, e, l, blk, loc);
@@ -329,9 +339,10 @@ __global__ void k_resolve(Ctx c) {
 // ---------------------------------------------------------------------------
 // _mark_ghost_and_T_junction for every level (adaptive_gimp.py:155-187).
 template <int D>
-__global__ void k_ghost_tj(Ctx c) {
+__global__ void k_ghost_tj(Batch B) {
+  SCENE_CTA(B, MAP_G);
   const long long tot = total_elems(c, 0, c.L, D);
-  GS_LOOP(e, tot) {
+  SCENE_LOOP(e, tot) {
     int l, loc;
     long long blk;
     decode_elem<D>(c, 0, c.L, e, l, blk, loc);
@@ -399,8 +410,7 @@ __global__ void k_ghost_tj(Ctx c) {
 // bins, so that every particle gets a slot in the new order.  The rank inside
 // the bin comes from a warp-aggregated atomic.
 template <int D>
-__global__ void k_bin(Ctx c) {
-  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void bin_one(const Ctx& c, int p) {
   const int lane = threadIdx.x & 31;
   int bin = -1;
   if (p < c.N) {
@@ -465,6 +475,12 @@ __global__ void k_bin(Ctx c) {
   }
 }
 
+template <int D>
+__global__ void k_bin(Batch B) {
+  SCENE_CTA(B, MAP_G);
+  SCENE_PARTICLES(p0) bin_one<D>(c, p0 + (int)threadIdx.x);
+}
+
 // ---------------------------------------------------------------------------
 // Bin storage: each CTA scans 1024 bins, reserves their particles and work
 // items with one atomic each, and writes the work-item descriptors.  Bins of
@@ -505,20 +521,22 @@ __device__ __forceinline__ int2 block_incl_scan2(int a, int b, int2* warp_sums) 
   return make_int2(a, b);
 }
 
-__global__ void __launch_bounds__(1024) k_offsets(Ctx c) {
+__global__ void __launch_bounds__(1024) k_offsets(Batch B) {
+  SCENE_CTA(B, MAP_O);
   __shared__ int2 warp_sums[32];
   __shared__ int2 s_base;
+  const int CH = c.chunk;
   long long nblk = 0;
   for (int q = 0; q < c.L; ++q) nblk += c.ctr[CTR_LEVEL + q];
   const long long nb = nblk + 1;  // block bins + the extra bin of particles without a level
-  for (long long t0 = (long long)blockIdx.x * blockDim.x; t0 < nb; t0 += (long long)gridDim.x * blockDim.x) {
+  for (long long t0 = (long long)bid_ * blockDim.x; t0 < nb; t0 += (long long)nblk_ * blockDim.x) {
     const long long b = t0 + threadIdx.x;
     int cnt = 0;
     if (b < nb) {
       cnt = c.bin_count[b];
       if (cnt) c.bin_count[b] = 0;
     }
-    const int nch = (cnt + CHUNK - 1) / CHUNK;
+    const int nch = (cnt + CH - 1) / CH;
     const int2 inc = block_incl_scan2(cnt, nch, warp_sums);
     if (threadIdx.x == blockDim.x - 1) {
       s_base.x = inc.x ? atomicAdd(&c.ctr[CTR_BINCUR], inc.x) : 0;
@@ -541,56 +559,54 @@ __global__ void __launch_bounds__(1024) k_offsets(Ctx c) {
       } else {
         c.ctr[CTR_UNBIN] = cnt;
       }
-      for (int j = 0; j < nch; ++j) c.chunks[ch0 + j] = make_int4(l, blk, start + j * CHUNK, min(CHUNK, cnt - j * CHUNK));
+      for (int j = 0; j < nch; ++j) c.chunks[ch0 + j] = make_int4(l, blk, start + j * CH, min(CH, cnt - j * CH));
     }
     __syncthreads();
   }
 }
 
-__global__ void k_scatter(Ctx c) {
-  const int p = blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >= c.N) return;
-  c.perm[c.bin_start[c.bin_of[p]] + c.rank_of[p]] = p;
+__global__ void k_scatter(Batch B) {
+  SCENE_CTA(B, MAP_G);
+  SCENE_LOOP(p, c.N) c.perm[c.bin_start[c.bin_of[p]] + c.rank_of[p]] = (int)p;
 }
 
 // ---------------------------------------------------------------------------
 // launch sequence (transfer kernels are in transfer.cu)
 template <int D>
-void launch_transfer(const Ctx& c, cudaStream_t s, cudaEvent_t* ev);
+void launch_transfer(const BatchLaunch& bl, cudaStream_t s, cudaEvent_t* ev);
 
 template <int D>
-static void run_topology(const Ctx& c, cudaStream_t s, cudaEvent_t* ev) {
-  const int G = c.sms * 8;
-  const int Gp = (c.N + 255) / 256;
+static void run_topology(const BatchLaunch& bl, cudaStream_t s, cudaEvent_t* ev) {
+  const Batch& B = bl.b;
+  const int G = bl.nct[MAP_G], Go = bl.nct[MAP_O];
   if (ev) cudaEventRecord(ev[0], s);
-  k_clear<D><<<G, 256, 0, s>>>(c);
-  cudaMemsetAsync(c.ctr + CTR_LEVEL, 0, MAXL * sizeof(int32_t), s);
-  if (Gp) k_touch_activate<D><<<Gp, 256, 0, s>>>(c);
-  k_dilate<D><<<G, 256, 0, s>>>(c);
+  k_clear<D><<<G, 256, 0, s>>>(B);
+  k_touch_activate<D><<<G, 256, 0, s>>>(B);
+  k_dilate<D><<<G, 256, 0, s>>>(B);
   if (ev) cudaEventRecord(ev[1], s);
-  if (!c.is_static) k_mark_hier<D><<<G, 256, 0, s>>>(c);
-  k_resolve<D><<<G, 256, 0, s>>>(c);
-  k_ghost_tj<D><<<G, 256, 0, s>>>(c);
+  if (bl.any_dynamic) k_mark_hier<D><<<G, 256, 0, s>>>(B);
+  k_resolve<D><<<G, 256, 0, s>>>(B);
+  k_ghost_tj<D><<<G, 256, 0, s>>>(B);
   if (ev) cudaEventRecord(ev[2], s);
-  if (Gp) k_bin<D><<<Gp, 256, 0, s>>>(c);
-  k_offsets<<<G / 4, 1024, 0, s>>>(c);
-  if (Gp) k_scatter<<<Gp, 256, 0, s>>>(c);
+  k_bin<D><<<G, 256, 0, s>>>(B);
+  k_offsets<<<Go, 1024, 0, s>>>(B);
+  k_scatter<<<G, 256, 0, s>>>(B);
   if (ev) cudaEventRecord(ev[3], s);
 }
 
-void launch_substep(const Ctx& c, cudaStream_t s, cudaEvent_t* ev) {
-  if (c.dim == 2) {
-    run_topology<2>(c, s, ev);
-    launch_transfer<2>(c, s, ev);
+void launch_substep(const BatchLaunch& bl, cudaStream_t s, cudaEvent_t* ev) {
+  if (bl.dim == 2) {
+    run_topology<2>(bl, s, ev);
+    launch_transfer<2>(bl, s, ev);
   } else {
-    run_topology<3>(c, s, ev);
-    launch_transfer<3>(c, s, ev);
+    run_topology<3>(bl, s, ev);
+    launch_transfer<3>(bl, s, ev);
   }
 }
 
-int kernels_per_substep(const Ctx& c) {
-  const int topo = 9 - (c.is_static ? 1 : 0) - (c.N ? 0 : 3);  // kernels (the memset node is not counted)
-  return topo + 3 + 2 * (c.L - 1);
+int kernels_per_substep(const BatchLaunch& bl) {
+  const int topo = 9 - (bl.any_dynamic ? 0 : 1);
+  return topo + 3 + 2 * (bl.maxL - 1);
 }
 
 }  // namespace agimp

@@ -7,11 +7,14 @@
 //   303-321 grid_prolongation -> k_prolong  (one launch per level, coarse->fine)
 //   252-275 g2p               -> k_g2p      (all levels in one launch)
 //
-// P2G/G2P: one CTA per work item = up to CHUNK particles of one bin (one 4^d
-// block of one level).  A bin's particles touch only the (4+2)^d nodes from
-// the block origin, so P2G accumulates into that tile in shared memory and
-// flushes it with one float4 atomic per touched node; G2P stages the same tile
-// of velocities in shared memory before gathering.
+// P2G: one CTA per work item = up to CH particles of one bin (one 4^d block of
+// one level).  A bin's particles touch only the (4+2)^d nodes from the block
+// origin, so P2G accumulates into that tile in shared memory and flushes it
+// with one float4 atomic per touched node.  G2P: one thread per particle slot
+// in bin order; neighbouring threads gather the same nodes through L1.
+//
+// Every kernel serves a batch of scenes (a single simulator is a batch of
+// one): each CTA works for the scene its launch range assigns it to.
 //
 // Restriction and prolongation are written as gathers (each destination node
 // sums its sources) instead of the reference's scatters, so they need no
@@ -20,8 +23,6 @@
 
 namespace agimp {
 
-#define GS_LOOP(i, n) \
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < (n); i += (long long)gridDim.x * blockDim.x)
 
 template <int D>
 struct Stencil {
@@ -64,7 +65,7 @@ __device__ __forceinline__ void chunk_origin(const LevelDev& V, long long blk, i
 }
 
 // ---------------------------------------------------------------------------
-// P2G (adaptive_gimp.py:230-250).  Per work item (up to CHUNK particles of one
+// P2G (adaptive_gimp.py:230-250).  Per work item (up to CH particles of one
 // 4^d block of one level):
 //  1. one thread per particle computes the scaled stress (utils.py:11-16,
 //     adaptive_gimp.py:240), its per-axis GIMP weights and gradients, m,
@@ -81,7 +82,7 @@ __device__ __forceinline__ void chunk_origin(const LevelDev& V, long long blk, i
 // Shared-memory atomics from different lanes of a warp never hit the same
 // node, which removes the serialisation of a per-particle scatter when many
 // particles share a cell (hundreds per cell on coarse levels).
-template <int D>
+template <int D, int CH>
 struct P2GLayout {
   static constexpr int NC = 1 << (2 * D);      // cells per block
   static constexpr int G3 = (D == 2) ? 9 : 27;  // stencil nodes
@@ -94,10 +95,9 @@ struct P2GLayout {
   //   float  [4(1+2D) ..] W[d][3], G[d][3]        per-axis weights / gradients
   static constexpr int OFF_WG = 4 * (1 + 2 * D);
   static constexpr int STRIDE = OFF_WG + ((6 * D + 3) & ~3);  // multiple of 4 floats
-  static constexpr int MAXTASK = NC + CHUNK / 32;
+  static constexpr int MAXTASK = NC + CH / 32;
   static constexpr size_t bytes() {
-    return sizeof(float) * ((size_t)CHUNK * STRIDE + 4 * TN) +
-           sizeof(int) * (3 * NC + 2 * CHUNK + 3 * MAXTASK + 4);
+    return sizeof(float) * ((size_t)CH * STRIDE + 4 * TN) + sizeof(int) * (3 * NC + CH + 3 * MAXTASK + 4);
   }
 };
 
@@ -141,18 +141,18 @@ __device__ __forceinline__ void p2g_node_term(const float* P, const int* n, floa
   }
 }
 
-template <int D>
-__global__ void __launch_bounds__(CHUNK, 4) k_p2g(Ctx c) {
-  using Y = P2GLayout<D>;
+template <int D, int CH>
+__global__ void __launch_bounds__(CH, 1024 / CH) k_p2g(Batch B) {
+  SCENE_CTA(B, MAP_G);
+  using Y = P2GLayout<D, CH>;
   extern __shared__ float dsm[];
-  float* pd = dsm;                              // [CHUNK][STRIDE]
-  float* tile = pd + CHUNK * Y::STRIDE;         // [4][TN]: p_x, p_y, p_z, m
+  float* pd = dsm;                              // [CH][STRIDE]
+  float* tile = pd + CH * Y::STRIDE;            // [4][TN]: p_x, p_y, p_z, m
   int* s_cnt = (int*)(tile + 4 * Y::TN);        // [NC]
   int* s_off = s_cnt + Y::NC;                   // [NC]
   int* s_tpre = s_off + Y::NC;                  // [NC]
-  int* s_sorted = s_tpre + Y::NC;               // [CHUNK]
-  int* s_unused = s_sorted + CHUNK;             // [CHUNK] (keeps the layout of bytes())
-  int* t_cell = s_unused + CHUNK;               // [MAXTASK]
+  int* s_sorted = s_tpre + Y::NC;               // [CH]
+  int* t_cell = s_sorted + CH;                  // [MAXTASK]
   int* t_start = t_cell + Y::MAXTASK;
   int* t_len = t_start + Y::MAXTASK;
   int* s_ntask = t_len + Y::MAXTASK;
@@ -163,7 +163,7 @@ __global__ void __launch_bounds__(CHUNK, 4) k_p2g(Ctx c) {
   const float r2 = 2.f * c.radius;
   const float kw = (D == 2) ? 1.f / (4.f * r2 * r2) : 1.f / (8.f * r2 * r2 * r2);
   const float kg = (D == 2) ? 1.f / (2.f * r2 * r2) : 1.f / (4.f * r2 * r2 * r2);
-  for (int ch = blockIdx.x; ch < nch; ch += gridDim.x) {
+  for (int ch = bid_; ch < nch; ch += nblk_) {
     const int4 wd = c.chunks[ch];
     const int l = wd.x;
     if (l < 0) continue;  // particles without a level: no transfer (uniform over the CTA)
@@ -177,23 +177,23 @@ __global__ void __launch_bounds__(CHUNK, 4) k_p2g(Ctx c) {
     const int i = threadIdx.x;
     int cell = -1;
     if (l >= 0 && i < wd.w) {
-      const int p = c.perm[wd.z + i];
+      const int p = __ldg(&c.perm[wd.z + i]);
       const long long N = c.N;
       const float inv = (float)(c.coarsest << l);
       const float dx = 1.f / inv;
       float xp[D], vp[D], F[D * D], Cm[D * D];
 #pragma unroll
       for (int d = 0; d < D; ++d) {
-        xp[d] = c.P.x[d * N + p];
-        vp[d] = c.P.v[d * N + p];
+        xp[d] = __ldg(&c.P.x[d * N + p]);
+        vp[d] = __ldg(&c.P.v[d * N + p]);
       }
 #pragma unroll
       for (int k = 0; k < D * D; ++k) {
-        F[k] = c.P.F[k * N + p];
-        Cm[k] = c.P.C[k * N + p];
+        F[k] = __ldg(&c.P.F[k * N + p]);
+        Cm[k] = __ldg(&c.P.C[k * N + p]);
       }
-      const float mp = c.P.m[p];
-      const float jp = c.plast == 1 ? c.P.Jp[p] : 1.f;
+      const float mp = __ldg(&c.P.m[p]);
+      const float jp = c.plast == 1 ? __ldg(&c.P.Jp[p]) : 1.f;
       float tc[D];
       cell = 0;
 #pragma unroll
@@ -375,12 +375,14 @@ __global__ void __launch_bounds__(CHUNK, 4) k_p2g(Ctx c) {
 // ---------------------------------------------------------------------------
 // grid_restriction(l) as a gather over coarse nodes K of level l-1.
 template <int D>
-__global__ void k_restrict(Ctx c, int l) {
+__global__ void k_restrict(Batch B, int l) {
+  SCENE_CTA(B, MAP_G);
+  if (l >= c.L) return;
   const LevelDev& Vc = c.lev[l - 1];
   const LevelDev& Vf = c.lev[l];
   const long long tot = (long long)c.ctr[CTR_LEVEL + l - 1] << (2 * D);
   const int lsz = Vf.size, l0sz = Vc.size;
-  GS_LOOP(e, tot) {
+  SCENE_LOOP(e, tot) {
     const long long blk = Vc.blist[e >> (2 * D)];
     const int loc = (int)(e & ((1 << (2 * D)) - 1));
     int K[D];
@@ -429,9 +431,10 @@ __global__ void k_restrict(Ctx c, int l) {
 // ---------------------------------------------------------------------------
 // grid_op (adaptive_gimp.py:277-287) for all levels.
 template <int D>
-__global__ void k_gridop(Ctx c) {
+__global__ void k_gridop(Batch B) {
+  SCENE_CTA(B, MAP_G);
   const long long tot = total_elems(c, 0, c.L, D);
-  GS_LOOP(e, tot) {
+  SCENE_LOOP(e, tot) {
     int l, loc;
     long long blk;
     decode_elem<D>(c, 0, c.L, e, l, blk, loc);
@@ -489,12 +492,14 @@ __global__ void k_gridop(Ctx c) {
 // other all-even nodes take the coincident coarse velocity if they are
 // activated and it is valid, else 0; the rest keep their value.
 template <int D>
-__global__ void k_prolong(Ctx c, int l) {
+__global__ void k_prolong(Batch B, int l) {
+  SCENE_CTA(B, MAP_G);
+  if (l >= c.L) return;
   const LevelDev& Vc = c.lev[l - 1];
   const LevelDev& Vf = c.lev[l];
   const long long tot = (long long)c.ctr[CTR_LEVEL + l] << (2 * D);
   const int lsz = Vf.size;
-  GS_LOOP(e, tot) {
+  SCENE_LOOP(e, tot) {
     const long long blk = Vf.blist[e >> (2 * D)];
     const int loc = (int)(e & ((1 << (2 * D)) - 1));
     int J[D];
@@ -734,8 +739,8 @@ __global__ void k_sur_finish(Ctx c) {
     }
     const long long N = c.N;
 #pragma unroll
-    for (int k = 0; k < D * D; ++k) c.Q.F[k * N + j] = F[k];
-    c.Q.Jp[j] = jp;
+    for (int k = 0; k < D * D; ++k) __stwb(&c.Q.F[k * N + j], F[k]);
+    __stwb(&c.Q.Jp[j], jp);
   }
 }
 
@@ -748,45 +753,43 @@ __device__ __forceinline__ void copy_particle(const Ctx& c, int p, int j) {
   const long long N = c.N;
 #pragma unroll
   for (int d = 0; d < D; ++d) {
-    c.Q.x[d * N + j] = c.P.x[d * N + p];
-    c.Q.v[d * N + j] = c.P.v[d * N + p];
+    __stwb(&c.Q.x[d * N + j], __ldg(&c.P.x[d * N + p]));
+    __stwb(&c.Q.v[d * N + j], __ldg(&c.P.v[d * N + p]));
   }
 #pragma unroll
   for (int k = 0; k < D * D; ++k) {
-    c.Q.F[k * N + j] = c.P.F[k * N + p];
-    c.Q.C[k * N + j] = c.P.C[k * N + p];
+    __stwb(&c.Q.F[k * N + j], __ldg(&c.P.F[k * N + p]));
+    __stwb(&c.Q.C[k * N + j], __ldg(&c.P.C[k * N + p]));
   }
-  c.Q.m[j] = c.P.m[p];
-  c.Q.Jp[j] = c.P.Jp[p];
-  c.Q.g[j] = c.P.g[p];
-  c.Q.id[j] = c.P.id[p];
-  c.Q.fl[j] = -1;
+  __stwb(&c.Q.m[j], __ldg(&c.P.m[p]));
+  __stwb(&c.Q.Jp[j], __ldg(&c.P.Jp[p]));
+  __stwb(&c.Q.g[j], __ldg(&c.P.g[p]));
+  __stwb(&c.Q.id[j], __ldg(&c.P.id[p]));
+  __stwb(&c.Q.fl[j], -1);
 }
 
+// One particle, slot j of this substep's bin order; the 3^d nodes come
+// through L1 (particles of a bin share a (4+2)^d node tile).
 template <int D>
-__global__ void __launch_bounds__(256, 3) k_g2p(Ctx c) {
-  // one thread per particle in bin order; the 3^d nodes come through L1
-  // (particles of a bin share a (4+2)^d node tile)
+__device__ __forceinline__ void g2p_one(const Ctx& c, int j) {
   const float pw = (D == 2) ? 0.25f : 0.125f;
   const float rd = (D == 2) ? c.radius * c.radius : c.radius * c.radius * c.radius;
   const long long N = c.N;
-  const int j = blockIdx.x * blockDim.x + threadIdx.x;
-  if (j >= c.N) return;
-  const int p = c.perm[j];
-  const int l = c.P.fl[p];
+  const int p = __ldg(&c.perm[j]);
+  const int l = __ldg(&c.P.fl[p]);
   if (l < 0) {
     copy_particle<D>(c, p, j);
     return;
   }
   float xp[D], F[D * D];
 #pragma unroll
-  for (int d = 0; d < D; ++d) xp[d] = c.P.x[d * N + p];
+  for (int d = 0; d < D; ++d) xp[d] = __ldg(&c.P.x[d * N + p]);
 #pragma unroll
-  for (int k = 0; k < D * D; ++k) F[k] = c.P.F[k * N + p];
-  const float mp = c.P.m[p];
-  const int gp = c.P.g[p];
-  const int idp = c.P.id[p];
-  float jp = c.plast == 1 ? c.P.Jp[p] : 1.f;
+  for (int k = 0; k < D * D; ++k) F[k] = __ldg(&c.P.F[k * N + p]);
+  const float mp = __ldg(&c.P.m[p]);
+  const int gp = __ldg(&c.P.g[p]);
+  const int idp = __ldg(&c.P.id[p]);
+  float jp = c.plast == 1 ? __ldg(&c.P.Jp[p]) : 1.f;
   const LevelDev& V = c.lev[l];
   const float inv = (float)(c.coarsest << l);
   const float dx = 1.f / inv;
@@ -830,11 +833,11 @@ __global__ void __launch_bounds__(256, 3) k_g2p(Ctx c) {
   }
 #pragma unroll
   for (int d = 0; d < D; ++d) {
-    c.Q.v[d * N + j] = nv[d];
-    c.Q.x[d * N + j] = xp[d] + c.dt * nv[d];
+    __stwb(&c.Q.v[d * N + j], nv[d]);
+    __stwb(&c.Q.x[d * N + j], xp[d] + c.dt * nv[d]);
   }
 #pragma unroll
-  for (int i = 0; i < D * D; ++i) c.Q.C[i * N + j] = G[i];
+  for (int i = 0; i < D * D; ++i) __stwb(&c.Q.C[i * N + j], G[i]);
   const float s = (c.dt * pw) / (rd * dx);
   float Fn[D * D];
 #pragma unroll
@@ -848,40 +851,67 @@ __global__ void __launch_bounds__(256, 3) k_g2p(Ctx c) {
     }
   if (c.plast == 1) snow_return_map<D>(c, Fn, jp, j);
 #pragma unroll
-  for (int i = 0; i < D * D; ++i) c.Q.F[i * N + j] = Fn[i];
-  c.Q.m[j] = mp;
-  c.Q.Jp[j] = jp;
-  c.Q.g[j] = gp;
-  c.Q.id[j] = idp;
-  c.Q.fl[j] = l;
-}
-
-// ---------------------------------------------------------------------------
-void prepare_transfer_kernels() {
-  cudaFuncSetAttribute(k_p2g<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)P2GLayout<2>::bytes());
-  cudaFuncSetAttribute(k_p2g<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)P2GLayout<3>::bytes());
+  for (int i = 0; i < D * D; ++i) __stwb(&c.Q.F[i * N + j], Fn[i]);
+  __stwb(&c.Q.m[j], mp);
+  __stwb(&c.Q.Jp[j], jp);
+  __stwb(&c.Q.g[j], gp);
+  __stwb(&c.Q.id[j], idp);
+  __stwb(&c.Q.fl[j], l);
 }
 
 template <int D>
-void launch_transfer(const Ctx& c, cudaStream_t s, cudaEvent_t* ev) {
-  const int G = c.sms * 8;
-  k_p2g<D><<<G, CHUNK, P2GLayout<D>::bytes(), s>>>(c);
+__global__ void __launch_bounds__(256, 3) k_g2p(Batch B) {
+  SCENE_CTA(B, MAP_G);
+  SCENE_LOOP(j, c.N) g2p_one<D>(c, (int)j);
+}
+
+// ---------------------------------------------------------------------------
+template <int D, int CH>
+static void set_p2g_smem() {
+  cudaFuncSetAttribute(k_p2g<D, CH>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)P2GLayout<D, CH>::bytes());
+}
+
+void prepare_transfer_kernels() {
+  set_p2g_smem<2, 64>();
+  set_p2g_smem<2, 128>();
+  set_p2g_smem<2, 256>();
+  set_p2g_smem<3, 64>();
+  set_p2g_smem<3, 128>();
+  set_p2g_smem<3, 256>();
+}
+
+template <int D>
+static void launch_p2g(const BatchLaunch& bl, cudaStream_t s) {
+  const int G = bl.nct[MAP_G];
+  switch (bl.chunk) {
+    case 64: k_p2g<D, 64><<<G, 64, P2GLayout<D, 64>::bytes(), s>>>(bl.b); break;
+    case 128: k_p2g<D, 128><<<G, 128, P2GLayout<D, 128>::bytes(), s>>>(bl.b); break;
+    default: k_p2g<D, 256><<<G, 256, P2GLayout<D, 256>::bytes(), s>>>(bl.b); break;
+  }
+}
+
+template <int D>
+void launch_transfer(const BatchLaunch& bl, cudaStream_t s, cudaEvent_t* ev) {
+  const int G = bl.nct[MAP_G];
+  launch_p2g<D>(bl, s);
   if (ev) cudaEventRecord(ev[4], s);
-  for (int l = c.L - 1; l >= 1; --l) k_restrict<D><<<G, 256, 0, s>>>(c, l);
+  for (int l = bl.maxL - 1; l >= 1; --l) k_restrict<D><<<G, 256, 0, s>>>(bl.b, l);
   if (ev) cudaEventRecord(ev[5], s);
-  k_gridop<D><<<G, 256, 0, s>>>(c);
+  k_gridop<D><<<G, 256, 0, s>>>(bl.b);
   if (ev) cudaEventRecord(ev[6], s);
-  for (int l = 1; l < c.L; ++l) k_prolong<D><<<G, 256, 0, s>>>(c, l);
+  for (int l = 1; l < bl.maxL; ++l) k_prolong<D><<<G, 256, 0, s>>>(bl.b, l);
   if (ev) cudaEventRecord(ev[7], s);
-  if (c.N) k_g2p<D><<<(c.N + 255) / 256, 256, 0, s>>>(c);
-  if (c.sur && c.plast == 1 && c.N) {
-    launch_mlp_forward_dev(c.mlp_packed, c.mlp_P, c.sur_X, c.sur_Y, c.ctr + CTR_SUR, c.N, c.ctr + CTR_ERR, c.sms, s);
-    k_sur_finish<D><<<c.sms * 8, 256, 0, s>>>(c);
+  k_g2p<D><<<G, 256, 0, s>>>(bl.b);
+  const Ctx* c = bl.single;
+  if (c && c->sur && c->plast == 1 && c->N) {
+    launch_mlp_forward_dev(c->mlp_packed, c->mlp_P, c->sur_X, c->sur_Y, c->ctr + CTR_SUR, c->N, c->ctr + CTR_ERR,
+                           c->sms, s);
+    k_sur_finish<D><<<c->sms * 8, 256, 0, s>>>(*c);
   }
   if (ev) cudaEventRecord(ev[8], s);
 }
 
-template void launch_transfer<2>(const Ctx&, cudaStream_t, cudaEvent_t*);
-template void launch_transfer<3>(const Ctx&, cudaStream_t, cudaEvent_t*);
+template void launch_transfer<2>(const BatchLaunch&, cudaStream_t, cudaEvent_t*);
+template void launch_transfer<3>(const BatchLaunch&, cudaStream_t, cudaEvent_t*);
 
 }  // namespace agimp

@@ -63,6 +63,7 @@ def parse():
                     help="snow return map through this trained surrogate (agimp.train_surrogate output); the line "
                          "then also reports the plain path's throughput and the position error against it")
     ap.add_argument("--sur-tol", type=float, default=1e-3, help="surrogate residual tolerance")
+    ap.add_argument("--no-autotune", action="store_true", help="config 4: keep the default launch sizes")
     return ap.parse_args()
 
 
@@ -206,9 +207,23 @@ def run_reference(a):
     if rank != 0:
         return
     from agimp import scenes
-    scene = scenes.make_config(a.config, scale=a.scale)
     threads = os.cpu_count() or 1
     budget = max(10.0, min(150.0, 2.0 * a.steps))
+    if a.config == 4:
+        sc = scenes.make_batch_config(scale=a.scale)
+        val, done, el, ns = cpu_oracle_batch(sc, budget, threads)
+        sample = "%d of the %d scenes one at a time, %d substeps each after 1 warm-up, %.1f s" % (ns, len(sc), done, el)
+        print(json.dumps({
+            "impl": "reference", "metric": METRIC, "value": val, "unit": METRIC, "n_gpus": a.gpus, "steps": done,
+            "warmup": 1, "ms_per_step": 1e3 * el / (done * ns), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "config4_batched_2d", "scenes": len(sc), "particles": sum(s.n for s in sc)},
+            "cpu_baseline": {"value": val, "unit": METRIC, "cores": threads, "kind": "port", "sample": sample},
+            "e2e": {"value": val, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "note": "the reference is Taichi code and Taichi cannot be installed offline; this arm runs the CPU "
+                    "restatement of its algorithm (oracle/oracle.cpp) with OpenMP on all host threads"}))
+        return
+    scene = scenes.make_config(a.config, scale=a.scale)
     val, done, el = cpu_oracle_run(scene, budget, threads, steps_cap=a.steps, warmup=min(a.warmup, 1))
     sample = "%s: %d substeps of the full %d-particle scene after %d warm-up, %.1f s" % (
         scene.name, done, scene.n, min(a.warmup, 1), el)
@@ -362,6 +377,214 @@ def run_agimp(a):
         print(json.dumps(out))
 
 
+def run_batch(a):
+    """Config 4: a batch of independent 2D scenes stepped by shared launches
+    (one launch per kernel for all scenes, one CUDA graph per substep), with
+    launch sizes from the autotuner; compared with the same scenes stepped one
+    at a time (each with its own graph)."""
+    import ctypes
+
+    import numpy as np
+    import torch
+
+    from agimp import scenes
+    from agimp.batch import SceneBatch
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    sc = scenes.make_batch_config(seed=rank, scale=a.scale)
+    dt = sc[0].dt
+    n_tot = sum(s.n for s in sc)
+    stream = torch.cuda.Stream()
+    st = ctypes.c_void_p(stream.cuda_stream)
+    sims = [s.build(device=local) for s in sc]
+    batch = SceneBatch(sims)
+    tuning = batch.autotune(dt, trials=3, stream=st) if not a.no_autotune else batch.tuning
+
+    def timed(step, clocks=None):
+        import contextlib
+        with torch.cuda.stream(stream):
+            for _ in range(a.warmup):
+                step()
+            torch.cuda.synchronize()
+            if dist:
+                dist.barrier()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            with (clocks or contextlib.nullcontext()):
+                e0.record(stream)
+                for _ in range(a.steps):
+                    step()
+                e1.record(stream)
+                torch.cuda.synchronize()
+            if dist:
+                dist.barrier()
+            return e0.elapsed_time(e1)
+
+    clk = Clocks(local)
+    ms = timed(lambda: batch.substep(dt, 1, stream=st), clk)
+    errors = [s.errors() for s in sims]
+    with torch.cuda.stream(stream):
+        prof = [batch.profile_substep(dt, stream=st) for _ in range(5)]
+    nb = sum(s.stats()["n_binned"] for s in sims)
+    # the same scenes one at a time, each through its own graph
+    alone = [s.build(device=local) for s in sc]
+
+    def one_at_a_time():
+        for s in alone:
+            s.substep(dt, stream=st)
+
+    ms_alone = timed(one_at_a_time)
+    # both runs took warmup + steps substeps; the batch ran 5 more for its profile
+    for s in alone:
+        with torch.cuda.stream(stream):
+            s.substep(dt, 5, stream=st)
+    torch.cuda.synchronize()
+    errs = []
+    for s, b in zip(alone, sims):
+        if s.n_particles:
+            errs.append(float(np.abs(s.x_p.to_numpy().astype(np.float64) - b.x_p.to_numpy()).max()))
+    for s in alone:
+        s.close()
+    ms_t = torch.tensor([ms, ms_alone], device="cuda")
+    if dist:
+        dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
+    ms_max, ms_alone_max = (float(v) for v in ms_t.tolist())
+    value = world * n_tot * a.steps / (ms_max / 1e3)
+    phases = {k: statistics.median(p[k] for p in prof) for k in prof[0]}
+    b_p2g, b_g2p = BYTES[(2, False)]
+    hbm, src = peaks()
+    dom = "p2g" if phases["p2g"] >= phases["g2p"] else "g2p"
+    dom_bytes = nb * (b_p2g if dom == "p2g" else b_g2p)
+    achieved = dom_bytes / (phases[dom] / 1e3) / 1e9
+    tr = profile_traffic("k_" + dom, "config4_batched")
+    roof = {"bound": "hbm", "kernel": "k_" + dom, "achieved": achieved, "peak": hbm, "peak_source": src,
+            "unit": "GB/s", "frac": achieved / hbm, "traffic": (tr * nb) if tr is not None else None,
+            "algorithmic_bytes": dom_bytes,
+            "p2g_g2p_combined_frac": (nb * (b_p2g + b_g2p) / ((phases["p2g"] + phases["g2p"]) / 1e3) / 1e9) / hbm}
+    levels = [s.level for s in sc]
+    out = {
+        "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
+        "ms_per_step": ms_max / a.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "config4_batched_2d", "scenes": len(sc), "particles": n_tot,
+                   "levels": {str(k): levels.count(k) for k in sorted(set(levels))},
+                   "particles_per_scene": [int(min(s.n for s in sc)), int(max(s.n for s in sc))],
+                   "dt": dt, "parallelism": "replicas" if world > 1 else "single",
+                   "l2": "inputs exceed L2 (particle state %.0f MB)" % (n_tot * 4 * 14 / 1e6),
+                   "description": "256 independent 2D scenes, 2-4 levels, finest 256^2 or 512^2, 1-3 elastic "
+                                  "boxes, lognormal 2k-60k particles, static level maps, one launch per kernel "
+                                  "for all scenes under a CUDA graph"},
+        "tuning": tuning,
+        "one_at_a_time": {"value": world * n_tot * a.steps / (ms_alone_max / 1e3),
+                          "ms_per_step": ms_alone_max / a.steps, "speedup_of_batch": ms_alone_max / ms_max,
+                          "position_error_vs_batch": {"max_over_scenes": max(errs), "median": float(np.median(errs)),
+                                                      "unit": "domain lengths"}},
+        "roofline": roof,
+        "phases_ms": phases,
+        "gpu_launches": a.steps * batch.kernels_per_substep(),
+        "clocks": clk.summary(),
+        "device_errors": int(np.bitwise_or.reduce(errors)),
+    }
+    if not a.no_e2e:
+        out["e2e"] = e2e_batch(a, sc, local)
+    if rank == 0 and world == 1 and not a.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        val, done, el, ns = cpu_oracle_batch(sc, a.cpu_seconds, threads)
+        out["cpu_baseline"] = {"value": val, "unit": METRIC, "cores": threads, "kind": "port",
+                               "sample": "%d of the %d scenes one at a time, %d substeps each, %.1f s, OpenMP"
+                                         % (ns, len(sc), done, el)}
+    batch.close()
+    for s in sims:
+        s.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(out))
+
+
+def cpu_oracle_batch(sc, seconds, threads, steps=3):
+    """The oracle stepping scenes one at a time (as the reference would), over
+    as many scenes as fit the time budget (setup and one warm-up substep per
+    scene untimed); returns (particle-substeps/s, substeps per scene, timed
+    seconds, scenes)."""
+    import numpy as np
+
+    import oracle as O
+    from agimp.simulator import tabulate_level_map
+    el, work, k = 0.0, 0, 0
+    for s in sc:
+        d, n = s.dim, s.n
+        sk = s.sim_kwargs
+        o = O.Oracle(d, s.level, s.coarsest, n, gravity=tuple(sk["gravity"]) + (0.0,), E=sk["E"], nu=sk["nu"],
+                     boundary_mode=1)
+        o.set_particles(s.x, s.v, np.tile(np.eye(d), (n, 1, 1)), np.zeros((n, d, d)), s.m, s.g)
+        t, H = tabulate_level_map(s.grid_initializer, d, s.level, s.coarsest)
+        o.set_level_map(t, H)
+        o.substep(s.dt, 1, threads)
+        t1 = time.perf_counter()
+        o.substep(s.dt, steps, threads)
+        el += time.perf_counter() - t1
+        work += n * steps
+        k += 1
+        if el >= seconds:
+            break
+    return work / el, steps, el, k
+
+
+def e2e_batch(a, sc, local):
+    """Same metric through the public API with host buffers: every scene is
+    uploaded from pinned host memory, then per substep the batch steps and
+    every scene's x_p is read back into pinned host memory."""
+    import numpy as np
+    import torch
+
+    from agimp.batch import SceneBatch
+    sims = [s.build(device=local) for s in sc]
+    batch = SceneBatch(sims)
+    hosts = []
+    for s in sc:
+        n, d = s.n, s.dim
+        h = {k: torch.empty(shape, dtype=torch.float32, pin_memory=True).numpy()
+             for k, shape in (("x", (n, d)), ("v", (n, d)), ("F", (n, d, d)), ("C", (n, d, d)), ("m", (n,)))}
+        h["g"] = torch.empty((n,), dtype=torch.int32, pin_memory=True).numpy()
+        h["x"][:] = s.x
+        h["v"][:] = s.v
+        h["F"][:] = np.eye(d, dtype=np.float32)
+        h["C"][:] = 0
+        h["m"][:] = s.m
+        h["g"][:] = s.g
+        h["out"] = torch.empty((n, d), dtype=torch.float32, pin_memory=True).numpy()
+        hosts.append(h)
+    n_tot = sum(s.n for s in sc)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for sim, h in zip(sims, hosts):
+        sim.set_particles(x=h["x"], v=h["v"], F=h["F"], C=h["C"], m=h["m"], g=h["g"])
+    for i in range(a.steps):
+        batch.substep(sc[0].dt)
+        for sim, h in zip(sims, hosts):
+            if sim.n_particles:
+                sim.x_p.to_numpy(out=h["out"])
+    torch.cuda.synchronize()
+    el = time.perf_counter() - t0
+    batch.close()
+    for s in sims:
+        s.close()
+    h2d = sum(s.n * 4 * (2 * 2 + 2 * 4 + 2) for s in sc)
+    return {"value": n_tot * a.steps / el, "unit": METRIC, "h2d_bytes_per_step": h2d / a.steps,
+            "d2h_bytes_per_step": n_tot * 2 * 4, "timing": "wall clock, host-synchronous readback of every scene "
+            "every substep", "note": "h2d is the one-time upload of the scenes spread over the timed substeps"}
+
+
 def e2e_run(a, scene, local, sur=None):
     """Same metric through the public API with host buffers: upload the scene
     from pinned host memory, then per substep call substep() and read x_p back
@@ -407,6 +630,8 @@ def main():
     a = parse()
     if a.impl == "reference":
         run_reference(a)
+    elif a.config == 4:
+        run_batch(a)
     else:
         run_agimp(a)
 

@@ -135,8 +135,10 @@ agimp_status agimp_clear_level_map(agimp_sim* s);
 
 /* Replaces AdaptiveGIMP.substep(dt0) (adaptive_gimp.py:323-352), run n_steps
  * times back to back.  Asynchronous on `stream`.  With graphs enabled (the
- * default) the substep is captured once per (dt, stream) as a CUDA graph and
- * replayed. */
+ * default) the substep is captured as a CUDA graph once per stream (and per
+ * particle buffer, which alternates between substeps) and replayed; dt and
+ * the other settings live in device memory, so changing them needs no new
+ * capture. */
 agimp_status agimp_substep(agimp_sim* s, float dt, int32_t n_steps, void* stream);
 agimp_status agimp_set_graphs(agimp_sim* s, int32_t enable);
 
@@ -233,6 +235,44 @@ agimp_status agimp_set_recorder(agimp_sim* s, float* X, float* T, int64_t capaci
 agimp_status agimp_recorded(agimp_sim* s, int64_t* count, int32_t reset);
 /* bit 0: a tensor-core completion wait timed out.  Synchronizes the device. */
 agimp_status agimp_mlp_errors(agimp_mlp* m, uint32_t* bits, int32_t clear);
+
+/* ---- Launch tuning (no counterpart in the reference: Taichi picks its own
+ * launch sizes).  Results do not depend on it beyond the order of float
+ * additions. */
+typedef struct agimp_tuning {
+  int32_t chunk;        /* particles per P2G work item (CTA size): 64, 128 or 256 */
+  int32_t ctas_per_sm;  /* CTAs of the grid-stride kernels per multiprocessor, 1..32 */
+  float ms_per_substep; /* the autotuner's measurement of this choice (else as set) */
+} agimp_tuning;
+agimp_status agimp_set_tuning(agimp_sim* s, const agimp_tuning* t);
+agimp_status agimp_get_tuning(const agimp_sim* s, agimp_tuning* t);
+/* Measure every (chunk, ctas_per_sm) in {64, 128, 256} x {2, 4, 8, 16}:
+ * two warm-up and `trials` timed substeps each, all from the current state,
+ * which is restored afterwards (the simulation does not advance).  Keeps and
+ * returns the fastest.  Synchronizes the stream. */
+agimp_status agimp_autotune(agimp_sim* s, float dt, int32_t trials, agimp_tuning* best, void* stream);
+
+/* ---- Batches (no counterpart in the reference).  Independent simulators on
+ * one device and of one dimension (any levels, sizes, particle counts, static
+ * or dynamic) stepped together: every kernel of the substep is launched once
+ * for all of them, and the sequence is captured as a CUDA graph.  Each
+ * simulator keeps its own state and readback; stepping a batch advances all
+ * of them by the same substeps, exactly as agimp_substep on each would (up to
+ * the order of float additions).  The simulators must outlive the batch; the
+ * surrogate return map is not available in batches of more than one. */
+typedef struct agimp_batch agimp_batch;
+agimp_status agimp_batch_create(agimp_sim* const* sims, int32_t n, agimp_batch** out);
+agimp_status agimp_batch_destroy(agimp_batch* b);
+const char* agimp_batch_last_error(const agimp_batch* b);
+agimp_status agimp_batch_substep(agimp_batch* b, float dt, int32_t n_steps, void* stream);
+agimp_status agimp_batch_set_graphs(agimp_batch* b, int32_t enable);
+agimp_status agimp_batch_set_tuning(agimp_batch* b, const agimp_tuning* t);
+agimp_status agimp_batch_get_tuning(const agimp_batch* b, agimp_tuning* t);
+/* As agimp_autotune, over the whole batch. */
+agimp_status agimp_batch_autotune(agimp_batch* b, float dt, int32_t trials, agimp_tuning* best, void* stream);
+int32_t agimp_batch_kernels_per_substep(const agimp_batch* b);
+/* As agimp_profile_substep, for one substep of the whole batch. */
+agimp_status agimp_batch_profile_substep(agimp_batch* b, float dt, float* ms, int32_t n, void* stream);
 
 #ifdef __cplusplus
 }

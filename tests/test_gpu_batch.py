@@ -1,0 +1,188 @@
+"""Batches (config 4 path) and launch tuning.
+
+* A batch of heterogeneous scenes (2-4 levels, 256^2-512^2, static maps, a
+  dynamic scene, an empty scene) stepped by shared launches matches the same
+  scenes stepped one at a time, and one of its scenes matches the oracle.
+* Every P2G work-item size and grid width gives the oracle's result.
+* The autotuner leaves the simulation where it was.
+"""
+import numpy as np
+import pytest
+
+import oracle as O
+from _gpu_util import gpu_state, have_gpu, oracle_kwargs
+
+pytestmark = [pytest.mark.gpu, pytest.mark.skipif(not have_gpu(), reason="needs a CUDA device")]
+
+
+def _batch_scenes():
+    from agimp import scenes
+    sc = scenes.make_batch_config(seed=5, n_scenes=5, scale=0.2)
+    sc.append(scenes.make_config(2, seed=1, scale=0.25))  # dynamic, 4 levels, snow
+    empty = scenes.make_batch_config(seed=6, n_scenes=1, scale=0.2)[0]
+    empty.x, empty.v, empty.g, empty.m = empty.x[:0], empty.v[:0], empty.g[:0], empty.m[:0]
+    sc.append(empty)
+    return sc
+
+
+def _step(sim, sc, i0, n):
+    for i in range(i0, i0 + n):
+        if sc.refine_every and i % sc.refine_every == 0:
+            sim.refine_levels(sc.refine_band)
+        sim.substep(sc.dt)
+
+
+def _oracles(scene):
+    from agimp.simulator import tabulate_level_map
+    d, n = scene.dim, scene.n
+    kw = oracle_kwargs(scene.sim_kwargs, d)
+    orcs = [O.Oracle(d, scene.level, scene.coarsest, n, f64=f, **kw) for f in (False, True)]
+    for o in orcs:
+        o.set_particles(scene.x, scene.v, np.tile(np.eye(d), (n, 1, 1)), np.zeros((n, d, d)), scene.m, scene.g)
+        if scene.grid_initializer is not None:
+            t, H = tabulate_level_map(scene.grid_initializer, d, scene.level, scene.coarsest)
+            o.set_level_map(t, H)
+    return orcs
+
+
+def _against_oracle(sim, scene, orcs):
+    g = gpu_state(sim)
+    p32, p64 = orcs[0].particles(), orcs[1].particles()
+    np.testing.assert_array_equal(g["fl"], p32["fl"])
+    disp = np.sqrt(((p64["x"] - scene.x) ** 2).sum(1).mean())
+    e_gpu = np.sqrt(((g["x"] - p32["x"]) ** 2).sum(1).mean()) / disp
+    e_floor = np.sqrt(((p32["x"] - p64["x"]) ** 2).sum(1).mean()) / disp
+    assert e_gpu <= max(10 * e_floor, 1e-3), (e_gpu, e_floor)
+
+
+def test_batch_matches_scenes_stepped_alone():
+    """Refinement rounds of the dynamic scene happen outside the batch step
+    (agimp_refine_levels on its simulator), at the same substeps in both runs."""
+    from agimp.batch import SceneBatch
+    sc = _batch_scenes()
+    dt = sc[0].dt
+    alone = [s.build() for s in sc]
+    together = [s.build() for s in sc]
+    batch = SceneBatch(together)
+    steps = 20
+    for i in range(steps):
+        for k, s in enumerate(sc):
+            if s.refine_every and i % s.refine_every == 0:
+                alone[k].refine_levels(s.refine_band)
+                together[k].refine_levels(s.refine_band)
+            alone[k].substep(dt)
+        batch.substep(dt)
+    for k, s in enumerate(sc):
+        a, b = gpu_state(alone[k]), gpu_state(together[k])
+        assert alone[k].errors() & ~2 == 0 and together[k].errors() & ~2 == 0
+        np.testing.assert_array_equal(a["fl"], b["fl"])
+        np.testing.assert_array_equal(a["g"], b["g"])
+        if s.n:
+            # float atomics: both runs differ from each other in the last bits only
+            assert np.abs(a["x"] - b["x"]).max() <= 1e-5, (k, np.abs(a["x"] - b["x"]).max())
+            assert np.abs(a["v"] - b["v"]).max() <= 1e-3 * max(1.0, np.abs(a["v"]).max())
+        assert together[k].stats()["substeps"] == steps
+    # 9 topology kernels (k_mark_hier included: one scene is dynamic), P2G,
+    # grid_op, G2P, and a restriction and a prolongation per level above 0
+    assert batch.kernels_per_substep() == 9 + 3 + 2 * (max(s.level for s in sc) - 1)
+    batch.close()
+    for s in alone + together:
+        s.close()
+
+
+def test_batched_scene_matches_oracle():
+    from agimp.batch import SceneBatch
+    sc = _batch_scenes()
+    k = int(np.argmax([s.level for s in sc[:5]]))  # a static scene with the most levels
+    sims = [s.build() for s in sc]
+    batch = SceneBatch(sims)
+    orcs = _oracles(sc[k])
+    for i in range(15):
+        batch.substep(sc[k].dt)
+        for o in orcs:
+            o.substep(sc[k].dt)
+    _against_oracle(sims[k], sc[k], orcs)
+    batch.close()
+    for s in sims:
+        s.close()
+
+
+@pytest.mark.parametrize("chunk,cps", [(64, 2), (128, 4), (256, 16), (64, 32)])
+@pytest.mark.parametrize("k,scale", [(1, 0.35), (3, 0.3)])
+def test_tuning_choices_match_oracle(chunk, cps, k, scale):
+    from agimp import scenes
+    scene = scenes.make_config(k, scale=scale)
+    sim = scene.build()
+    sim.set_tuning(chunk, cps)
+    assert sim.tuning["chunk"] == chunk and sim.tuning["ctas_per_sm"] == cps
+    orcs = _oracles(scene)
+    steps = 10
+    for i in range(steps):
+        if scene.refine_every and i % scene.refine_every == 0:
+            sim.refine_levels(scene.refine_band)
+            for o in orcs:
+                o.refine_levels(scene.refine_band)
+        sim.substep(scene.dt)
+        for o in orcs:
+            o.substep(scene.dt)
+    assert sim.errors() & ~2 == 0
+    _against_oracle(sim, scene, orcs)
+    sim.close()
+
+
+def test_autotune_restores_state_and_batch_autotune():
+    from agimp import scenes
+    from agimp.batch import SceneBatch
+    scene = scenes.make_config(3, scale=0.3)
+    sim = scene.build()
+    _step(sim, scene, 0, 5)
+    before = gpu_state(sim)
+    n0 = sim.stats()["substeps"]
+    best = sim.autotune(scene.dt, trials=2)
+    assert best["chunk"] in (64, 128, 256) and best["ctas_per_sm"] in (2, 4, 8, 16) and best["ms_per_substep"] > 0
+    assert sim.tuning["chunk"] == best["chunk"]
+    after = gpu_state(sim)
+    for key in before:
+        np.testing.assert_array_equal(before[key], after[key])
+    assert sim.stats()["substeps"] == n0
+    assert sim.errors() & ~2 == 0
+    _step(sim, scene, 5, 3)  # keeps stepping normally
+    assert sim.stats()["substeps"] == n0 + 3
+    sim.close()
+
+    sc = _batch_scenes()
+    sims = [s.build() for s in sc]
+    batch = SceneBatch(sims)
+    batch.substep(sc[0].dt, 3)
+    xs = [s.x_p.to_numpy() for s in sims]
+    t = batch.autotune(sc[0].dt, trials=2)
+    assert t["ms_per_substep"] > 0 and batch.tuning["chunk"] == t["chunk"]
+    for s, x in zip(sims, xs):
+        np.testing.assert_array_equal(s.x_p.to_numpy(), x)
+    batch.substep(sc[0].dt, 2)
+    batch.close()
+    for s in sims:
+        s.close()
+
+
+def test_batch_rejects_surrogate_and_mixed_dims():
+    from agimp import AgimpError, scenes
+    from agimp.batch import SceneBatch
+    from agimp.surrogate import MLP
+    a = scenes.make_config(2, scale=0.2).build()
+    b = scenes.make_config(2, seed=3, scale=0.2).build()
+    c3 = scenes.make_config(3, scale=0.2).build()
+    with pytest.raises(AgimpError):
+        SceneBatch([a, c3])
+    with pytest.raises(AgimpError):
+        SceneBatch([a, a])
+    batch = SceneBatch([a, b])
+    mlp = MLP()
+    a.set_surrogate(mlp, xmax=np.ones(7, np.float32), tol=0.1)
+    with pytest.raises(AgimpError):
+        batch.substep(5e-5)
+    a.set_surrogate(None)
+    batch.substep(5e-5)
+    batch.close()
+    for s in (a, b, c3):
+        s.close()

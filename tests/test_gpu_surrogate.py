@@ -109,44 +109,47 @@ def _gap(a, b):
                  for u, v in zip((a[0], a[1], np.log(a[2])), (b[0], b[1], np.log(b[2]))))
 
 
-def _within_floor(gap, floor, what):
+def _within_floor(gap, floors, what):
     # P2G accumulates with float atomics, so two runs of the same path differ
-    # in the last bits and the difference grows with the substeps: compare
-    # against the gap between two plain runs (10x, plus one f32 ulp of 1).
-    for g, f, name in zip(gap, floor, ("x", "F", "log Jp")):
-        assert g <= 10.0 * f + 1.2e-7, (what, name, g, f)
+    # in the last bits, and after the collision the difference grows by orders
+    # of magnitude within tens of substeps: compare against the larger gap
+    # between the reference run and two more plain runs (20x, plus one f32
+    # ulp of 1).
+    for k, name in enumerate(("x", "F", "log Jp")):
+        f = max(fl[k] for fl in floors)
+        assert gap[k] <= 20.0 * f + 1.2e-7, (what, name, gap[k], f)
 
 
 def test_rejected_predictions_reproduce_plain_path():
     from agimp.surrogate import MLP
     sc = _scene()
-    a, b, sur = sc.build(), sc.build(), sc.build()
+    a, b, b2, sur = sc.build(), sc.build(), sc.build(), sc.build()
     mlp = MLP(seed=1)  # untrained: its predictions break the residual test
     sur.set_surrogate(mlp, xmax=np.full(7, 1e6, np.float32), tol=1e-12)
-    for sim in (a, b, sur):
-        _run(sim, sc, 120)  # the boxes touch after about 70 substeps
+    for sim in (a, b, b2, sur):
+        _run(sim, sc, 90)  # the boxes touch after about 70 substeps
     st = sur.stats()
     assert st["n_surrogate"] > 0
     assert st["n_fallback"] == st["n_surrogate"], st
     assert a.errors() == 0 and sur.errors() == 0 and mlp.errors() == 0
     ref = _state(a)
-    _within_floor(_gap(_state(sur), ref), _gap(_state(b), ref), "all rejected")
-    for sim in (a, b, sur):
+    _within_floor(_gap(_state(sur), ref), [_gap(_state(b), ref), _gap(_state(b2), ref)], "all rejected")
+    for sim in (a, b, b2, sur):
         sim.close()
 
 
 def test_out_of_range_features_take_exact_path():
     from agimp.surrogate import MLP
     sc = _scene()
-    a, b, sur = sc.build(), sc.build(), sc.build()
+    a, b, b2, sur = sc.build(), sc.build(), sc.build(), sc.build()
     mlp = MLP(seed=2)
     sur.set_surrogate(mlp, xmax=np.full(7, 1e-9, np.float32), tol=0.5)  # nothing is in range
-    for sim in (a, b, sur):
-        _run(sim, sc, 100)
+    for sim in (a, b, b2, sur):
+        _run(sim, sc, 90)
     assert sur.stats()["n_surrogate"] == 0
     ref = _state(a)
-    _within_floor(_gap(_state(sur), ref), _gap(_state(b), ref), "out of range")
-    for sim in (a, b, sur):
+    _within_floor(_gap(_state(sur), ref), [_gap(_state(b), ref), _gap(_state(b2), ref)], "out of range")
+    for sim in (a, b, b2, sur):
         sim.close()
 
 

@@ -77,3 +77,29 @@ def test_band_level_map_is_aligned_to_coarse_cells():
     k = 1 << (s.level - 1)
     blocks = inner.reshape(s.coarsest, k, s.coarsest, k)
     assert np.all(blocks.min(axis=(1, 3)) == blocks.max(axis=(1, 3)))
+
+
+def test_batch_config_shapes():
+    """Config 4: 256 scenes, 2-4 levels, finest 256 or 512, 1-3 boxes that do
+    not overlap, lognormal particle counts clipped to [2k, 60k]."""
+    from agimp import scenes
+    sc = scenes.make_batch_config()
+    assert len(sc) == 256
+    n = np.array([s.n for s in sc])
+    assert n.min() >= 1900 and n.max() <= 61000  # the fill rounds the clipped target
+    assert 2e6 < n.sum() < 8e6
+    assert set(s.level for s in sc) == {2, 3, 4}
+    assert set(s.coarsest << (s.level - 1) for s in sc) == {256, 512}
+    for s in sc:
+        assert s.dim == 2 and s.dt == 1e-4 and s.grid_initializer is not None
+        assert np.all((s.x >= 0.1) & (s.x < 0.9))
+        # 4 particles per finest cell; boxes do not overlap, so only cells that
+        # two neighbouring boxes share at their edges hold more
+        fin = s.coarsest << (s.level - 1)
+        cells = np.floor(s.x * fin).astype(np.int64)
+        _, counts = np.unique(cells[:, 0] * fin + cells[:, 1], return_counts=True)
+        assert counts.max() <= 8 and (counts > 4).mean() < 0.02
+    # seeded: the same call gives the same scenes
+    again = scenes.make_batch_config(n_scenes=3)
+    for a, b in zip(sc[:3], again):
+        np.testing.assert_array_equal(a.x, b.x)
