@@ -72,74 +72,36 @@ __device__ __forceinline__ void chunk_origin(const LevelDev& V, long long blk, i
 //     a = m (v - C (tc+1)) and B = m C, and its base cell inside the block,
 //     and stores them in shared memory;
 //  2. the particles are counting-sorted by base cell in shared memory and cut
-//     into tasks of <= 32 particles of one cell;
-//  3. a warp takes a task with one lane per stencil node (3^d lanes; in 2D
-//     three lane groups take every third particle): all particles of a base
-//     cell touch the same nodes, so each lane sums its node's mass and
-//     momentum, w m and w (a + B n) + S grad w, over the task in registers;
+//     into tasks of <= TMAX particles of one cell;
+//  3. a lane owns one row of three stencil nodes (the last axis runs along
+//     the row; 3^(d-1) rows per cell) of one task, and a warp serves SLOTS
+//     tasks at once (3 in 3D, 10 in 2D).  All particles of a task share a base
+//     cell, so the lane sums w m and w (a + B n) + S grad w of its three nodes
+//     over the task's particles in registers: one read of a particle record
+//     serves three nodes, and the row's weight products are shared;
 //  4. each lane adds its sums once into the (4+2)^d node tile in shared
 //     memory; the tile is flushed with one float4 atomic per touched node.
-// Shared-memory atomics from different lanes of a warp never hit the same
-// node, which removes the serialisation of a per-particle scatter when many
-// particles share a cell (hundreds per cell on coarse levels).
 template <int D, int CH>
 struct P2GLayout {
-  static constexpr int NC = 1 << (2 * D);      // cells per block
-  static constexpr int G3 = (D == 2) ? 9 : 27;  // stencil nodes
-  static constexpr int NGROUP = 32 / G3;        // lane groups per warp
-  static constexpr int TN = (D == 2) ? 36 : 216;
-  // per-particle record, read by every lane of a task:
-  //   float4 [0]          (m, a_0, a_1, a_2)      a = m (v - C (tc + 1))
-  //   float4 [1 .. D]     rows of B = m C         (4th lane unused)
-  //   float4 [1+D .. 2D]  rows of the scaled stress S
-  //   float  [4(1+2D) ..] W[d][3], G[d][3]        per-axis weights / gradients
-  static constexpr int OFF_WG = 4 * (1 + 2 * D);
-  static constexpr int STRIDE = OFF_WG + ((6 * D + 3) & ~3);  // multiple of 4 floats
-  static constexpr int MAXTASK = NC + CH / 32;
+  static constexpr int NC = 1 << (2 * D);        // cells per block
+  static constexpr int ROWS = (D == 2) ? 3 : 9;   // node rows per stencil
+  static constexpr int SLOTS = 32 / ROWS;         // tasks served by one warp at once
+  static constexpr int TN = (D == 2) ? 36 : 216;  // nodes of the (4+2)^d tile
+  static constexpr int TMAX = 16;                 // particles per task
+  // per-particle record:
+  //   [0, 4)          m, a_0 .. a_{d-1}                 a = m (v - C (tc + 1))
+  //   [4, 4 + 2d^2)   B = m C (row-major), then the scaled stress S (row-major)
+  //   [OFF_WP, ..)    {W_k[n], G_k[n]} pairs, n = 0..2, for the axes k < d-1
+  //   [OFF_WL, +4)    W_{d-1}[0..2] (last axis), then [OFF_WL + 4, +4) G_{d-1}[0..2]
+  static constexpr int OFF_BS = 4;
+  static constexpr int OFF_WP = OFF_BS + ((2 * D * D + 3) & ~3);
+  static constexpr int OFF_WL = OFF_WP + ((6 * (D - 1) + 3) & ~3);
+  static constexpr int STRIDE = OFF_WL + 8;  // 3D 44, 2D 28 floats: 16-byte aligned records
+  static constexpr int MAXTASK = NC + CH / TMAX;
   static constexpr size_t bytes() {
     return sizeof(float) * ((size_t)CH * STRIDE + 4 * TN) + sizeof(int) * (3 * NC + CH + 3 * MAXTASK + 4);
   }
 };
-
-// One particle's contribution to the node at offset n of its base cell:
-// mass w m and momentum w (a + B n) + S grad w (adaptive_gimp.py:249-250).
-template <int D, class Y>
-__device__ __forceinline__ void p2g_node_term(const float* P, const int* n, float kw, float kg, float& am, float* ap) {
-  const float4* P4 = (const float4*)P;
-  const float* W = P + Y::OFF_WG;
-  const float* G = W + 3 * D;
-  float w, gw[D];
-  if (D == 2) {
-    const float wx = W[n[0]], wy = W[3 + n[1]];
-    w = wx * wy * kw;
-    gw[0] = G[n[0]] * wy * kg;
-    gw[1] = wx * G[3 + n[1]] * kg;
-  } else {
-    const float wx = W[n[0]], wy = W[3 + n[1]], wz = W[6 + n[2]];
-    const float wyz = wy * wz;
-    w = wx * wyz * kw;
-    gw[0] = G[n[0]] * wyz * kg;
-    gw[1] = wx * G[3 + n[1]] * wz * kg;
-    gw[2] = wx * wy * G[6 + n[2]] * kg;
-  }
-  const float4 ma = P4[0];
-  am += w * ma.x;
-  const float av[3] = {ma.y, ma.z, ma.w};
-#pragma unroll
-  for (int r = 0; r < D; ++r) {
-    const float4 Br = P4[1 + r];
-    const float4 Sr = P4[1 + D + r];
-    const float bb[3] = {Br.x, Br.y, Br.z};
-    const float ss[3] = {Sr.x, Sr.y, Sr.z};
-    float u = av[r];
-#pragma unroll
-    for (int b = 0; b < D; ++b) u += bb[b] * (float)n[b];
-    float s = 0.f;
-#pragma unroll
-    for (int b = 0; b < D; ++b) s += ss[b] * gw[b];
-    ap[r] += w * u + s;
-  }
-}
 
 template <int D, int CH>
 __global__ void __launch_bounds__(CH, 1024 / CH) k_p2g(Batch B) {
@@ -216,7 +178,6 @@ __global__ void __launch_bounds__(CH, 1024 / CH) k_p2g(Batch B) {
       const float diag = la * J * (J - 1.f);
       const float sc = (-c.dt * pw) / (rd * dx);
       float* P = pd + i * Y::STRIDE;
-      float4* P4 = (float4*)P;
       float a[D];
 #pragma unroll
       for (int r = 0; r < D; ++r) {
@@ -225,23 +186,29 @@ __global__ void __launch_bounds__(CH, 1024 / CH) k_p2g(Batch B) {
         for (int b = 0; b < D; ++b) cd += Cm[r * D + b] * (tc[b] + 1.f);
         a[r] = mp * (vp[r] - cd);
       }
-      P4[0] = make_float4(mp, a[0], a[1], D == 3 ? a[D - 1] : 0.f);
+      *(float4*)P = make_float4(mp, a[0], a[1], D == 3 ? a[D - 1] : 0.f);
 #pragma unroll
-      for (int r = 0; r < D; ++r) {
-        float s[3] = {0.f, 0.f, 0.f};
+      for (int r = 0; r < D; ++r)
 #pragma unroll
         for (int b = 0; b < D; ++b) {
           float acc = 0.f;
 #pragma unroll
           for (int k = 0; k < D; ++k) acc += (tmu * (F[r * D + k] - Rm[r * D + k])) * F[b * D + k];
-          s[b] = sc * (acc + (r == b ? diag : 0.f));
+          P[Y::OFF_BS + r * D + b] = mp * Cm[r * D + b];
+          P[Y::OFF_BS + D * D + r * D + b] = sc * (acc + (r == b ? diag : 0.f));
         }
-        P4[1 + r] = make_float4(mp * Cm[r * D], mp * Cm[r * D + 1], D == 3 ? mp * Cm[r * D + D - 1] : 0.f, 0.f);
-        P4[1 + D + r] = make_float4(s[0], s[1], s[2], 0.f);
-      }
 #pragma unroll
-      for (int d = 0; d < D; ++d)
-        axis_weights(tc[d], c.radius, P + Y::OFF_WG + 3 * d, P + Y::OFF_WG + 3 * D + 3 * d);
+      for (int d = 0; d < D; ++d) {
+        float W[3], G[3];
+        axis_weights(tc[d], c.radius, W, G);
+        if (d < D - 1) {
+#pragma unroll
+          for (int k = 0; k < 3; ++k) *(float2*)(P + Y::OFF_WP + 6 * d + 2 * k) = make_float2(W[k], G[k]);
+        } else {
+          *(float4*)(P + Y::OFF_WL) = make_float4(W[0], W[1], W[2], 0.f);
+          *(float4*)(P + Y::OFF_WL + 4) = make_float4(G[0], G[1], G[2], 0.f);
+        }
+      }
     }
     // rank inside the cell (warp-aggregated shared atomics)
     int rank = 0;
@@ -260,7 +227,7 @@ __global__ void __launch_bounds__(CH, 1024 / CH) k_p2g(Batch B) {
       for (int c0 = 0; c0 < Y::NC; c0 += 32) {
         const int cc = c0 + lane;
         const int n = cc < Y::NC ? s_cnt[cc] : 0;
-        const int nt = (n + 31) >> 5;
+        const int nt = (n + Y::TMAX - 1) / Y::TMAX;
         int ic = n, it = nt;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
@@ -283,70 +250,98 @@ __global__ void __launch_bounds__(CH, 1024 / CH) k_p2g(Batch B) {
     if (cell >= 0) s_sorted[s_off[cell] + rank] = i;
     for (int cc = threadIdx.x; cc < Y::NC; cc += blockDim.x) {
       const int n = s_cnt[cc];
-      for (int j = 0, t = s_tpre[cc]; j < n; j += 32, ++t) {
+      for (int j = 0, t = s_tpre[cc]; j < n; j += Y::TMAX, ++t) {
         t_cell[t] = cc;
         t_start[t] = s_off[cc] + j;
-        t_len[t] = min(32, n - j);
+        t_len[t] = min(Y::TMAX, n - j);
       }
     }
     __syncthreads();
-    // -- 3. tasks: lane <-> stencil node --------------------------------------
+    // -- 3. tasks: lane <-> row of three nodes ---------------------------------
     {
       const int ntask = *s_ntask;
-      const int g = lane / Y::G3, k = lane % Y::G3;
-      const bool on = g < Y::NGROUP;
-      int n[D];
-      {
-        int t = k;
-#pragma unroll
-        for (int d = D - 1; d >= 0; --d) {
-          n[d] = t % 3;
-          t /= 3;
-        }
-      }
-      for (int t = warp; t < ntask; t += nwarps) {
+      const int q = lane / Y::ROWS, row = lane % Y::ROWS;
+      const int n0 = (D == 2) ? row : row / 3, n1 = (D == 2) ? 0 : row % 3;
+      for (int t0 = warp * Y::SLOTS; t0 < ntask; t0 += nwarps * Y::SLOTS) {
+        const int t = t0 + q;
+        if (q >= Y::SLOTS || t >= ntask) continue;
         const int cc = t_cell[t], s0 = t_start[t], len = t_len[t];
-        float am = 0.f, ap[D];
+        float am[3], ap[3][D];
 #pragma unroll
-        for (int d = 0; d < D; ++d) ap[d] = 0.f;
-        if (on) {
-          // two particles per step: independent accumulators hide shared-memory latency
-          float am2 = 0.f, ap2[D];
+        for (int k = 0; k < 3; ++k) {
+          am[k] = 0.f;
 #pragma unroll
-          for (int d = 0; d < D; ++d) ap2[d] = 0.f;
-          int j = g;
-          for (; j + Y::NGROUP < len; j += 2 * Y::NGROUP) {
-            p2g_node_term<D, Y>(pd + s_sorted[s0 + j] * Y::STRIDE, n, kw, kg, am, ap);
-            p2g_node_term<D, Y>(pd + s_sorted[s0 + j + Y::NGROUP] * Y::STRIDE, n, kw, kg, am2, ap2);
-          }
-          if (j < len) p2g_node_term<D, Y>(pd + s_sorted[s0 + j] * Y::STRIDE, n, kw, kg, am, ap);
-          am += am2;
-#pragma unroll
-          for (int d = 0; d < D; ++d) ap[d] += ap2[d];
+          for (int d = 0; d < D; ++d) ap[k][d] = 0.f;
         }
-        if (Y::NGROUP > 1) {  // 2D: fold lane groups 1.. onto group 0 (sources read before any add)
-          __syncwarp();
-          float sm_ = 0.f, sp_[D];
+#pragma unroll 2
+        for (int j = 0; j < len; ++j) {
+          const float* R = pd + s_sorted[s0 + j] * Y::STRIDE;
+          const float4 ma = *(const float4*)R;
+          float bs[2 * D * D];
 #pragma unroll
-          for (int d = 0; d < D; ++d) sp_[d] = 0.f;
-#pragma unroll
-          for (int q = 1; q < Y::NGROUP; ++q) {
-            sm_ += __shfl_down_sync(0xffffffffu, am, q * Y::G3);
-#pragma unroll
-            for (int d = 0; d < D; ++d) sp_[d] += __shfl_down_sync(0xffffffffu, ap[d], q * Y::G3);
+          for (int k = 0; k < (2 * D * D + 3) / 4; ++k) {
+            const float4 v = *(const float4*)(R + Y::OFF_BS + 4 * k);
+            if (4 * k + 0 < 2 * D * D) bs[4 * k + 0] = v.x;
+            if (4 * k + 1 < 2 * D * D) bs[4 * k + 1] = v.y;
+            if (4 * k + 2 < 2 * D * D) bs[4 * k + 2] = v.z;
+            if (4 * k + 3 < 2 * D * D) bs[4 * k + 3] = v.w;
           }
-          am += sm_;
+          const float* Bm = bs;
+          const float* Sm = bs + D * D;
+          const float4 wl = *(const float4*)(R + Y::OFF_WL);
+          const float4 gl = *(const float4*)(R + Y::OFF_WL + 4);
+          const float wL[3] = {wl.x, wl.y, wl.z}, gL[3] = {gl.x, gl.y, gl.z};
+          // weight and gradient factors of the row (all axes but the last)
+          float cw, cg[D];
+          const float av[3] = {ma.y, ma.z, ma.w};
+          float u[D];
+          if (D == 2) {
+            const float2 wg0 = *(const float2*)(R + Y::OFF_WP + 2 * n0);
+            cw = wg0.x * kw;
+            cg[0] = wg0.y * kg;
+            cg[1] = wg0.x * kg;
 #pragma unroll
-          for (int d = 0; d < D; ++d) ap[d] += sp_[d];
+            for (int r = 0; r < D; ++r) u[r] = av[r] + Bm[r * D] * (float)n0;
+          } else {
+            const float2 wg0 = *(const float2*)(R + Y::OFF_WP + 2 * n0);
+            const float2 wg1 = *(const float2*)(R + Y::OFF_WP + 6 + 2 * n1);
+            const float wxy = wg0.x * wg1.x;
+            cw = wxy * kw;
+            cg[0] = wg0.y * wg1.x * kg;
+            cg[1] = wg0.x * wg1.y * kg;
+            cg[D - 1] = wxy * kg;
+#pragma unroll
+            for (int r = 0; r < D; ++r) u[r] = av[r] + Bm[r * D] * (float)n0 + Bm[r * D + 1] * (float)n1;
+          }
+#pragma unroll
+          for (int k = 0; k < 3; ++k) {
+            // node n_{d-1} = k of the row
+            const float w = cw * wL[k];
+            float gw[D];
+#pragma unroll
+            for (int b = 0; b < D - 1; ++b) gw[b] = cg[b] * wL[k];
+            gw[D - 1] = cg[D - 1] * gL[k];
+            am[k] += w * ma.x;
+#pragma unroll
+            for (int r = 0; r < D; ++r) {
+              const float ur = u[r] + Bm[r * D + D - 1] * (float)k;
+              float sv = 0.f;
+#pragma unroll
+              for (int b = 0; b < D; ++b) sv += Sm[r * D + b] * gw[b];
+              ap[k][r] += w * ur + sv;
+            }
+          }
         }
-        if (g == 0) {
-          int ti = 0;
+        int ti = 0;
 #pragma unroll
-          for (int d = 0; d < D; ++d) ti = ti * 6 + ((cc >> (2 * (D - 1 - d))) & 3) + n[d];
-          if (am != 0.f) atomicAdd(&tile[3 * Y::TN + ti], am);
+        for (int d = 0; d < D - 1; ++d) ti = ti * 6 + ((cc >> (2 * (D - 1 - d))) & 3) + (d == 0 ? n0 : n1);
+        ti = ti * 6 + (cc & 3);
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+          if (am[k] != 0.f) atomicAdd(&tile[3 * Y::TN + ti + k], am[k]);
 #pragma unroll
           for (int d = 0; d < D; ++d)
-            if (ap[d] != 0.f) atomicAdd(&tile[d * Y::TN + ti], ap[d]);
+            if (ap[k][d] != 0.f) atomicAdd(&tile[d * Y::TN + ti + k], ap[k][d]);
         }
       }
     }
