@@ -130,9 +130,11 @@ static BatchLaunch make_launch(agimp_batch* b, int ph) {
   bl.dim = b->dim;
   bl.maxL = 1;
   bl.any_dynamic = 0;
+  bl.any_plastic = 0;
   for (agimp_sim* s : b->sims) {
     bl.maxL = std::max(bl.maxL, s->c.L);
     if (!s->c.is_static) bl.any_dynamic = 1;
+    if (s->c.plast == 1) bl.any_plastic = 1;
   }
   for (int k = 0; k < NMAP; ++k) bl.nct[k] = b->nct[k];
   bl.chunk = b->tune.chunk;
@@ -145,6 +147,7 @@ static agimp_batch::Key launch_key(const BatchLaunch& bl, cudaStream_t use) {
   std::memset(&k, 0, sizeof(k));
   k.maxL = bl.maxL;
   k.any_dynamic = bl.any_dynamic;
+  k.any_plastic = bl.any_plastic;
   k.chunk = bl.chunk;
   k.sur = bl.single && bl.single->sur && bl.single->plast == 1 && bl.single->N;
   for (int i = 0; i < NMAP; ++i) k.nct[i] = bl.nct[i];

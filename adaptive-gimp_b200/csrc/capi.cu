@@ -270,6 +270,11 @@ agimp_status agimp_create(const agimp_params* p, int32_t device, agimp_sim** out
     V.nb = V.size / 4 + 3;
     V.nblocks = 1;
     for (int d = 0; d < D; ++d) V.nblocks *= V.nb;
+    if (V.nblocks * per > 0x7fffffffLL) {  // element indices are 32-bit in the kernels
+      s->err = "lattice too large: a level holds more than 2^31 stored elements";
+      agimp_destroy(s);
+      return AGIMP_CAPACITY;
+    }
     tot_blocks += V.nblocks;
     AL(V.cell, V.nblocks * per);
     AL(V.node, V.nblocks * per);
@@ -301,6 +306,7 @@ agimp_status agimp_create(const agimp_params* p, int32_t device, agimp_sim** out
   AL(c.bin_of, N + 1);
   AL(c.rank_of, N + 1);
   AL(c.perm, N + 1);
+  AL(c.proj, N + 1);
   for (int k = 0; k < 2; ++k) {
     Particles& P = s->buf[k];
     AL(P.x, D * N + 1);

@@ -45,6 +45,7 @@ enum {
   CTR_REC = 14,    // recorded (features, projected state) pairs since the recorder was armed
   CTR_SURFB = 15,  // surrogate predictions rejected (exact return map used instead)
   // [16, 22): particle bounding box used by the refinement rule
+  CTR_PROJ = 22,   // particles whose trial state needs the return map this substep
   CTR_COUNT = 24
 };
 
@@ -91,6 +92,7 @@ struct Ctx {
   int32_t* bin_of;
   int32_t* rank_of;
   int32_t* perm;
+  int32_t* proj;  // [N] slots of the particles listed for the return map (CTR_PROJ of them)
   // Particle state, SoA.  P holds the state the substep starts from, in the
   // bin order of the previous substep; G2P writes the new state into Q in this
   // substep's bin order (the host swaps P and Q between substeps).
@@ -146,34 +148,38 @@ __device__ __forceinline__ bool in_store(const LevelDev& V, const int* I) {
   return true;
 }
 
+// Element and block indices fit in 32 bits (agimp_create rejects lattices of
+// more than 2^31 elements per level), so the index arithmetic is 32-bit.
 template <int D>
 __device__ __forceinline__ long long elem_of(const LevelDev& V, const int* I) {
-  long long b = 0;
-  int loc = 0;
+  unsigned b = 0, loc = 0;
 #pragma unroll
   for (int d = 0; d < D; ++d) {
-    int a = I[d] + HALO;
-    b = b * V.nb + (a >> 2);
-    loc = (loc << 2) | (a & 3);
+    const unsigned a = (unsigned)(I[d] + HALO);
+    b = b * (unsigned)V.nb + (a >> 2);
+    loc = (loc << 2) | (a & 3u);
   }
-  return (b << (2 * D)) | loc;
+  return (long long)((b << (2 * D)) | loc);
 }
 
 template <int D>
 __device__ __forceinline__ long long block_of(const LevelDev& V, const int* I) {
-  long long b = 0;
+  unsigned b = 0;
 #pragma unroll
-  for (int d = 0; d < D; ++d) b = b * V.nb + ((I[d] + HALO) >> 2);
-  return b;
+  for (int d = 0; d < D; ++d) b = b * (unsigned)V.nb + ((unsigned)(I[d] + HALO) >> 2);
+  return (long long)b;
 }
 
 // element coordinates of local index `loc` in stored block `blk`
 template <int D>
 __device__ __forceinline__ void elem_coords(const LevelDev& V, long long blk, int loc, int* I) {
+  unsigned b = (unsigned)blk;
+  const unsigned nb = (unsigned)V.nb;
 #pragma unroll
   for (int d = D - 1; d >= 0; --d) {
-    int bd = (int)(blk % V.nb);
-    blk /= V.nb;
+    const unsigned q = b / nb;
+    const int bd = (int)(b - q * nb);
+    b = q;
     I[d] = (bd << 2) + ((loc >> (2 * (D - 1 - d))) & 3) - HALO;
   }
 }
@@ -574,6 +580,7 @@ struct BatchLaunch {
   int nct[NMAP];     // CTAs of each launch kind
   int chunk;         // P2G work-item size of every scene
   int any_dynamic;   // some scene activates cells from g_p (runs k_mark_hier)
+  int any_plastic;   // some scene has snow plasticity (runs k_project)
   const Ctx* single; // host context of a single simulator (surrogate step), else null
 };
 

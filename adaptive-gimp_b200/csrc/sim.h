@@ -33,7 +33,7 @@ struct agimp_sim {
 // that changed.
 struct agimp_batch {
   struct Key {  // launch structure a captured substep holds
-    int maxL, any_dynamic, chunk, sur;
+    int maxL, any_dynamic, any_plastic, chunk, sur;
     int nct[agimp::NMAP];
     cudaStream_t stream;
   };

@@ -50,6 +50,7 @@ __global__ void k_clear(Batch B) {
     c.ctr[CTR_UNBIN] = 0;
     c.ctr[CTR_SUR] = 0;
     c.ctr[CTR_SURFB] = 0;
+    c.ctr[CTR_PROJ] = 0;
   }
   const long long tot = total_elems(c, 0, c.L, D);
   SCENE_LOOP(e, tot) {
@@ -148,27 +149,49 @@ __device__ __forceinline__ void touch_one(const Ctx& c, int p) {
       cell_or<D>(c, gl, I, ACT);
     }
   } else {
+    // The lookups depend on the finest base cell fb, then on (level, base):
+    // lanes of a warp that share them would repeat identical lookups and
+    // activations, so the first lane of each group does them for the group.
+    const unsigned act = __activemask();
+    const int lane = threadIdx.x & 31;
     int fb[D];
+    long long fk = 0;
 #pragma unroll
-    for (int d = 0; d < D; ++d) fb[d] = (int)(xp[d] * (float)c.sz + 0.5f) - 1;
-#pragma unroll 1
-    for (int a = 0; a < (1 << (2 * D)); ++a) {
-      int I[D];
-#pragma unroll
-      for (int d = 0; d < D; ++d) I[d] = fb[d] + ((a >> (2 * (D - 1 - d))) & 3) - 1;
-      grid_init<D>(c, I);
+    for (int d = 0; d < D; ++d) {
+      fb[d] = (int)(xp[d] * (float)c.sz + 0.5f) - 1;
+      fk = fk * (c.sz + 4) + (fb[d] + 2);
     }
-    const int level = grid_init<D>(c, fb);
+    const unsigned g1 = __match_any_sync(act, fk);
+    const int lead1 = __ffs(g1) - 1;
+    int level = 0;
+    if (lane == lead1) {
+#pragma unroll 1
+      for (int a = 0; a < (1 << (2 * D)); ++a) {
+        int I[D];
+#pragma unroll
+        for (int d = 0; d < D; ++d) I[d] = fb[d] + ((a >> (2 * (D - 1 - d))) & 3) - 1;
+        grid_init<D>(c, I);
+      }
+      level = grid_init<D>(c, fb);
+    }
+    level = __shfl_sync(g1, level, lead1);
     const float inv = (float)(c.coarsest << level);
     int base[D];
+    long long bk = level;
 #pragma unroll
-    for (int d = 0; d < D; ++d) base[d] = (int)(xp[d] * inv + 0.5f) - 1;
+    for (int d = 0; d < D; ++d) {
+      base[d] = (int)(xp[d] * inv + 0.5f) - 1;
+      bk = bk * (c.sz + 4) + (base[d] + 2);
+    }
+    const unsigned g2 = __match_any_sync(act, bk);
+    if (lane == __ffs(g2) - 1) {
 #pragma unroll
-    for (int a = 0; a < (1 << D); ++a) {
-      int I[D];
+      for (int a = 0; a < (1 << D); ++a) {
+        int I[D];
 #pragma unroll
-      for (int d = 0; d < D; ++d) I[d] = (base[d] + ((a >> (D - 1 - d)) & 1)) * (1 << (c.L - 1 - level));
-      grid_init<D>(c, I);
+        for (int d = 0; d < D; ++d) I[d] = (base[d] + ((a >> (D - 1 - d)) & 1)) * (1 << (c.L - 1 - level));
+        grid_init<D>(c, I);
+      }
     }
   }
 }
@@ -425,7 +448,8 @@ __device__ __forceinline__ void bin_one(const Ctx& c, int p) {
     int nbins = 0;
     for (int q = 0; q < c.L; ++q) nbins += c.ctr[CTR_LEVEL + q];
     if (!esc) {
-      for (int l = 0; l < c.L; ++l) {
+      // the finest level with an ACTIVATED cell: search from the finest down
+      for (int l = c.L - 1; l >= 0 && fl < 0; --l) {
         const float inv = (float)(c.coarsest << l);
         int base[D];
 #pragma unroll
@@ -606,7 +630,7 @@ void launch_substep(const BatchLaunch& bl, cudaStream_t s, cudaEvent_t* ev) {
 
 int kernels_per_substep(const BatchLaunch& bl) {
   const int topo = 9 - (bl.any_dynamic ? 0 : 1);
-  return topo + 3 + 2 * (bl.maxL - 1);
+  return topo + 3 + (bl.any_plastic ? 1 : 0) + 2 * (bl.maxL - 1);
 }
 
 }  // namespace agimp

@@ -844,7 +844,10 @@ __device__ __forceinline__ void g2p_one(const Ctx& c, int j) {
       for (int k = 0; k < D; ++k) a += ((i == k ? 1.f : 0.f) + s * G[i * D + k]) * F[k * D + q];
       Fn[i * D + q] = a;
     }
-  if (c.plast == 1) snow_return_map<D>(c, Fn, jp, j);
+  // trial states that may leave the elastic interval get the return map in
+  // k_project (it needs an SVD, whose registers would halve G2P's occupancy)
+  if (c.plast == 1 && !singular_values_within<D>(Fn, 1.f - c.theta_c, 1.f + c.theta_s))
+    c.proj[reserve_slot(&c.ctr[CTR_PROJ])] = j;
 #pragma unroll
   for (int i = 0; i < D * D; ++i) __stwb(&c.Q.F[i * N + j], Fn[i]);
   __stwb(&c.Q.m[j], mp);
@@ -858,6 +861,27 @@ template <int D>
 __global__ void __launch_bounds__(256, 3) k_g2p(Batch B) {
   SCENE_CTA(B, MAP_G);
   SCENE_LOOP(j, c.N) g2p_one<D>(c, (int)j);
+}
+
+// Snow return map (extension) of the particles G2P listed: the trial state
+// written to Q is projected in place (or handed to the surrogate).
+template <int D>
+__global__ void __launch_bounds__(256) k_project(Batch B) {
+  SCENE_CTA(B, MAP_G);
+  if (c.plast != 1) return;
+  const int n = c.ctr[CTR_PROJ];
+  const long long N = c.N;
+  SCENE_LOOP(s, n) {
+    const int j = c.proj[s];
+    float F[D * D];
+#pragma unroll
+    for (int k = 0; k < D * D; ++k) F[k] = c.Q.F[k * N + j];
+    float jp = c.Q.Jp[j];
+    snow_return_map<D>(c, F, jp, j);
+#pragma unroll
+    for (int k = 0; k < D * D; ++k) __stwb(&c.Q.F[k * N + j], F[k]);
+    __stwb(&c.Q.Jp[j], jp);
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -897,6 +921,7 @@ void launch_transfer(const BatchLaunch& bl, cudaStream_t s, cudaEvent_t* ev) {
   for (int l = 1; l < bl.maxL; ++l) k_prolong<D><<<G, 256, 0, s>>>(bl.b, l);
   if (ev) cudaEventRecord(ev[7], s);
   k_g2p<D><<<G, 256, 0, s>>>(bl.b);
+  if (bl.any_plastic) k_project<D><<<G, 256, 0, s>>>(bl.b);
   const Ctx* c = bl.single;
   if (c && c->sur && c->plast == 1 && c->N) {
     launch_mlp_forward_dev(c->mlp_packed, c->mlp_P, c->sur_X, c->sur_Y, c->ctr + CTR_SUR, c->N, c->ctr + CTR_ERR,
