@@ -106,7 +106,7 @@ __device__ __forceinline__ int grid_init(const Ctx& c, const int* I) {
   return l;
 }
 
-// one particle slot p (may be >= N: the warp-collective part still runs)
+// one particle slot p (may be >= N)
 template <int D>
 __device__ __forceinline__ void touch_one(const Ctx& c, int p) {
   const bool valid = p < c.N;
@@ -118,35 +118,24 @@ __device__ __forceinline__ void touch_one(const Ctx& c, int p) {
     if (!(xp[d] >= 0.f && xp[d] < 1.f)) esc = true;
   }
   if (valid && esc) set_err(c, ERR_ESCAPED);
-  const LevelDev& Vf = c.lev[c.L - 1];
-  int key = -1;
-  if (!esc) {
-    long long b = 0;
-#pragma unroll
-    for (int d = 0; d < D; ++d) b = b * Vf.nb + ((((int)(xp[d] * (float)c.sz)) >> 2) + 1);
-    key = (int)b;
-  }
-  const unsigned grp = __match_any_sync(0xffffffffu, key);
-  if (key >= 0 && (int)(threadIdx.x & 31) == __ffs(grp) - 1) {
-    if (c.touch_flag[key] == 0u && atomicExch(&c.touch_flag[key], 1u) == 0u) {
-      const int i = atomicAdd(&c.ctr[CTR_TOUCH], 1);
-      c.touch_list[i] = key;
-    }
-  }
   if (esc) return;
+  // reach of this particle's activations, recorded with its finest block: 1
+  // in dynamic mode, L - (level of its level-map cell) in static mode
+  unsigned reach = 1;
   if (!c.is_static) {
     const int gl = c.P.g[p];
-    if (gl < 0 || gl >= c.L) return;
-    const float inv = (float)(c.coarsest << gl);
-    int base[D];
+    if (gl >= 0 && gl < c.L) {
+      const float inv = (float)(c.coarsest << gl);
+      int base[D];
 #pragma unroll
-    for (int d = 0; d < D; ++d) base[d] = (int)(xp[d] * inv + 0.5f) - 1;
+      for (int d = 0; d < D; ++d) base[d] = (int)(xp[d] * inv + 0.5f) - 1;
 #pragma unroll
-    for (int a = 0; a < (1 << D); ++a) {
-      int I[D];
+      for (int a = 0; a < (1 << D); ++a) {
+        int I[D];
 #pragma unroll
-      for (int d = 0; d < D; ++d) I[d] = base[d] + ((a >> (D - 1 - d)) & 1);
-      cell_or<D>(c, gl, I, ACT);
+        for (int d = 0; d < D; ++d) I[d] = base[d] + ((a >> (D - 1 - d)) & 1);
+        cell_or<D>(c, gl, I, ACT);
+      }
     }
   } else {
     // The lookups depend on the finest base cell fb, then on (level, base):
@@ -175,6 +164,7 @@ __device__ __forceinline__ void touch_one(const Ctx& c, int p) {
       level = grid_init<D>(c, fb);
     }
     level = __shfl_sync(g1, level, lead1);
+    reach = (unsigned)(c.L - level);
     const float inv = (float)(c.coarsest << level);
     int base[D];
     long long bk = level;
@@ -194,6 +184,19 @@ __device__ __forceinline__ void touch_one(const Ctx& c, int p) {
       }
     }
   }
+  // record the finest block for the active-block lists (first toucher appends)
+  const LevelDev& Vf = c.lev[c.L - 1];
+  unsigned b = 0;
+#pragma unroll
+  for (int d = 0; d < D; ++d) b = b * (unsigned)Vf.nb + (unsigned)((((int)(xp[d] * (float)c.sz)) >> 2) + 1);
+  const int key = (int)b;
+  const unsigned grp = __match_any_sync(__activemask(), key);
+  const unsigned rmax = __reduce_max_sync(grp, reach);
+  if ((int)(threadIdx.x & 31) == __ffs(grp) - 1 && c.touch_flag[key] < rmax &&
+      atomicMax(&c.touch_flag[key], rmax) == 0u) {
+    const int i = atomicAdd(&c.ctr[CTR_TOUCH], 1);
+    c.touch_list[i] = key;
+  }
 }
 
 template <int D>
@@ -208,21 +211,28 @@ __global__ void k_touch_activate(Batch B) {
 // Active-block lists: level l gets the blocks within R_l blocks of each
 // touched finest block (shifted to that level).  Dynamic activation, culling,
 // ghost/T marking and the transfers stay within 2 cells of a particle at every
-// level, so R_l = 1.  A static level-map lookup (adaptive_gimp.py:82-85) can
-// land up to two cells of the particle's own level away, i.e. up to 2^L finest
-// cells, and activate a cell of any level there; with the ghost / T /
-// corner reach on top, level l then needs ceil((2^(l+1) + 6) / 4) blocks.
-__device__ __forceinline__ int dilate_radius(const Ctx& c, int l) {
-  return c.is_static ? ((1 << (l + 1)) + 9) / 4 : 1;
+// level, so R_l = 1.  A static level-map lookup (adaptive_gimp.py:82-85) lands
+// up to two cells of the level the map gives at the particle (lv) away, i.e.
+// rho = max(2, 2^(L - lv)) finest cells, and activates a cell of any level
+// there; with the ghost / T / corner reach on top (6 cells), level l needs
+// ceil((ceil(rho / 2^(L-1-l)) + 6) / 4) blocks.  The touched block records
+// L - lv of its coarsest-mapped particle (`reach`; 1 in dynamic mode).
+__device__ __forceinline__ int dilate_radius(const Ctx& c, int l, unsigned reach) {
+  if (!c.is_static) return 1;
+  const int rho = max(2, 1 << (int)reach);  // reach = L - lv
+  const int div = 1 << (c.L - 1 - l);
+  return ((rho + div - 1) / div + 9) / 4;
 }
 
 template <int D>
 __global__ void k_dilate(Batch B) {
   SCENE_CTA(B, MAP_G);
+  // work items laid out for the largest reach (a particle mapped to level 0);
+  // items beyond a block's own radius are skipped
   int per_level[MAXL];
   long long W = 0;
   for (int l = 0; l < c.L; ++l) {
-    const int w = 2 * dilate_radius(c, l) + 1;
+    const int w = 2 * dilate_radius(c, l, (unsigned)c.L) + 1;
     per_level[l] = (D == 2) ? w * w : w * w * w;
     W += per_level[l];
   }
@@ -236,10 +246,10 @@ __global__ void k_dilate(Batch B) {
       r -= per_level[l];
       ++l;
     }
-    const int R = dilate_radius(c, l);
-    const int w = 2 * R + 1;
+    const int Rmax = dilate_radius(c, l, (unsigned)c.L);
+    const int w = 2 * Rmax + 1;
     const int key = c.touch_list[t];
-    if (l == c.L - 1 && r == per_level[l] / 2) c.touch_flag[key] = 0u;
+    const int R = dilate_radius(c, l, c.touch_flag[key]);
     int fb[D];
     long long k = key;
 #pragma unroll
@@ -251,13 +261,15 @@ __global__ void k_dilate(Batch B) {
     const int s = c.L - 1 - l;
     int dl[D];
     int tt = r;
+    bool ok = true;
 #pragma unroll
     for (int d = D - 1; d >= 0; --d) {
-      dl[d] = tt % w - R;
+      dl[d] = tt % w - Rmax;
       tt /= w;
+      ok = ok && dl[d] >= -R && dl[d] <= R;
     }
+    if (!ok) continue;
     long long b = 0;
-    bool ok = true;
 #pragma unroll
     for (int d = 0; d < D; ++d) {
       const int cb = (fb[d] >> s) + dl[d] + 1;
@@ -320,6 +332,9 @@ __global__ void k_mark_hier(Batch B) {
 template <int D>
 __global__ void k_resolve(Batch B) {
   SCENE_CTA(B, MAP_G);
+  // k_dilate has read the touched blocks' reach: clear the flags for the next
+  // substep (they are read again only by k_touch_activate)
+  SCENE_LOOP(t, c.ctr[CTR_TOUCH]) c.touch_flag[c.touch_list[t]] = 0u;
   const long long tot = total_elems(c, 0, c.L, D);
   SCENE_LOOP(e, tot) {
     int l, loc;
