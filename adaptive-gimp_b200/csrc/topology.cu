@@ -152,16 +152,15 @@ __device__ __forceinline__ void touch_one(const Ctx& c, int p) {
     }
     const unsigned g1 = __match_any_sync(act, fk);
     const int lead1 = __ffs(g1) - 1;
+    const int r1 = __popc(g1 & ((1u << lane) - 1u)), n1 = __popc(g1);
     int level = 0;
-    if (lane == lead1) {
+    if (lane == lead1) level = grid_init<D>(c, fb);
 #pragma unroll 1
-      for (int a = 0; a < (1 << (2 * D)); ++a) {
-        int I[D];
+    for (int a = r1; a < (1 << (2 * D)); a += n1) {
+      int I[D];
 #pragma unroll
-        for (int d = 0; d < D; ++d) I[d] = fb[d] + ((a >> (2 * (D - 1 - d))) & 3) - 1;
-        grid_init<D>(c, I);
-      }
-      level = grid_init<D>(c, fb);
+      for (int d = 0; d < D; ++d) I[d] = fb[d] + ((a >> (2 * (D - 1 - d))) & 3) - 1;
+      grid_init<D>(c, I);
     }
     level = __shfl_sync(g1, level, lead1);
     reach = (unsigned)(c.L - level);
@@ -174,14 +173,13 @@ __device__ __forceinline__ void touch_one(const Ctx& c, int p) {
       bk = bk * (c.sz + 4) + (base[d] + 2);
     }
     const unsigned g2 = __match_any_sync(act, bk);
-    if (lane == __ffs(g2) - 1) {
+    const int r2 = __popc(g2 & ((1u << lane) - 1u)), n2 = __popc(g2);
+#pragma unroll 1
+    for (int a = r2; a < (1 << D); a += n2) {
+      int I[D];
 #pragma unroll
-      for (int a = 0; a < (1 << D); ++a) {
-        int I[D];
-#pragma unroll
-        for (int d = 0; d < D; ++d) I[d] = (base[d] + ((a >> (D - 1 - d)) & 1)) * (1 << (c.L - 1 - level));
-        grid_init<D>(c, I);
-      }
+      for (int d = 0; d < D; ++d) I[d] = (base[d] + ((a >> (D - 1 - d)) & 1)) * (1 << (c.L - 1 - level));
+      grid_init<D>(c, I);
     }
   }
   // record the finest block for the active-block lists (first toucher appends)
@@ -227,61 +225,49 @@ __device__ __forceinline__ int dilate_radius(const Ctx& c, int l, unsigned reach
 template <int D>
 __global__ void k_dilate(Batch B) {
   SCENE_CTA(B, MAP_G);
-  // work items laid out for the largest reach (a particle mapped to level 0);
-  // items beyond a block's own radius are skipped
-  int per_level[MAXL];
-  long long W = 0;
-  for (int l = 0; l < c.L; ++l) {
-    const int w = 2 * dilate_radius(c, l, (unsigned)c.L) + 1;
-    per_level[l] = (D == 2) ? w * w : w * w * w;
-    W += per_level[l];
-  }
-  const long long tot = (long long)c.ctr[CTR_TOUCH] * W;
+  // one warp per touched finest block; its lanes walk the block's
+  // (2R_l + 1)^d neighbourhood at every level
+  const int lane = threadIdx.x & 31;
+  const int wid = bid_ * (blockDim.x >> 5) + (threadIdx.x >> 5), nw = nblk_ * (blockDim.x >> 5);
   const LevelDev& Vf = c.lev[c.L - 1];
-  SCENE_LOOP(e, tot) {
-    const int t = (int)(e / W);
-    int r = (int)(e % W);
-    int l = 0;
-    while (l < c.L - 1 && r >= per_level[l]) {
-      r -= per_level[l];
-      ++l;
-    }
-    const int Rmax = dilate_radius(c, l, (unsigned)c.L);
-    const int w = 2 * Rmax + 1;
+  const int ntouch = c.ctr[CTR_TOUCH];
+  for (int t = wid; t < ntouch; t += nw) {
     const int key = c.touch_list[t];
-    const int R = dilate_radius(c, l, c.touch_flag[key]);
+    const unsigned reach = c.touch_flag[key];
     int fb[D];
-    long long k = key;
+    unsigned k = (unsigned)key;
 #pragma unroll
     for (int d = D - 1; d >= 0; --d) {
-      fb[d] = (int)(k % Vf.nb) - 1;
-      k /= Vf.nb;
+      fb[d] = (int)(k % (unsigned)Vf.nb) - 1;
+      k /= (unsigned)Vf.nb;
     }
-    const LevelDev& V = c.lev[l];
-    const int s = c.L - 1 - l;
-    int dl[D];
-    int tt = r;
-    bool ok = true;
+    for (int l = 0; l < c.L; ++l) {
+      const int R = dilate_radius(c, l, reach);
+      const int w = 2 * R + 1;
+      const int items = (D == 2) ? w * w : w * w * w;
+      const LevelDev& V = c.lev[l];
+      const int s = c.L - 1 - l;
+      for (int r = lane; r < items; r += 32) {
+        int tt = r;
+        unsigned b = 0;
+        bool ok = true;
+        int cb[D];
 #pragma unroll
-    for (int d = D - 1; d >= 0; --d) {
-      dl[d] = tt % w - Rmax;
-      tt /= w;
-      ok = ok && dl[d] >= -R && dl[d] <= R;
-    }
-    if (!ok) continue;
-    long long b = 0;
+        for (int d = D - 1; d >= 0; --d) {
+          cb[d] = (fb[d] >> s) + (tt % w - R) + 1;
+          tt /= w;
+          ok = ok && cb[d] >= 0 && cb[d] < V.nb;
+        }
+        if (!ok) continue;  // beyond the stored lattice: nothing can be written there
 #pragma unroll
-    for (int d = 0; d < D; ++d) {
-      const int cb = (fb[d] >> s) + dl[d] + 1;
-      ok = ok && cb >= 0 && cb < V.nb;
-      b = b * V.nb + cb;
-    }
-    if (!ok) continue;  // beyond the stored lattice: nothing can be written there
-    int* bm = &V.bmap[b];
-    if (*bm == -1 && atomicCAS(bm, -1, -2) == -1) {
-      const int i = atomicAdd(&c.ctr[CTR_LEVEL + l], 1);
-      V.blist[i] = (int)b;
-      *bm = i;
+        for (int d = 0; d < D; ++d) b = b * (unsigned)V.nb + (unsigned)cb[d];
+        int* bm = &V.bmap[b];
+        if (*bm == -1 && atomicCAS(bm, -1, -2) == -1) {
+          const int i = atomicAdd(&c.ctr[CTR_LEVEL + l], 1);
+          V.blist[i] = (int)b;
+          *bm = i;
+        }
+      }
     }
   }
 }
