@@ -64,6 +64,8 @@ def parse():
                          "then also reports the plain path's throughput and the position error against it")
     ap.add_argument("--sur-tol", type=float, default=1e-3, help="surrogate residual tolerance")
     ap.add_argument("--no-autotune", action="store_true", help="config 4: keep the default launch sizes")
+    ap.add_argument("--tuning", default=None, metavar="CHUNK,CTAS_PER_SM",
+                    help="fixed launch sizes instead of the autotuner (e.g. 64,16)")
     return ap.parse_args()
 
 
@@ -406,7 +408,12 @@ def run_batch(a):
     st = ctypes.c_void_p(stream.cuda_stream)
     sims = [s.build(device=local) for s in sc]
     batch = SceneBatch(sims)
-    tuning = batch.autotune(dt, trials=3, stream=st) if not a.no_autotune else batch.tuning
+    if a.tuning:
+        ch, cps = (int(v) for v in a.tuning.split(","))
+        batch.set_tuning(ch, cps)
+        tuning = batch.tuning
+    else:
+        tuning = batch.autotune(dt, trials=3, stream=st) if not a.no_autotune else batch.tuning
 
     def timed(step, clocks=None):
         import contextlib
