@@ -23,38 +23,6 @@
 
 namespace agimp {
 
-
-template <int D>
-struct Stencil {
-  float W[D][3], G[D][3];
-  float kw, kg;
-};
-
-template <int D>
-__device__ __forceinline__ void make_stencil(const float* tc, float r, Stencil<D>& s) {
-#pragma unroll
-  for (int d = 0; d < D; ++d) axis_weights(tc[d], r, s.W[d], s.G[d]);
-  const float r2 = 2.f * r;
-  s.kw = (D == 2) ? 1.f / (4.f * r2 * r2) : 1.f / (8.f * r2 * r2 * r2);
-  s.kg = (D == 2) ? 1.f / (2.f * r2 * r2) : 1.f / (4.f * r2 * r2 * r2);
-}
-
-template <int D>
-__device__ __forceinline__ void node_weight(const Stencil<D>& s, const int* n, float& w, float* g) {
-  if (D == 2) {
-    const float wx = s.W[0][n[0]], wy = s.W[1][n[1]];
-    w = wx * wy * s.kw;
-    g[0] = s.G[0][n[0]] * wy * s.kg;
-    g[1] = wx * s.G[1][n[1]] * s.kg;
-  } else {
-    const float wx = s.W[0][n[0]], wy = s.W[1][n[1]], wz = s.W[2][n[2]];
-    w = wx * wy * wz * s.kw;
-    g[0] = s.G[0][n[0]] * wy * wz * s.kg;
-    g[1] = wx * s.G[1][n[1]] * wz * s.kg;
-    g[2] = wx * wy * s.G[2][n[2]] * s.kg;
-  }
-}
-
 template <int D>
 __device__ __forceinline__ void chunk_origin(const LevelDev& V, long long blk, int* O) {
 #pragma unroll
@@ -99,7 +67,7 @@ struct P2GLayout {
   static constexpr int STRIDE = OFF_WL + 8;  // 3D 44, 2D 28 floats: 16-byte aligned records
   static constexpr int MAXTASK = NC + CH / TMAX;
   static constexpr size_t bytes() {
-    return sizeof(float) * ((size_t)CH * STRIDE + 4 * TN) + sizeof(int) * (3 * NC + CH + 3 * MAXTASK + 4);
+    return sizeof(float) * ((size_t)CH * STRIDE + 4 * TN) + sizeof(int) * (2 * NC + 2 * CH + 3 * MAXTASK + 4);
   }
 };
 
@@ -112,9 +80,9 @@ __global__ void __launch_bounds__(CH, 1024 / CH) k_p2g(Batch B) {
   float* tile = pd + CH * Y::STRIDE;            // [4][TN]: p_x, p_y, p_z, m
   int* s_cnt = (int*)(tile + 4 * Y::TN);        // [NC]
   int* s_off = s_cnt + Y::NC;                   // [NC]
-  int* s_tpre = s_off + Y::NC;                  // [NC]
-  int* s_sorted = s_tpre + Y::NC;               // [CH]
-  int* t_cell = s_sorted + CH;                  // [MAXTASK]
+  int* s_sorted = s_off + Y::NC;                // [CH]
+  int* s_pc = s_sorted + CH;                    // [CH] cell << 8 | rank of each particle
+  int* t_cell = s_pc + CH;                      // [MAXTASK]
   int* t_start = t_cell + Y::MAXTASK;
   int* t_len = t_start + Y::MAXTASK;
   int* s_ntask = t_len + Y::MAXTASK;
@@ -125,16 +93,18 @@ __global__ void __launch_bounds__(CH, 1024 / CH) k_p2g(Batch B) {
   const float r2 = 2.f * c.radius;
   const float kw = (D == 2) ? 1.f / (4.f * r2 * r2) : 1.f / (8.f * r2 * r2 * r2);
   const float kg = (D == 2) ? 1.f / (2.f * r2 * r2) : 1.f / (4.f * r2 * r2 * r2);
+  // the node tile and the cell counts start at zero; each work item's flush
+  // leaves them at zero again
+  for (int i = threadIdx.x; i < 4 * Y::TN; i += blockDim.x) tile[i] = 0.f;
+  for (int i = threadIdx.x; i < Y::NC; i += blockDim.x) s_cnt[i] = 0;
+  __syncthreads();
   for (int ch = bid_; ch < nch; ch += nblk_) {
     const int4 wd = c.chunks[ch];
     const int l = wd.x;
     if (l < 0) continue;  // particles without a level: no transfer (uniform over the CTA)
     const LevelDev& V = c.lev[l];
-    for (int i = threadIdx.x; i < 4 * Y::TN; i += blockDim.x) tile[i] = 0.f;
-    for (int i = threadIdx.x; i < Y::NC; i += blockDim.x) s_cnt[i] = 0;
     int O[D];
     chunk_origin<D>(V, wd.y, O);
-    __syncthreads();
     // -- 1. per-particle quantities ------------------------------------------
     const int i = threadIdx.x;
     int cell = -1;
@@ -220,8 +190,9 @@ __global__ void __launch_bounds__(CH, 1024 / CH) k_p2g(Batch B) {
       old = __shfl_sync(0xffffffffu, old, leader);
       rank = old + __popc(grp & ((1u << lane) - 1u));
     }
+    if (cell >= 0) s_pc[i] = (cell << 8) | rank;
     __syncthreads();
-    // -- 2. cell offsets and tasks (warp 0) ----------------------------------
+    // -- 2. cell offsets, tasks and the cell order (warp 0) --------------------
     if (warp == 0) {
       int run_c = 0, run_t = 0;
       for (int c0 = 0; c0 < Y::NC; c0 += 32) {
@@ -238,22 +209,22 @@ __global__ void __launch_bounds__(CH, 1024 / CH) k_p2g(Batch B) {
           }
         }
         if (cc < Y::NC) {
-          s_off[cc] = run_c + ic - n;
-          s_tpre[cc] = run_t + it - nt;
+          const int off = run_c + ic - n;
+          s_off[cc] = off;
+          for (int j = 0, t = run_t + it - nt; j < n; j += Y::TMAX, ++t) {
+            t_cell[t] = cc;
+            t_start[t] = off + j;
+            t_len[t] = min(Y::TMAX, n - j);
+          }
         }
         run_c += __shfl_sync(0xffffffffu, ic, 31);
         run_t += __shfl_sync(0xffffffffu, it, 31);
       }
       if (lane == 0) *s_ntask = run_t;
-    }
-    __syncthreads();
-    if (cell >= 0) s_sorted[s_off[cell] + rank] = i;
-    for (int cc = threadIdx.x; cc < Y::NC; cc += blockDim.x) {
-      const int n = s_cnt[cc];
-      for (int j = 0, t = s_tpre[cc]; j < n; j += Y::TMAX, ++t) {
-        t_cell[t] = cc;
-        t_start[t] = s_off[cc] + j;
-        t_len[t] = min(Y::TMAX, n - j);
+      __syncwarp();
+      for (int k = lane; k < wd.w; k += 32) {
+        const int v = s_pc[k];
+        s_sorted[s_off[v >> 8] + (v & 255)] = k;
       }
     }
     __syncthreads();
@@ -357,12 +328,15 @@ __global__ void __launch_bounds__(CH, 1024 / CH) k_p2g(Batch B) {
         I[d] = O[d] + tt % 6;
         tt /= 6;
       }
+      tile[t] = tile[Y::TN + t] = tile[3 * Y::TN + t] = 0.f;
+      if (D == 3) tile[2 * Y::TN + t] = 0.f;
       if (!in_store<D>(V, I)) {
         set_err(c, ERR_OOB);
         continue;
       }
       atomicAdd(&V.node[elem_of<D>(V, I)], val);
     }
+    for (int i = threadIdx.x; i < Y::NC; i += blockDim.x) s_cnt[i] = 0;
     __syncthreads();
   }
 }
@@ -796,34 +770,60 @@ __device__ __forceinline__ void g2p_one(const Ctx& c, int j) {
     base[d] = (int)(xs + 0.5f) - 1;
     tc[d] = xs - (float)(base[d] + 1);
   }
-  Stencil<D> st;
-  make_stencil<D>(tc, c.radius, st);
+  // Gather by rows along the last axis: the weights are products of per-axis
+  // terms, so a row's nodes are first summed with the last axis's weight (S)
+  // and gradient (T), and the other axes' factors are applied once per row.
+  float W[D][3], Gw[D][3];
+#pragma unroll
+  for (int d = 0; d < D; ++d) axis_weights(tc[d], c.radius, W[d], Gw[d]);
+  const float r2 = 2.f * c.radius;
+  const float kw = (D == 2) ? 1.f / (4.f * r2 * r2) : 1.f / (8.f * r2 * r2 * r2);
+  const float kg = (D == 2) ? 1.f / (2.f * r2 * r2) : 1.f / (4.f * r2 * r2 * r2);
   float nv[D], G[D * D];
 #pragma unroll
   for (int i = 0; i < D; ++i) nv[i] = 0.f;
 #pragma unroll
   for (int i = 0; i < D * D; ++i) G[i] = 0.f;
 #pragma unroll
-  for (int k = 0; k < ((D == 2) ? 9 : 27); ++k) {
-    int n[D], I[D];
-    int t = k;
+  for (int row = 0; row < ((D == 2) ? 3 : 9); ++row) {
+    const int n0 = (D == 2) ? row : row / 3, n1 = (D == 2) ? 0 : row % 3;
+    float S[D], T[D];
 #pragma unroll
-    for (int d = D - 1; d >= 0; --d) {
-      n[d] = t % 3;
-      t /= 3;
+    for (int i = 0; i < D; ++i) S[i] = T[i] = 0.f;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      int I[D];
+      I[0] = base[0] + n0;
+      if (D == 3) I[1] = base[1] + n1;
+      I[D - 1] = base[D - 1] + k;
+      // base lies in [-1, size-1] for an in-domain particle: always in store
+      const float4 nd = __ldg(&V.node[elem_of<D>(V, I)]);
+      const float gv[3] = {nd.x, nd.y, nd.z};
+#pragma unroll
+      for (int i = 0; i < D; ++i) {
+        S[i] += gv[i] * W[D - 1][k];
+        T[i] += gv[i] * Gw[D - 1][k];
+      }
+    }
+    // row factors: weight, and the gradient components of the other axes
+    float cw, cg[D];
+    if (D == 2) {
+      cw = W[0][n0] * kw;
+      cg[0] = Gw[0][n0] * kg;
+      cg[1] = W[0][n0] * kg;
+    } else {
+      const float wxy = W[0][n0] * W[1][n1];
+      cw = wxy * kw;
+      cg[0] = Gw[0][n0] * W[1][n1] * kg;
+      cg[1] = W[0][n0] * Gw[1][n1] * kg;
+      cg[D - 1] = wxy * kg;
     }
 #pragma unroll
-    for (int d = 0; d < D; ++d) I[d] = base[d] + n[d];
-    // base lies in [-1, size-1] for an in-domain particle: always in store
-    const float4 nd = __ldg(&V.node[elem_of<D>(V, I)]);
-    const float gv[3] = {nd.x, nd.y, nd.z};
-    float w, gw[D];
-    node_weight<D>(st, n, w, gw);
-#pragma unroll
     for (int i = 0; i < D; ++i) {
-      nv[i] += gv[i] * w;
+      nv[i] += cw * S[i];
 #pragma unroll
-      for (int q = 0; q < D; ++q) G[i * D + q] += gv[i] * gw[q];
+      for (int q = 0; q < D - 1; ++q) G[i * D + q] += cg[q] * S[i];
+      G[i * D + D - 1] += cg[D - 1] * T[i];
     }
   }
 #pragma unroll
