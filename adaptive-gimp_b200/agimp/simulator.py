@@ -375,7 +375,7 @@ class AdaptiveGIMP:
         return t.as_dict()
 
     def set_tuning(self, chunk=256, ctas_per_sm=8):
-        """P2G work-item size (64, 128, 256) and grid-stride CTAs per SM."""
+        """P2G work-item size (64, 128, 256, 512) and grid-stride CTAs per SM."""
         t = _capi.Tuning(int(chunk), int(ctas_per_sm), 0.0)
         _capi.check(self._L.agimp_set_tuning(self._h, ctypes.byref(t)), self._h, "set tuning")
 

@@ -209,8 +209,9 @@ int batch_kernels(agimp_batch* b) {
 }
 
 agimp_status batch_set_tuning(agimp_batch* b, const agimp_tuning* t) {
-  if (!t || (t->chunk != 64 && t->chunk != 128 && t->chunk != 256) || t->ctas_per_sm < 1 || t->ctas_per_sm > 32) {
-    b->err = "tuning: chunk must be 64, 128 or 256 and ctas_per_sm in [1, 32]";
+  if (!t || (t->chunk != 64 && t->chunk != 128 && t->chunk != 256 && t->chunk != 512) || t->ctas_per_sm < 1 ||
+      t->ctas_per_sm > 32) {
+    b->err = "tuning: chunk must be 64, 128, 256 or 512 and ctas_per_sm in [1, 32]";
     return AGIMP_INVALID_ARG;
   }
   b->tune.chunk = t->chunk;
@@ -308,9 +309,9 @@ agimp_status batch_autotune(agimp_batch* b, float dt, int trials, agimp_tuning* 
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
   agimp_status st = AGIMP_OK;
-  const int chunks[3] = {64, 128, 256};
+  const int chunks[4] = {64, 128, 256, 512};
   const int cps[4] = {2, 4, 8, 16};
-  for (int ci = 0; ci < 3 && st == AGIMP_OK; ++ci)
+  for (int ci = 0; ci < 4 && st == AGIMP_OK; ++ci)
     for (int gi = 0; gi < 4 && st == AGIMP_OK; ++gi) {
       agimp_tuning t{chunks[ci], cps[gi], 0.f};
       st = batch_set_tuning(b, &t);

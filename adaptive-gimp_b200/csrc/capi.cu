@@ -301,7 +301,7 @@ agimp_status agimp_create(const agimp_params* p, int32_t device, agimp_sim** out
   AL(c.bin_start, tot_blocks + 1);
   cudaMemset(c.bin_count, 0, (tot_blocks + 1) * sizeof(int32_t));
   const long long N = c.N;
-  AL(c.chunks, N / MIN_CHUNK + tot_blocks + 2);
+  AL(c.chunks, N / MIN_CHUNK + tot_blocks + 2);  // enough for any work-item size
   c.chunk = CHUNK;
   AL(c.bin_of, N + 1);
   AL(c.rank_of, N + 1);

@@ -26,7 +26,8 @@
 namespace agimp {
 
 constexpr int MAXL = 8;
-constexpr int CHUNK = 256;      // largest P2G work item (particles of one bin) = largest P2G CTA
+constexpr int CHUNK = 256;      // default P2G work item (particles of one bin) = P2G CTA size
+constexpr int MAX_CHUNK = 512;  // largest work item the tuning may choose
 constexpr int MIN_CHUNK = 64;   // smallest work item (sizes the work-item buffer)
 constexpr int HALO = 4;
 

@@ -81,7 +81,7 @@ __global__ void __launch_bounds__(CH, 1024 / CH) k_p2g(Batch B) {
   int* s_cnt = (int*)(tile + 4 * Y::TN);        // [NC]
   int* s_off = s_cnt + Y::NC;                   // [NC]
   int* s_sorted = s_off + Y::NC;                // [CH]
-  int* s_pc = s_sorted + CH;                    // [CH] cell << 8 | rank of each particle
+  int* s_pc = s_sorted + CH;                    // [CH] cell << 10 | rank of each particle
   int* t_cell = s_pc + CH;                      // [MAXTASK]
   int* t_start = t_cell + Y::MAXTASK;
   int* t_len = t_start + Y::MAXTASK;
@@ -190,7 +190,7 @@ __global__ void __launch_bounds__(CH, 1024 / CH) k_p2g(Batch B) {
       old = __shfl_sync(0xffffffffu, old, leader);
       rank = old + __popc(grp & ((1u << lane) - 1u));
     }
-    if (cell >= 0) s_pc[i] = (cell << 8) | rank;
+    if (cell >= 0) s_pc[i] = (cell << 10) | rank;
     __syncthreads();
     // -- 2. cell offsets, tasks and the cell order (warp 0) --------------------
     if (warp == 0) {
@@ -224,7 +224,7 @@ __global__ void __launch_bounds__(CH, 1024 / CH) k_p2g(Batch B) {
       __syncwarp();
       for (int k = lane; k < wd.w; k += 32) {
         const int v = s_pc[k];
-        s_sorted[s_off[v >> 8] + (v & 255)] = k;
+        s_sorted[s_off[v >> 10] + (v & 1023)] = k;
       }
     }
     __syncthreads();
@@ -897,6 +897,8 @@ void prepare_transfer_kernels() {
   set_p2g_smem<3, 64>();
   set_p2g_smem<3, 128>();
   set_p2g_smem<3, 256>();
+  set_p2g_smem<2, 512>();
+  set_p2g_smem<3, 512>();
 }
 
 template <int D>
@@ -905,6 +907,7 @@ static void launch_p2g(const BatchLaunch& bl, cudaStream_t s) {
   switch (bl.chunk) {
     case 64: k_p2g<D, 64><<<G, 64, P2GLayout<D, 64>::bytes(), s>>>(bl.b); break;
     case 128: k_p2g<D, 128><<<G, 128, P2GLayout<D, 128>::bytes(), s>>>(bl.b); break;
+    case 512: k_p2g<D, 512><<<G, 512, P2GLayout<D, 512>::bytes(), s>>>(bl.b); break;
     default: k_p2g<D, 256><<<G, 256, P2GLayout<D, 256>::bytes(), s>>>(bl.b); break;
   }
 }

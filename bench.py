@@ -63,7 +63,7 @@ def parse():
                     help="snow return map through this trained surrogate (agimp.train_surrogate output); the line "
                          "then also reports the plain path's throughput and the position error against it")
     ap.add_argument("--sur-tol", type=float, default=1e-3, help="surrogate residual tolerance")
-    ap.add_argument("--no-autotune", action="store_true", help="config 4: keep the default launch sizes")
+    ap.add_argument("--no-autotune", action="store_true", help="keep the default launch sizes")
     ap.add_argument("--tuning", default=None, metavar="CHUNK,CTAS_PER_SM",
                     help="fixed launch sizes instead of the autotuner (e.g. 64,16)")
     return ap.parse_args()
@@ -266,13 +266,14 @@ def timed_steps(sim, scene, a, stream, dist=None, clocks=None):
     return e0.elapsed_time(e1)
 
 
-def surrogate_report(a, scene, sim, ms, local):
+def surrogate_report(a, scene, sim, ms, local, tuning):
     """Plain (SVD return map) run of the same scene for comparison: its
     throughput and the surrogate run's position error against it."""
     import numpy as np
     import torch
     st = sim.stats()
     plain = scene.build(device=local)
+    plain.set_tuning(tuning["chunk"], tuning["ctas_per_sm"])
     stream = torch.cuda.Stream()
     with torch.cuda.stream(stream):
         ms_plain = timed_steps(plain, scene, a, stream)
@@ -304,14 +305,21 @@ def run_agimp(a):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     scene = scenes.make_config(a.config, seed=rank, scale=a.scale)
     sim = scene.build(device=local)
+    import ctypes
+    stream = torch.cuda.Stream()
+    st = ctypes.c_void_p(stream.cuda_stream)
+    if a.tuning:
+        ch, cps = (int(v) for v in a.tuning.split(","))
+        sim.set_tuning(ch, cps)
+    elif not a.no_autotune:
+        with torch.cuda.stream(stream):
+            sim.autotune(scene.dt, trials=3, stream=st)
+    tuning = sim.tuning
     mlp = None
     if a.surrogate:
         from agimp.surrogate import load
         mlp, xmax = load(a.surrogate, device=local)
         sim.set_surrogate(mlp, xmax, a.sur_tol)
-    import ctypes
-    stream = torch.cuda.Stream()
-    st = ctypes.c_void_p(stream.cuda_stream)
     with torch.cuda.stream(stream):
         clk = Clocks(local)
         ms = timed_steps(sim, scene, a, stream, dist, clk)
@@ -351,6 +359,7 @@ def run_agimp(a):
                    "description": scene.description},
         "roofline": roof,
         "phases_ms": phases,
+        "tuning": tuning,
         "gpu_launches": launches,
         "clocks": clk.summary(),
         "device_errors": errors,
@@ -359,12 +368,13 @@ def run_agimp(a):
         # the per-phase profile above ran extra substeps: rebuild for the comparison
         sim.close()
         sim = scene.build(device=local)
+        sim.set_tuning(tuning["chunk"], tuning["ctas_per_sm"])
         sim.set_surrogate(mlp, xmax, a.sur_tol)
         with torch.cuda.stream(stream):
             timed_steps(sim, scene, a, stream)
-        out["surrogate"] = surrogate_report(a, scene, sim, ms, local)
+        out["surrogate"] = surrogate_report(a, scene, sim, ms, local, tuning)
     if not a.no_e2e:
-        out["e2e"] = e2e_run(a, scene, local, a.surrogate and (mlp, xmax, a.sur_tol))
+        out["e2e"] = e2e_run(a, scene, local, a.surrogate and (mlp, xmax, a.sur_tol), tuning)
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         threads = os.cpu_count() or 1
         val, done, el = cpu_oracle_run(scene, a.cpu_seconds, threads)
@@ -592,7 +602,7 @@ def e2e_batch(a, sc, local):
             "every substep", "note": "h2d is the one-time upload of the scenes spread over the timed substeps"}
 
 
-def e2e_run(a, scene, local, sur=None):
+def e2e_run(a, scene, local, sur=None, tuning=None):
     """Same metric through the public API with host buffers: upload the scene
     from pinned host memory, then per substep call substep() and read x_p back
     into pinned host memory."""
@@ -614,6 +624,8 @@ def e2e_run(a, scene, local, sur=None):
     hJ[:] = 1
     out = pinned((n, d))
     sim = scene.build(device=local)
+    if tuning:
+        sim.set_tuning(tuning["chunk"], tuning["ctas_per_sm"])
     if sur:
         sim.set_surrogate(*sur)
     torch.cuda.synchronize()

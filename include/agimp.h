@@ -240,13 +240,13 @@ agimp_status agimp_mlp_errors(agimp_mlp* m, uint32_t* bits, int32_t clear);
  * launch sizes).  Results do not depend on it beyond the order of float
  * additions. */
 typedef struct agimp_tuning {
-  int32_t chunk;        /* particles per P2G work item (CTA size): 64, 128 or 256 */
+  int32_t chunk;        /* particles per P2G work item (CTA size): 64, 128, 256 or 512 */
   int32_t ctas_per_sm;  /* CTAs of the grid-stride kernels per multiprocessor, 1..32 */
   float ms_per_substep; /* the autotuner's measurement of this choice (else as set) */
 } agimp_tuning;
 agimp_status agimp_set_tuning(agimp_sim* s, const agimp_tuning* t);
 agimp_status agimp_get_tuning(const agimp_sim* s, agimp_tuning* t);
-/* Measure every (chunk, ctas_per_sm) in {64, 128, 256} x {2, 4, 8, 16}:
+/* Measure every (chunk, ctas_per_sm) in {64, 128, 256, 512} x {2, 4, 8, 16}:
  * two warm-up and `trials` timed substeps each, all from the current state,
  * which is restored afterwards (the simulation does not advance).  Keeps and
  * returns the fastest.  Synchronizes the stream. */

@@ -108,7 +108,7 @@ def test_batched_scene_matches_oracle():
         s.close()
 
 
-@pytest.mark.parametrize("chunk,cps", [(64, 2), (128, 4), (256, 16), (64, 32)])
+@pytest.mark.parametrize("chunk,cps", [(64, 2), (128, 4), (256, 16), (512, 8), (64, 32)])
 @pytest.mark.parametrize("k,scale", [(1, 0.35), (3, 0.3)])
 def test_tuning_choices_match_oracle(chunk, cps, k, scale):
     from agimp import scenes
@@ -140,7 +140,7 @@ def test_autotune_restores_state_and_batch_autotune():
     before = gpu_state(sim)
     n0 = sim.stats()["substeps"]
     best = sim.autotune(scene.dt, trials=2)
-    assert best["chunk"] in (64, 128, 256) and best["ctas_per_sm"] in (2, 4, 8, 16) and best["ms_per_substep"] > 0
+    assert best["chunk"] in (64, 128, 256, 512) and best["ctas_per_sm"] in (2, 4, 8, 16) and best["ms_per_substep"] > 0
     assert sim.tuning["chunk"] == best["chunk"]
     after = gpu_state(sim)
     for key in before:
