@@ -367,6 +367,8 @@ agimp_status agimp_destroy(agimp_sim* s) {
     s->self = nullptr;
   }
   for (void* p : s->allocs) cudaFree(p);
+  if (s->rimg) cudaFree(s->rimg);
+  if (s->rwin) cudaFree(s->rwin);
   if (s->map_dev) cudaFree(s->map_dev);
   if (s->internal) cudaStreamDestroy(s->internal);
   if (s->ev_in) cudaEventDestroy(s->ev_in);
@@ -682,6 +684,24 @@ agimp_status agimp_profile_substep(agimp_sim* s, float dt, float* ms, int32_t n,
   if (st != AGIMP_OK) return from_batch(s, st);
   if (e != cudaSuccess) return cuda_fail(s, e, "profile substep");
   return AGIMP_OK;
+}
+
+// ---------------------------------------------------------------------------
+// headless drawing (gui.py)
+agimp_status agimp_render_mask(agimp_sim* s, int32_t res, int32_t show_ghost, int32_t show_node, float* img,
+                               int32_t memory, void* stream) {
+  if (!s) return AGIMP_INVALID_ARG;
+  CK(cudaSetDevice(s->device));
+  StreamUse su(s, stream);
+  return render_mask(s, res, show_ghost, show_node, img, memory, su.use);
+}
+
+agimp_status agimp_render_particles(agimp_sim* s, int32_t res, float radius, const float* colors,
+                                    int32_t colors_memory, float* img, int32_t memory, void* stream) {
+  if (!s) return AGIMP_INVALID_ARG;
+  CK(cudaSetDevice(s->device));
+  StreamUse su(s, stream);
+  return render_particles(s, res, radius, colors, colors_memory, img, memory, su.use);
 }
 
 // ---------------------------------------------------------------------------

@@ -24,6 +24,10 @@ struct agimp_sim {
   int8_t* map_dev = nullptr;
   long long substeps = 0;
   agimp_batch* self = nullptr;  // the simulator as a batch of one (its substep path)
+  float* rimg = nullptr;        // headless drawing: image scratch for host outputs
+  size_t rimg_floats = 0;
+  int* rwin = nullptr;          // headless drawing: particle covering each pixel
+  size_t rwin_n = 0;
 };
 
 // Several simulators (scenes) stepped together: one launch per kernel serves
@@ -70,4 +74,8 @@ agimp_status batch_step(agimp_batch* b, float dt, int n, cudaStream_t use, cudaE
 int batch_kernels(agimp_batch* b);
 agimp_status batch_autotune(agimp_batch* b, float dt, int trials, agimp_tuning* best, cudaStream_t use);
 agimp_status batch_set_tuning(agimp_batch* b, const agimp_tuning* t);
+// headless drawing (render.cu)
+agimp_status render_mask(agimp_sim* s, int res, int show_ghost, int show_node, float* img, int memory, cudaStream_t st);
+agimp_status render_particles(agimp_sim* s, int res, float radius, const float* colors, int colors_memory, float* img,
+                              int memory, cudaStream_t st);
 }  // namespace agimp

@@ -236,6 +236,26 @@ agimp_status agimp_recorded(agimp_sim* s, int64_t* count, int32_t reset);
 /* bit 0: a tensor-core completion wait timed out.  Synchronizes the device. */
 agimp_status agimp_mlp_errors(agimp_mlp* m, uint32_t* bits, int32_t clear);
 
+/* ---- Headless drawing (2D).  The reference's GUI (gui.py) draws into a GGUI
+ * window; there is no window here, the image goes to a buffer.  img is
+ * [res][res][3] f32 RGB indexed [i][j] like gui.py's bg_img[i, j] (i along x,
+ * j along y). */
+/* GUI.visualize_mask (gui.py:12-43) after the last substep: activated and
+ * (show_ghost) ghost cells of every level, coarse to fine, with their edge
+ * colours, then (show_node) the 3x3-pixel markers of activated, T-junction
+ * and ghost finest nodes.  res >= finest size.  Where markers overlap
+ * (res / finest < 3) each pixel takes the last covering node in row-major
+ * order (the reference's result then depends on its thread order). */
+agimp_status agimp_render_mask(agimp_sim* s, int32_t res, int32_t show_ghost, int32_t show_node, float* img,
+                               int32_t memory, void* stream);
+/* canvas.circles(x_p, radius, per_vertex_color=c_p) (gui.py:69) over img: a
+ * pixel whose centre lies within radius * res pixels of a particle takes the
+ * particle's colour (colors [N][3] in the caller's particle order; later
+ * particles on top).  Allocates its scratch (res^2 ints, and an image for
+ * host img) on first use. */
+agimp_status agimp_render_particles(agimp_sim* s, int32_t res, float radius, const float* colors,
+                                    int32_t colors_memory, float* img, int32_t memory, void* stream);
+
 /* ---- Launch tuning (no counterpart in the reference: Taichi picks its own
  * launch sizes).  Results do not depend on it beyond the order of float
  * additions. */

@@ -1,0 +1,45 @@
+"""The numpy restatement of the reference GUI's mask view (oracle/render_ref.py)
+on hand-made masks: colours, edges and node markers where gui.py:12-43 puts
+them."""
+import numpy as np
+
+import render_ref as R
+
+
+def test_restated_mask_view():
+    # 2 levels, coarsest 4, finest 8, res 24: scale 6 (level 0), 3 (level 1)
+    c0 = np.zeros((4 + 12, 4 + 12), np.int32)
+    c1 = np.zeros((8 + 12, 8 + 12), np.int32)
+    lo = -4
+    c0[0 - lo, 0 - lo] = R.ACT   # level-0 cell (0, 0): pixels [0, 6)^2
+    c1[3 - lo, 3 - lo] = R.ACT   # level-1 cell (3, 3): pixels [9, 12)^2
+    c1[4 - lo, 3 - lo] = R.GHO   # ghost cell (4, 3): pixels [12, 15) x [9, 12)
+    nm = np.zeros((9, 9), np.int32)
+    nm[2, 2] = R.ACT
+    nm[5, 5] = R.TJ
+    nm[6, 6] = R.GHO
+    img = R.render_mask([c0, c1], lo, nm, 4, 24, show_ghost=True, show_node=False)
+    f = lambda c: np.float32(c)
+    assert (img[2, 2] == f(R.ACT_FILL)).all() and (img[0, 3] == f(R.ACT_EDGE)).all()
+    assert (img[10, 10] == f(R.ACT_FILL)).all() and (img[9, 10] == f(R.ACT_EDGE)).all()
+    assert (img[13, 10] == f(R.GHO_FILL)).all() and (img[12, 10] == f(R.GHO_EDGE)).all()
+    assert (img[20, 20] == 0).all()
+    no_ghost = R.render_mask([c0, c1], lo, nm, 4, 24, show_ghost=False, show_node=False)
+    assert (no_ghost[13, 10] == 0).all()
+    with_nodes = R.render_mask([c0, c1], lo, nm, 4, 24, show_ghost=True, show_node=True)
+    # node (2, 2) at pixel (6, 6) (fscale 3): a 3x3 red square
+    assert (with_nodes[5:8, 5:8] == f(R.NODE_ACT)).all()
+    assert (with_nodes[15, 15] == f(R.NODE_TJ)).all() and (with_nodes[18, 18] == f(R.NODE_GHO)).all()
+
+
+def test_restated_particle_circles():
+    img = np.zeros((20, 20, 3), np.float32)
+    x = np.array([[0.5, 0.5], [0.52, 0.5]], np.float32)
+    cols = np.array([[1, 0, 0], [0, 1, 0]], np.float32)
+    R.splat_particles(img, x, cols, radius=0.1)  # 2-pixel radius, centres at (10, 10) and (10.4, 10)
+    assert (img[9, 9] == [0, 1, 0]).all()      # covered by both: the later particle wins
+    assert (img[11, 8] == [0, 1, 0]).all()     # only the second: (11.5-10)^2 + (8.5-10)^2 > 4
+    R.splat_particles(img, x[::-1].copy(), cols[::-1].copy(), radius=0.1)
+    assert (img[9, 9] == [1, 0, 0]).all()      # drawn in the other order
+    assert (img[11, 8] == [0, 1, 0]).all()
+    assert (img[0, 0] == 0).all()
