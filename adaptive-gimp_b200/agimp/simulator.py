@@ -64,15 +64,27 @@ class ParticleField:
         args[self._ORDER.index(self.name)] = buf
         return args
 
-    def to_numpy(self, out=None):
-        """Copy to host memory (into `out` when given, e.g. a pinned buffer)."""
+    def to_numpy(self, out=None, blocking=True, stream=None):
+        """Copy to host memory (into `out` when given, e.g. a pinned buffer).
+
+        blocking=False enqueues the copy on `stream` (a CUDA stream handle;
+        default the current torch stream) and returns at once: `out` (required,
+        pinned for the copy to overlap) holds the state once that stream has
+        run the copy.  The next substep may run meanwhile; the library orders
+        whatever would overwrite this state after the copy."""
         if out is None:
+            if not blocking:
+                raise ValueError("an asynchronous copy needs `out`")
             out = np.empty(self.shape, self.dtype)
         elif out.shape != self.shape or out.dtype != self.dtype or not out.flags.c_contiguous:
             raise ValueError("out must be a C-contiguous %s array of shape %s" % (np.dtype(self.dtype), self.shape))
         a = self._args(_ptr(out))
         s = self.sim
-        _capi.check(s._L.agimp_get_particles(s._h, *a, AGIMP_MEM_HOST, None), s._h, "get " + self.name)
+        if blocking:
+            _capi.check(s._L.agimp_get_particles(s._h, *a, AGIMP_MEM_HOST, stream), s._h, "get " + self.name)
+        else:
+            st = stream if stream is not None else _torch_stream()
+            _capi.check(s._L.agimp_get_particles_async(s._h, *a, st), s._h, "get " + self.name)
         return out
 
     def from_numpy(self, arr):

@@ -168,6 +168,8 @@ agimp_status batch_step(agimp_batch* b, float dt, int n, cudaStream_t use, cudaE
     if (st != AGIMP_OK) return st;
   }
   for (int i = 0; i < n; ++i) {
+    // the substep writes each scene's other buffer: wait for readbacks of it
+    for (agimp_sim* s : b->sims) wait_readback(s, 1 - s->par, use);
     const int ph = b->single ? b->sims[0]->par : (int)(b->steps & 1);
     agimp_status st = sync_contexts(b, ph, dt, use);
     if (st != AGIMP_OK) return st;
@@ -199,7 +201,18 @@ agimp_status batch_step(agimp_batch* b, float dt, int n, cudaStream_t use, cudaE
     }
     b->steps += 1;
   }
+  // state-ready marks for asynchronous readbacks (a batch of one always
+  // records it; larger batches only for scenes that read asynchronously)
+  for (agimp_sim* s : b->sims)
+    if ((b->single || s->async_used) && n > 0) BCK(cudaEventRecord(s->ev_state, use));
   return AGIMP_OK;
+}
+
+void wait_readback(agimp_sim* s, int buf, cudaStream_t use) {
+  if (s->read_pending[buf]) {
+    cudaStreamWaitEvent(use, s->ev_read[buf], 0);
+    s->read_pending[buf] = false;
+  }
 }
 
 int batch_kernels(agimp_batch* b) {

@@ -337,7 +337,10 @@ agimp_status agimp_create(const agimp_params* p, int32_t device, agimp_sim** out
 #undef AL
   if (cudaStreamCreateWithFlags(&s->internal, cudaStreamNonBlocking) != cudaSuccess ||
       cudaEventCreateWithFlags(&s->ev_in, cudaEventDisableTiming) != cudaSuccess ||
-      cudaEventCreateWithFlags(&s->ev_out, cudaEventDisableTiming) != cudaSuccess) {
+      cudaEventCreateWithFlags(&s->ev_out, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&s->ev_state, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&s->ev_read[0], cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&s->ev_read[1], cudaEventDisableTiming) != cudaSuccess) {
     agimp_destroy(s);
     return AGIMP_CUDA_ERROR;
   }
@@ -368,6 +371,9 @@ agimp_status agimp_destroy(agimp_sim* s) {
   }
   for (void* p : s->allocs) cudaFree(p);
   if (s->rimg) cudaFree(s->rimg);
+  if (s->astage) cudaFree(s->astage);
+  for (cudaEvent_t e : {s->ev_state, s->ev_read[0], s->ev_read[1]})
+    if (e) cudaEventDestroy(e);
   if (s->rwin) cudaFree(s->rwin);
   if (s->map_dev) cudaFree(s->map_dev);
   if (s->internal) cudaStreamDestroy(s->internal);
@@ -433,6 +439,7 @@ agimp_status agimp_set_particles(agimp_sim* s, const float* x, const float* v, c
   if (!s || (memory != AGIMP_MEM_DEVICE && memory != AGIMP_MEM_HOST)) return fail(s, AGIMP_INVALID_ARG, "bad args");
   CK(cudaSetDevice(s->device));
   StreamUse su(s, stream);
+  wait_readback(s, s->par, su.use);  // the upload overwrites the state being read
   const int D = s->c.dim;
   const Particles& P = s->buf[s->par];
   agimp_status r;
@@ -463,6 +470,62 @@ agimp_status agimp_get_particles(agimp_sim* s, float* x, float* v, float* F, flo
   if (Jp && (r = download_soa(s, P.Jp, Jp, 1, memory, su.use))) return r;
   if (g && (r = copy_i32(s, P.g, g, 0, memory, su.use))) return r;
   if (fl && (r = copy_i32(s, P.fl, fl, 0, memory, su.use))) return r;
+  return AGIMP_OK;
+}
+
+agimp_status agimp_get_particles_async(agimp_sim* s, float* x, float* v, float* F, float* C, float* m, int32_t* g,
+                                       int32_t* fl, float* Jp, void* stream) {
+  if (!s) return AGIMP_INVALID_ARG;
+  CK(cudaSetDevice(s->device));
+  StreamUse su(s, stream);
+  const long long N = s->c.N;
+  const int D = s->c.dim;
+  const int k = s->par;
+  const Particles& P = s->buf[k];
+  if (!s->async_used) {
+    // from now on every substep marks when the state is ready; the substeps
+    // issued so far were ordered before this call on the library's streams
+    s->async_used = true;
+    CK(cudaEventRecord(s->ev_state, su.use));
+  }
+  CK(cudaStreamWaitEvent(su.use, s->ev_state, 0));  // the state is written
+  if (s->last_read >= 0) CK(cudaStreamWaitEvent(su.use, s->ev_read[s->last_read], 0));  // staging is free
+  const size_t need = (size_t)N * (2 * D + 2 * D * D + 4) + 16;
+  if (need > s->astage_floats) {
+    CK(cudaStreamSynchronize(su.use));
+    if (s->astage) cudaFree(s->astage);
+    s->astage = nullptr;
+    s->astage_floats = 0;
+    CK(cudaMalloc(&s->astage, need * sizeof(float)));
+    s->astage_floats = need;
+  }
+  float* st = s->astage;
+  auto field = [&](const float* src, float* dst, int comps) -> cudaError_t {
+    if (!dst || !N) return cudaSuccess;
+    k_soa_to_aos<<<gs_blocks(N * comps), 256, 0, su.use>>>(src, P.id, st, N, comps);
+    cudaError_t e = cudaMemcpyAsync(dst, st, N * comps * sizeof(float), cudaMemcpyDeviceToHost, su.use);
+    st += N * comps;
+    return e;
+  };
+  auto ifield = [&](const int32_t* src, int32_t* dst) -> cudaError_t {
+    if (!dst || !N) return cudaSuccess;
+    k_i32_out<<<gs_blocks(N), 256, 0, su.use>>>(src, P.id, (int32_t*)st, N);
+    cudaError_t e = cudaMemcpyAsync(dst, st, N * sizeof(int32_t), cudaMemcpyDeviceToHost, su.use);
+    st += N;
+    return e;
+  };
+  CK(field(P.x, x, D));
+  CK(field(P.v, v, D));
+  CK(field(P.F, F, D * D));
+  CK(field(P.C, C, D * D));
+  CK(field(P.m, m, 1));
+  CK(field(P.Jp, Jp, 1));
+  CK(ifield(P.g, g));
+  CK(ifield(P.fl, fl));
+  CK(cudaGetLastError());
+  CK(cudaEventRecord(s->ev_read[k], su.use));
+  s->read_pending[k] = true;
+  s->last_read = k;
   return AGIMP_OK;
 }
 
@@ -523,6 +586,7 @@ agimp_status agimp_refine_levels(agimp_sim* s, int32_t band, void* stream) {
   if (!s || band < 1 || band > 32) return fail(s, AGIMP_INVALID_ARG, "band must be in [1, 32]");
   CK(cudaSetDevice(s->device));
   StreamUse su(s, stream);
+  wait_readback(s, s->par, su.use);  // g_p of the state being read is rewritten
   launch_refine(cur(s), band, su.use);
   CK(cudaGetLastError());
   return AGIMP_OK;

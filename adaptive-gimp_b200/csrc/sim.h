@@ -24,6 +24,15 @@ struct agimp_sim {
   int8_t* map_dev = nullptr;
   long long substeps = 0;
   agimp_batch* self = nullptr;  // the simulator as a batch of one (its substep path)
+  // asynchronous readback: the state is ready after ev_state; a copy of
+  // buffer k is in flight until ev_read[k]
+  bool async_used = false;
+  cudaEvent_t ev_state = nullptr;
+  cudaEvent_t ev_read[2] = {nullptr, nullptr};
+  bool read_pending[2] = {false, false};
+  int last_read = -1;           // buffer of the last asynchronous readback (its staging is busy until ev_read)
+  float* astage = nullptr;      // staging of asynchronous readbacks
+  size_t astage_floats = 0;
   float* rimg = nullptr;        // headless drawing: image scratch for host outputs
   size_t rimg_floats = 0;
   int* rwin = nullptr;          // headless drawing: particle covering each pixel
@@ -72,6 +81,8 @@ void batch_drop_graphs(agimp_batch* b);
 // and no graph.
 agimp_status batch_step(agimp_batch* b, float dt, int n, cudaStream_t use, cudaEvent_t* ev);
 int batch_kernels(agimp_batch* b);
+// make `use` wait for asynchronous readbacks of the buffer the next work writes
+void wait_readback(agimp_sim* s, int buf, cudaStream_t use);
 agimp_status batch_autotune(agimp_batch* b, float dt, int trials, agimp_tuning* best, cudaStream_t use);
 agimp_status batch_set_tuning(agimp_batch* b, const agimp_tuning* t);
 // headless drawing (render.cu)

@@ -622,26 +622,42 @@ def e2e_run(a, scene, local, sur=None, tuning=None):
     hm[:] = scene.m
     hg[:] = scene.g
     hJ[:] = 1
-    out = pinned((n, d))
+    outs = [pinned((n, d)), pinned((n, d))]
     sim = scene.build(device=local)
     if tuning:
         sim.set_tuning(tuning["chunk"], tuning["ctas_per_sm"])
     if sur:
         sim.set_surrogate(*sur)
+    import ctypes
+    main_s, copy_s = torch.cuda.Stream(), torch.cuda.Stream()
+    sm, sc = ctypes.c_void_p(main_s.cuda_stream), ctypes.c_void_p(copy_s.cuda_stream)
+    done = [None, None]
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     sim.set_particles(x=hx, v=hv, F=hF, C=hC, m=hm, g=hg, Jp=hJ)
     for i in range(a.steps):
         if scene.refine_every and i % scene.refine_every == 0:
-            sim.refine_levels(scene.refine_band)
-        sim.substep(scene.dt)
-        sim.x_p.to_numpy(out=out)
-    torch.cuda.synchronize()
+            sim.refine_levels(scene.refine_band, stream=sm)
+        sim.substep(scene.dt, stream=sm)
+        # x_p of this substep into one of two pinned buffers on a copy stream;
+        # the next substep runs meanwhile.  The host takes a buffer back only
+        # after its copy has landed.
+        k = i % 2
+        if done[k] is not None:
+            done[k].synchronize()
+        sim.x_p.to_numpy(out=outs[k], blocking=False, stream=sc)
+        done[k] = torch.cuda.Event()
+        done[k].record(copy_s)
+    for e in done:
+        if e is not None:
+            e.synchronize()
     el = time.perf_counter() - t0
     sim.close()
     h2d = n * 4 * (2 * d + 2 * d * d + 3)
     return {"value": n * a.steps / el, "unit": METRIC, "h2d_bytes_per_step": h2d / a.steps,
-            "d2h_bytes_per_step": n * d * 4, "timing": "wall clock, host-synchronous readback every substep",
+            "d2h_bytes_per_step": n * d * 4,
+            "timing": "wall clock; every substep's x_p read back to pinned host memory (asynchronous copy on a "
+                      "second stream overlapping the next substep, double-buffered, all landed before the clock stops)",
             "note": "h2d is the one-time upload of the scene state spread over the timed substeps"}
 
 

@@ -122,6 +122,18 @@ agimp_status agimp_set_particles(agimp_sim* s, const float* x, const float* v, c
 agimp_status agimp_get_particles(agimp_sim* s, float* x, float* v, float* F, float* C, float* m, int32_t* g,
                                  int32_t* fl, float* Jp, int32_t memory, void* stream);
 
+/* Asynchronous field readback into HOST memory (pinned, for the copy to
+ * overlap): enqueues the copy of the current state on `stream` and returns at
+ * once; the outputs hold the state once `stream` has run the enqueued work
+ * (synchronize it or wait on an event recorded after the call).  No counterpart
+ * in the reference (Taichi's to_numpy blocks).  The copy waits for the
+ * substeps already issued, and later substeps, uploads or refinements that
+ * would overwrite the state being copied wait for the copy, whatever streams
+ * they use: the state of substep k can be read while substep k+1 runs.
+ * Allocates its staging (N x (2 dim + 2 dim^2 + 4) floats) on first use. */
+agimp_status agimp_get_particles_async(agimp_sim* s, float* x, float* v, float* F, float* C, float* m, int32_t* g,
+                                       int32_t* fl, float* Jp, void* stream);
+
 /* Replaces the grid_initializer hook and static adaptivity
  * (adaptive_gimp.py:65-66, 72-85; init.py:34-98).  `table` tabulates the
  * initializer over finest cells [-halo, finest+halo)^dim, first axis slowest:

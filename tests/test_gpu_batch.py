@@ -187,3 +187,36 @@ def test_batch_rejects_surrogate_and_mixed_dims():
     batch.close()
     for s in (a, b, c3):
         s.close()
+
+
+def test_async_readback_overlaps_next_substep():
+    """x_p read asynchronously on a copy stream while the following substeps
+    run on another stream equals the state a blocking read returns at the
+    same substep (the library orders the overwrite after the copy)."""
+    import ctypes
+
+    import torch
+
+    from agimp import scenes
+    sc = scenes.make_config(3, scale=0.3)
+    a, b = sc.build(), sc.build()
+    main_s, copy_s = torch.cuda.Stream(), torch.cuda.Stream()
+    sm, scp = ctypes.c_void_p(main_s.cuda_stream), ctypes.c_void_p(copy_s.cuda_stream)
+    steps = 12
+    outs = [torch.empty((sc.n, 3), dtype=torch.float32, pin_memory=True).numpy() for _ in range(steps)]
+    ref = []
+    for i in range(steps):
+        if i % sc.refine_every == 0:
+            a.refine_levels(sc.refine_band, stream=sm)
+            b.refine_levels(sc.refine_band)
+        a.substep(sc.dt, stream=sm)
+        a.x_p.to_numpy(out=outs[i], blocking=False, stream=scp)
+        b.substep(sc.dt)
+        ref.append(b.x_p.to_numpy())
+    copy_s.synchronize()
+    main_s.synchronize()
+    for i in range(steps):
+        assert np.abs(outs[i] - ref[i]).max() <= 1e-5, (i, np.abs(outs[i] - ref[i]).max())
+    assert a.stats()["substeps"] == steps
+    a.close()
+    b.close()
