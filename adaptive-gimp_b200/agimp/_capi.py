@@ -33,7 +33,7 @@ EXPORTS = (
     "agimp_batch_create", "agimp_batch_destroy", "agimp_batch_last_error", "agimp_batch_substep",
     "agimp_batch_set_graphs", "agimp_batch_set_tuning", "agimp_batch_get_tuning", "agimp_batch_autotune",
     "agimp_batch_kernels_per_substep", "agimp_batch_profile_substep",
-    "agimp_render_mask", "agimp_render_particles", "agimp_get_particles_async",
+    "agimp_render_mask", "agimp_render_particles", "agimp_get_particles_async", "agimp_batch_positions_async",
 )
 PHASES = ("blocks", "topology", "binning", "p2g", "restrict", "gridop", "prolong", "g2p")
 
@@ -134,6 +134,7 @@ def load(path: str | None = None):
     L.agimp_batch_kernels_per_substep.restype = ctypes.c_int32
     L.agimp_batch_profile_substep.argtypes = [vp, ctypes.c_float, fp, ctypes.c_int32, vp]
     L.agimp_get_particles_async.argtypes = [vp, vp, vp, vp, vp, vp, vp, vp, vp, vp]
+    L.agimp_batch_positions_async.argtypes = [vp, vp, vp]
     L.agimp_render_mask.argtypes = [vp, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, vp, ctypes.c_int32, vp]
     L.agimp_render_particles.argtypes = [vp, ctypes.c_int32, ctypes.c_float, vp, ctypes.c_int32, vp, ctypes.c_int32, vp]
     _lib = L

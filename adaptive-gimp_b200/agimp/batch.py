@@ -73,5 +73,26 @@ class SceneBatch:
                     "batch profile", batch=True)
         return dict(zip(_capi.PHASES, list(ms)))
 
+    def positions(self, out=None, blocking=True, stream=None):
+        """x_p of every scene, concatenated in batch order ([sum of N][dim]).
+        blocking=False returns at once (out required, pinned for overlap); the
+        copy has landed once `stream` has run it."""
+        import numpy as np
+        dim = self.sims[0].dim if self.sims else 2
+        shape = (self.n_particles, dim)
+        if out is None:
+            if not blocking:
+                raise ValueError("an asynchronous copy needs `out`")
+            out = np.empty(shape, np.float32)
+        elif out.shape != shape or out.dtype != np.float32 or not out.flags.c_contiguous:
+            raise ValueError("out must be a C-contiguous float32 array of shape %s" % (shape,))
+        st = stream if stream is not None else _torch_stream()
+        _capi.check(self._L.agimp_batch_positions_async(self._h, ctypes.c_void_p(out.ctypes.data), st), self._h,
+                    "batch positions", batch=True)
+        if blocking:
+            import torch
+            torch.cuda.synchronize()
+        return out
+
     def kernels_per_substep(self):
         return int(self._L.agimp_batch_kernels_per_substep(self._h))

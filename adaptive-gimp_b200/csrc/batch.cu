@@ -50,6 +50,8 @@ agimp_status batch_init(agimp_batch* b) {
     BCK(cudaStreamCreateWithFlags(&b->internal, cudaStreamNonBlocking));
     BCK(cudaEventCreateWithFlags(&b->ev_in, cudaEventDisableTiming));
     BCK(cudaEventCreateWithFlags(&b->ev_out, cudaEventDisableTiming));
+    BCK(cudaEventCreateWithFlags(&b->ev_done, cudaEventDisableTiming));
+    BCK(cudaEventCreateWithFlags(&b->ev_read, cudaEventDisableTiming));
   }
   return AGIMP_OK;
 }
@@ -70,6 +72,13 @@ void batch_free(agimp_batch* b) {
   if (b->internal) cudaStreamDestroy(b->internal);
   if (b->ev_in) cudaEventDestroy(b->ev_in);
   if (b->ev_out) cudaEventDestroy(b->ev_out);
+  if (b->ev_done) cudaEventDestroy(b->ev_done);
+  if (b->ev_read) cudaEventDestroy(b->ev_read);
+  if (b->xstage) cudaFree(b->xstage);
+  if (b->dsrc) cudaFree(b->dsrc);
+  b->ev_done = b->ev_read = nullptr;
+  b->xstage = nullptr;
+  b->dsrc = nullptr;
   b->dctx[0] = b->dctx[1] = nullptr;
   b->dofs = nullptr;
   b->internal = nullptr;
@@ -170,6 +179,10 @@ agimp_status batch_step(agimp_batch* b, float dt, int n, cudaStream_t use, cudaE
   for (int i = 0; i < n; ++i) {
     // the substep writes each scene's other buffer: wait for readbacks of it
     for (agimp_sim* s : b->sims) wait_readback(s, 1 - s->par, use);
+    if (b->read_pending && b->steps > b->read_step) {  // the batch copy read those buffers
+      BCK(cudaStreamWaitEvent(use, b->ev_read, 0));
+      b->read_pending = false;
+    }
     const int ph = b->single ? b->sims[0]->par : (int)(b->steps & 1);
     agimp_status st = sync_contexts(b, ph, dt, use);
     if (st != AGIMP_OK) return st;
@@ -205,6 +218,74 @@ agimp_status batch_step(agimp_batch* b, float dt, int n, cudaStream_t use, cudaE
   // records it; larger batches only for scenes that read asynchronously)
   for (agimp_sim* s : b->sims)
     if ((b->single || s->async_used) && n > 0) BCK(cudaEventRecord(s->ev_state, use));
+  if (b->ev_done && n > 0) BCK(cudaEventRecord(b->ev_done, use));
+  return AGIMP_OK;
+}
+
+namespace {
+struct GatherSrc {
+  const float* x;
+  const int32_t* id;
+  long long N, off;
+};
+
+// every scene's positions, in its caller's particle order, at its offset
+template <int D>
+__global__ void k_gather_x(const int* ofs, int n, const GatherSrc* src, float* out) {
+  const int cta = (int)blockIdx.x;
+  int lo = 0, hi = n - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (ofs[mid] <= cta)
+      lo = mid;
+    else
+      hi = mid - 1;
+  }
+  const GatherSrc g = src[lo];
+  const int bid = cta - ofs[lo], nblk = ofs[lo + 1] - ofs[lo];
+  for (long long s = bid * (long long)blockDim.x + threadIdx.x; s < g.N; s += (long long)nblk * blockDim.x) {
+    const long long o = (g.off + g.id[s]) * D;
+#pragma unroll
+    for (int d = 0; d < D; ++d) out[o + d] = g.x[d * g.N + s];
+  }
+}
+}  // namespace
+
+agimp_status batch_positions_async(agimp_batch* b, float* x, cudaStream_t use) {
+  BCK(cudaSetDevice(b->device));
+  if (b->single || !x) {
+    b->err = "batch positions: a batch of several scenes and an output are required";
+    return AGIMP_INVALID_ARG;
+  }
+  if (!b->maps_valid) {
+    const agimp_status st = build_maps(b, use);
+    if (st != AGIMP_OK) return st;
+  }
+  const int n = (int)b->sims.size();
+  std::vector<GatherSrc> src(n);
+  long long tot = 0;
+  for (int i = 0; i < n; ++i) {
+    agimp_sim* s = b->sims[i];
+    src[i] = GatherSrc{s->buf[s->par].x, s->buf[s->par].id, (long long)s->c.N, tot};
+    tot += s->c.N;
+  }
+  if (!b->xstage) {
+    BCK(cudaMalloc(&b->xstage, std::max<long long>(tot * b->dim, 1) * sizeof(float)));
+    BCK(cudaMalloc(&b->dsrc, sizeof(GatherSrc) * n));
+  }
+  BCK(cudaStreamWaitEvent(use, b->ev_done, 0));  // the batch's last substep is written
+  if (b->read_pending) BCK(cudaStreamWaitEvent(use, b->ev_read, 0));  // the staging is free
+  BCK(cudaMemcpyAsync(b->dsrc, src.data(), sizeof(GatherSrc) * n, cudaMemcpyHostToDevice, use));
+  const int G = b->nct[MAP_G];
+  if (b->dim == 2)
+    k_gather_x<2><<<G, 256, 0, use>>>(b->dofs + MAP_G * (n + 1), n, (const GatherSrc*)b->dsrc, b->xstage);
+  else
+    k_gather_x<3><<<G, 256, 0, use>>>(b->dofs + MAP_G * (n + 1), n, (const GatherSrc*)b->dsrc, b->xstage);
+  BCK(cudaGetLastError());
+  BCK(cudaMemcpyAsync(x, b->xstage, tot * b->dim * sizeof(float), cudaMemcpyDeviceToHost, use));
+  BCK(cudaEventRecord(b->ev_read, use));
+  b->read_pending = true;
+  b->read_step = b->steps;
   return AGIMP_OK;
 }
 

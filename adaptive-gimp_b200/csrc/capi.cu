@@ -897,6 +897,12 @@ agimp_status agimp_batch_profile_substep(agimp_batch* b, float dt, float* ms, in
   return AGIMP_OK;
 }
 
+agimp_status agimp_batch_positions_async(agimp_batch* b, float* x, void* stream) {
+  if (!b) return AGIMP_INVALID_ARG;
+  BatchStream bs(b, stream);
+  return batch_positions_async(b, x, bs.use);
+}
+
 int32_t agimp_batch_kernels_per_substep(const agimp_batch* b) {
   return b ? batch_kernels(const_cast<agimp_batch*>(b)) : 0;
 }

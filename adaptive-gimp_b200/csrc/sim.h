@@ -68,6 +68,13 @@ struct agimp_batch {
   cudaStream_t internal = nullptr;  // used when the caller passes no stream (own batches only)
   cudaEvent_t ev_in = nullptr, ev_out = nullptr;
   std::string err;
+  // batch readback of positions (own batches only): the last step's work is
+  // done at ev_done; a copy started after `read_step` steps ends at ev_read
+  cudaEvent_t ev_done = nullptr, ev_read = nullptr;
+  bool read_pending = false;
+  long long read_step = 0;
+  float* xstage = nullptr;
+  void* dsrc = nullptr;  // per-scene sources of the gather
 };
 
 namespace agimp {
@@ -81,6 +88,7 @@ void batch_drop_graphs(agimp_batch* b);
 // and no graph.
 agimp_status batch_step(agimp_batch* b, float dt, int n, cudaStream_t use, cudaEvent_t* ev);
 int batch_kernels(agimp_batch* b);
+agimp_status batch_positions_async(agimp_batch* b, float* x, cudaStream_t use);
 // make `use` wait for asynchronous readbacks of the buffer the next work writes
 void wait_readback(agimp_sim* s, int buf, cudaStream_t use);
 agimp_status batch_autotune(agimp_batch* b, float dt, int trials, agimp_tuning* best, cudaStream_t use);

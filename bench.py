@@ -511,7 +511,7 @@ def run_batch(a):
         "device_errors": int(np.bitwise_or.reduce(errors)),
     }
     if not a.no_e2e:
-        out["e2e"] = e2e_batch(a, sc, local)
+        out["e2e"] = e2e_batch(a, sc, local, tuning)
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         threads = os.cpu_count() or 1
         val, done, el, ns = cpu_oracle_batch(sc, a.cpu_seconds, threads)
@@ -557,10 +557,10 @@ def cpu_oracle_batch(sc, seconds, threads, steps=3):
     return work / el, steps, el, k
 
 
-def e2e_batch(a, sc, local):
+def e2e_batch(a, sc, local, tuning=None):
     """Same metric through the public API with host buffers: every scene is
-    uploaded from pinned host memory, then per substep the batch steps and
-    every scene's x_p is read back into pinned host memory."""
+    uploaded from pinned host memory, then per substep the batch steps and all
+    scenes' positions are read back into pinned host memory."""
     import numpy as np
     import torch
 
@@ -579,27 +579,43 @@ def e2e_batch(a, sc, local):
         h["C"][:] = 0
         h["m"][:] = s.m
         h["g"][:] = s.g
-        h["out"] = torch.empty((n, d), dtype=torch.float32, pin_memory=True).numpy()
         hosts.append(h)
     n_tot = sum(s.n for s in sc)
+    if tuning:
+        batch.set_tuning(tuning["chunk"], tuning["ctas_per_sm"])
+    import ctypes
+    main_s, copy_s = torch.cuda.Stream(), torch.cuda.Stream()
+    sm, scp = ctypes.c_void_p(main_s.cuda_stream), ctypes.c_void_p(copy_s.cuda_stream)
+    outs = [torch.empty((n_tot, 2), dtype=torch.float32, pin_memory=True).numpy() for _ in range(2)]
+    done = [None, None]
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     for sim, h in zip(sims, hosts):
         sim.set_particles(x=h["x"], v=h["v"], F=h["F"], C=h["C"], m=h["m"], g=h["g"])
     for i in range(a.steps):
-        batch.substep(sc[0].dt)
-        for sim, h in zip(sims, hosts):
-            if sim.n_particles:
-                sim.x_p.to_numpy(out=h["out"])
-    torch.cuda.synchronize()
+        batch.substep(sc[0].dt, stream=sm)
+        # every scene's x_p in one gathered copy on a copy stream, overlapping
+        # the next substep; double-buffered
+        k = i % 2
+        if done[k] is not None:
+            done[k].synchronize()
+        batch.positions(out=outs[k], blocking=False, stream=scp)
+        done[k] = torch.cuda.Event()
+        done[k].record(copy_s)
+    for e in done:
+        if e is not None:
+            e.synchronize()
     el = time.perf_counter() - t0
     batch.close()
     for s in sims:
         s.close()
     h2d = sum(s.n * 4 * (2 * 2 + 2 * 4 + 2) for s in sc)
     return {"value": n_tot * a.steps / el, "unit": METRIC, "h2d_bytes_per_step": h2d / a.steps,
-            "d2h_bytes_per_step": n_tot * 2 * 4, "timing": "wall clock, host-synchronous readback of every scene "
-            "every substep", "note": "h2d is the one-time upload of the scenes spread over the timed substeps"}
+            "d2h_bytes_per_step": n_tot * 2 * 4,
+            "timing": "wall clock; every substep's positions of all scenes read back to pinned host memory in one "
+                      "asynchronous gathered copy overlapping the next substep, double-buffered, all landed before "
+                      "the clock stops",
+            "note": "h2d is the one-time upload of the scenes spread over the timed substeps"}
 
 
 def e2e_run(a, scene, local, sur=None, tuning=None):

@@ -303,6 +303,14 @@ agimp_status agimp_batch_get_tuning(const agimp_batch* b, agimp_tuning* t);
 /* As agimp_autotune, over the whole batch. */
 agimp_status agimp_batch_autotune(agimp_batch* b, float dt, int32_t trials, agimp_tuning* best, void* stream);
 int32_t agimp_batch_kernels_per_substep(const agimp_batch* b);
+/* Positions of all scenes in one copy: x [sum of N][dim] in HOST memory
+ * (pinned, for overlap), scene after scene in batch order, each scene in its
+ * caller's particle order.  Asynchronous like agimp_get_particles_async: the
+ * copy waits for the batch's substeps already issued, and the batch's second
+ * substep after it waits for the copy, so a copy overlaps the next substep.
+ * (Orders only against the batch's own steps.)  Allocates its staging on first
+ * use. */
+agimp_status agimp_batch_positions_async(agimp_batch* b, float* x, void* stream);
 /* As agimp_profile_substep, for one substep of the whole batch. */
 agimp_status agimp_batch_profile_substep(agimp_batch* b, float dt, float* ms, int32_t n, void* stream);
 

@@ -220,3 +220,39 @@ def test_async_readback_overlaps_next_substep():
     assert a.stats()["substeps"] == steps
     a.close()
     b.close()
+
+
+def test_batch_positions_readback():
+    """One gathered copy of all scenes' positions equals the per-simulator
+    readbacks, also when taken asynchronously while the batch keeps stepping."""
+    import ctypes
+
+    import torch
+
+    from agimp.batch import SceneBatch
+    sc = _batch_scenes()[:5] + [_batch_scenes()[6]]  # static scenes and the empty one
+    sims = [s.build() for s in sc]
+    batch = SceneBatch(sims)
+    batch.substep(sc[0].dt, 3)
+    whole = batch.positions()
+    np.testing.assert_array_equal(whole, np.concatenate([s.x_p.to_numpy() for s in sims]))
+    main_s, copy_s = torch.cuda.Stream(), torch.cuda.Stream()
+    sm, scp = ctypes.c_void_p(main_s.cuda_stream), ctypes.c_void_p(copy_s.cuda_stream)
+    outs = [torch.empty(whole.shape, dtype=torch.float32, pin_memory=True).numpy() for _ in range(4)]
+    ref = [s.build() for s in sc]
+    rbatch = SceneBatch(ref)
+    rbatch.substep(sc[0].dt, 3)
+    refs = []
+    for i in range(4):
+        batch.substep(sc[0].dt, stream=sm)
+        batch.positions(out=outs[i], blocking=False, stream=scp)
+        rbatch.substep(sc[0].dt)
+        refs.append(rbatch.positions())
+    copy_s.synchronize()
+    main_s.synchronize()
+    for i in range(4):
+        assert np.abs(outs[i] - refs[i]).max() <= 1e-5, i
+    batch.close()
+    rbatch.close()
+    for s in sims + ref:
+        s.close()
