@@ -298,8 +298,12 @@ agimp_status agimp_create(const agimp_params* p, int32_t device, agimp_sim** out
   AL(c.touch_list, Vf.nblocks);
   cudaMemset(c.touch_flag, 0, Vf.nblocks * sizeof(uint32_t));
   AL(c.bin_count, tot_blocks + 1);  // + the bin of particles without a level
-  AL(c.bin_start, tot_blocks + 1);
   cudaMemset(c.bin_count, 0, (tot_blocks + 1) * sizeof(int32_t));
+  AL(c.cell_count, (tot_blocks + 1) * per);
+  AL(c.cell_off, (tot_blocks + 1) * per);
+  AL(c.bin_start, tot_blocks + 1);
+  AL(c.full_bins, tot_blocks + 1);
+  cudaMemset(c.cell_count, 0, (tot_blocks + 1) * per * sizeof(int32_t));
   const long long N = c.N;
   AL(c.chunks, N / MIN_CHUNK + tot_blocks + 2);  // enough for any work-item size
   c.chunk = CHUNK;

@@ -47,6 +47,7 @@ enum {
   CTR_SURFB = 15,  // surrogate predictions rejected (exact return map used instead)
   // [16, 22): particle bounding box used by the refinement rule
   CTR_PROJ = 22,   // particles whose trial state needs the return map this substep
+  CTR_FULL = 23,   // non-empty bins this substep (listed in full_bins)
   CTR_COUNT = 24
 };
 
@@ -87,10 +88,13 @@ struct Ctx {
   int32_t* ctr;
   uint32_t* touch_flag;
   int32_t* touch_list;
-  int32_t* bin_count;
+  int32_t* bin_count;   // [bins]: particles per bin
+  int32_t* cell_count;  // [bins][4^d]: particles per (bin, base cell inside the bin's block)
+  int32_t* cell_off;    // [bins][4^d]: their offsets inside the bin (particles of a bin are cell-sorted)
   int32_t* bin_start;
+  int32_t* full_bins;   // [bins]: the non-empty bins of this substep
   int4* chunks;  // {level, block (stored linear id), start, count}
-  int32_t* bin_of;
+  int32_t* bin_of;      // per particle: bin * 4^d + base cell
   int32_t* rank_of;
   int32_t* perm;
   int32_t* proj;  // [N] slots of the particles listed for the return map (CTR_PROJ of them)

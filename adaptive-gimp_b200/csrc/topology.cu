@@ -51,6 +51,7 @@ __global__ void k_clear(Batch B) {
     c.ctr[CTR_SUR] = 0;
     c.ctr[CTR_SURFB] = 0;
     c.ctr[CTR_PROJ] = 0;
+    c.ctr[CTR_FULL] = 0;
   }
   const long long tot = total_elems(c, 0, c.L, D);
   SCENE_LOOP(e, tot) {
@@ -468,11 +469,14 @@ __device__ __forceinline__ void bin_one(const Ctx& c, int p) {
         const LevelDev& V = c.lev[fl];
         long long b = 0;
         bool ok = true;
+        int cell = 0;
 #pragma unroll
         for (int d = 0; d < D; ++d) {
-          const int cb = ((((int)(xp[d] * inv + 0.5f)) - 1) >> 2) + 1;
+          const int base = ((int)(xp[d] * inv + 0.5f)) - 1;
+          const int cb = (base >> 2) + 1;
           ok = ok && cb >= 0 && cb < V.nb;
           b = b * V.nb + cb;
+          cell = (cell << 2) | (base & 3);  // base cell inside the block
         }
         const int bi = ok ? V.bmap[b] : -1;
         if (bi < 0) {
@@ -481,18 +485,24 @@ __device__ __forceinline__ void bin_one(const Ctx& c, int p) {
         } else {
           int lb = 0;
           for (int q = 0; q < fl; ++q) lb += c.ctr[CTR_LEVEL + q];
-          bin = lb + bi;
+          bin = ((lb + bi) << (2 * D)) | cell;
         }
       }
     }
-    if (fl < 0) bin = nbins;  // the extra bin
+    if (fl < 0) bin = nbins << (2 * D);  // the extra bin
     c.P.fl[p] = fl;
+  }
+  // bin sizes and the rank inside the (bin, cell): warp-aggregated atomics
+  {
+    const int b = bin >= 0 ? bin >> (2 * D) : -1;
+    const unsigned gb = __match_any_sync(0xffffffffu, b);
+    if (b >= 0 && lane == __ffs(gb) - 1) atomicAdd(&c.bin_count[b], __popc(gb));
   }
   const unsigned grp = __match_any_sync(0xffffffffu, bin);
   const int leader = __ffs(grp) - 1;
   const int rank = __popc(grp & ((1u << lane) - 1u));
   int base = 0;
-  if (bin >= 0 && lane == leader) base = atomicAdd(&c.bin_count[bin], __popc(grp));
+  if (bin >= 0 && lane == leader) base = atomicAdd(&c.cell_count[bin], __popc(grp));
   base = __shfl_sync(0xffffffffu, base, leader);
   if (bin >= 0) {
     c.bin_of[p] = bin;
@@ -546,6 +556,7 @@ __device__ __forceinline__ int2 block_incl_scan2(int a, int b, int2* warp_sums) 
   return make_int2(a, b);
 }
 
+template <int D>
 __global__ void __launch_bounds__(1024) k_offsets(Batch B) {
   SCENE_CTA(B, MAP_O);
   __shared__ int2 warp_sums[32];
@@ -571,6 +582,7 @@ __global__ void __launch_bounds__(1024) k_offsets(Batch B) {
     if (cnt > 0) {
       const int start = s_base.x + inc.x - cnt;
       c.bin_start[b] = start;
+      c.full_bins[atomicAdd(&c.ctr[CTR_FULL], 1)] = (int)b;
       const int ch0 = s_base.y + inc.y - nch;
       int l = -1, blk = 0;  // level -1 marks the extra bin
       if (b < nblk) {
@@ -590,9 +602,52 @@ __global__ void __launch_bounds__(1024) k_offsets(Batch B) {
   }
 }
 
+// Offsets of the cells inside each bin (the bin's particles are stored in
+// cell order); one warp per bin, cell counts cleared for the next substep.
+template <int D>
+__global__ void k_cell_offsets(Batch B) {
+  SCENE_CTA(B, MAP_G);
+  constexpr int NC = 1 << (2 * D), PER = (NC + 31) / 32;
+  const int lane = threadIdx.x & 31;
+  const int wid = bid_ * (blockDim.x >> 5) + (threadIdx.x >> 5), nw = nblk_ * (blockDim.x >> 5);
+  const int nfull = c.ctr[CTR_FULL];
+  for (int t = wid; t < nfull; t += nw) {
+    const int b = c.full_bins[t];
+    int* cc = c.cell_count + ((long long)b << (2 * D));
+    int n[PER], tot = 0;
+#pragma unroll
+    for (int k = 0; k < PER; ++k) {
+      const int cell = lane * PER + k;
+      n[k] = cell < NC ? cc[cell] : 0;
+      tot += n[k];
+    }
+    int inc = tot;  // inclusive scan of the lanes' totals
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, inc, o);
+      if (lane >= o) inc += y;
+    }
+    int run = inc - tot;
+    int* co = c.cell_off + ((long long)b << (2 * D));
+#pragma unroll
+    for (int k = 0; k < PER; ++k) {
+      const int cell = lane * PER + k;
+      if (cell < NC) {
+        co[cell] = run;
+        run += n[k];
+        if (n[k]) cc[cell] = 0;
+      }
+    }
+  }
+}
+
+template <int D>
 __global__ void k_scatter(Batch B) {
   SCENE_CTA(B, MAP_G);
-  SCENE_LOOP(p, c.N) c.perm[c.bin_start[c.bin_of[p]] + c.rank_of[p]] = (int)p;
+  SCENE_LOOP(p, c.N) {
+    const int key = c.bin_of[p];
+    c.perm[c.bin_start[key >> (2 * D)] + c.cell_off[key] + c.rank_of[p]] = (int)p;
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -614,8 +669,9 @@ static void run_topology(const BatchLaunch& bl, cudaStream_t s, cudaEvent_t* ev)
   k_ghost_tj<D><<<G, 256, 0, s>>>(B);
   if (ev) cudaEventRecord(ev[2], s);
   k_bin<D><<<G, 256, 0, s>>>(B);
-  k_offsets<<<Go, 1024, 0, s>>>(B);
-  k_scatter<<<G, 256, 0, s>>>(B);
+  k_offsets<D><<<Go, 1024, 0, s>>>(B);
+  k_cell_offsets<D><<<G, 256, 0, s>>>(B);
+  k_scatter<D><<<G, 256, 0, s>>>(B);
   if (ev) cudaEventRecord(ev[3], s);
 }
 
@@ -630,7 +686,7 @@ void launch_substep(const BatchLaunch& bl, cudaStream_t s, cudaEvent_t* ev) {
 }
 
 int kernels_per_substep(const BatchLaunch& bl) {
-  const int topo = 9 - (bl.any_dynamic ? 0 : 1);
+  const int topo = 10 - (bl.any_dynamic ? 0 : 1);
   return topo + 3 + (bl.any_plastic ? 1 : 0) + 2 * (bl.maxL - 1);
 }
 
