@@ -39,8 +39,9 @@ __device__ __forceinline__ void chunk_origin(const LevelDev& V, long long blk, i
 //     adaptive_gimp.py:240), its per-axis GIMP weights and gradients, m,
 //     a = m (v - C (tc+1)) and B = m C, and its base cell inside the block,
 //     and stores them in shared memory;
-//  2. the particles are counting-sorted by base cell in shared memory and cut
-//     into tasks of <= TMAX particles of one cell;
+//  2. the work item's particles are already in base-cell order (bins store
+//     their particles sorted by cell), so counting them per cell gives each
+//     cell's run of records; the runs are cut into tasks of <= TMAX particles;
 //  3. a lane owns one row of three stencil nodes (the last axis runs along
 //     the row; 3^(d-1) rows per cell) of one task, and a warp serves SLOTS
 //     tasks at once (3 in 3D, 10 in 2D).  All particles of a task share a base
@@ -67,7 +68,7 @@ struct P2GLayout {
   static constexpr int STRIDE = OFF_WL + 8;  // 3D 44, 2D 28 floats: 16-byte aligned records
   static constexpr int MAXTASK = NC + CH / TMAX;
   static constexpr size_t bytes() {
-    return sizeof(float) * ((size_t)CH * STRIDE + 4 * TN) + sizeof(int) * (2 * NC + 2 * CH + 3 * MAXTASK + 4);
+    return sizeof(float) * ((size_t)CH * STRIDE + 4 * TN) + sizeof(int) * (2 * NC + 3 * MAXTASK + 4);
   }
 };
 
@@ -80,9 +81,7 @@ __global__ void __launch_bounds__(CH, 1024 / CH) k_p2g(Batch B) {
   float* tile = pd + CH * Y::STRIDE;            // [4][TN]: p_x, p_y, p_z, m
   int* s_cnt = (int*)(tile + 4 * Y::TN);        // [NC]
   int* s_off = s_cnt + Y::NC;                   // [NC]
-  int* s_sorted = s_off + Y::NC;                // [CH]
-  int* s_pc = s_sorted + CH;                    // [CH] cell << 10 | rank of each particle
-  int* t_cell = s_pc + CH;                      // [MAXTASK]
+  int* t_cell = s_off + Y::NC;                  // [MAXTASK]
   int* t_start = t_cell + Y::MAXTASK;
   int* t_len = t_start + Y::MAXTASK;
   int* s_ntask = t_len + Y::MAXTASK;
@@ -180,19 +179,13 @@ __global__ void __launch_bounds__(CH, 1024 / CH) k_p2g(Batch B) {
         }
       }
     }
-    // rank inside the cell (warp-aggregated shared atomics)
-    int rank = 0;
+    // particles per cell (warp-aggregated shared atomics)
     {
       const unsigned grp = __match_any_sync(0xffffffffu, cell);
-      const int leader = __ffs(grp) - 1;
-      int old = 0;
-      if (cell >= 0 && lane == leader) old = atomicAdd(&s_cnt[cell], __popc(grp));
-      old = __shfl_sync(0xffffffffu, old, leader);
-      rank = old + __popc(grp & ((1u << lane) - 1u));
+      if (cell >= 0 && lane == __ffs(grp) - 1) atomicAdd(&s_cnt[cell], __popc(grp));
     }
-    if (cell >= 0) s_pc[i] = (cell << 10) | rank;
     __syncthreads();
-    // -- 2. cell offsets, tasks and the cell order (warp 0) --------------------
+    // -- 2. cell offsets and tasks (warp 0) ------------------------------------
     if (warp == 0) {
       int run_c = 0, run_t = 0;
       for (int c0 = 0; c0 < Y::NC; c0 += 32) {
@@ -221,11 +214,6 @@ __global__ void __launch_bounds__(CH, 1024 / CH) k_p2g(Batch B) {
         run_t += __shfl_sync(0xffffffffu, it, 31);
       }
       if (lane == 0) *s_ntask = run_t;
-      __syncwarp();
-      for (int k = lane; k < wd.w; k += 32) {
-        const int v = s_pc[k];
-        s_sorted[s_off[v >> 10] + (v & 1023)] = k;
-      }
     }
     __syncthreads();
     // -- 3. tasks: lane <-> row of three nodes ---------------------------------
@@ -246,7 +234,7 @@ __global__ void __launch_bounds__(CH, 1024 / CH) k_p2g(Batch B) {
         }
 #pragma unroll 2
         for (int j = 0; j < len; ++j) {
-          const float* R = pd + s_sorted[s0 + j] * Y::STRIDE;
+          const float* R = pd + (s0 + j) * Y::STRIDE;
           const float4 ma = *(const float4*)R;
           float bs[2 * D * D];
 #pragma unroll
