@@ -738,15 +738,9 @@ __device__ __forceinline__ void g2p_one(const Ctx& c, int j) {
     copy_particle<D>(c, p, j);
     return;
   }
-  float xp[D], F[D * D];
+  float xp[D];
 #pragma unroll
   for (int d = 0; d < D; ++d) xp[d] = __ldg(&c.P.x[d * N + p]);
-#pragma unroll
-  for (int k = 0; k < D * D; ++k) F[k] = __ldg(&c.P.F[k * N + p]);
-  const float mp = __ldg(&c.P.m[p]);
-  const int gp = __ldg(&c.P.g[p]);
-  const int idp = __ldg(&c.P.id[p]);
-  float jp = c.plast == 1 ? __ldg(&c.P.Jp[p]) : 1.f;
   const LevelDev& V = c.lev[l];
   const float inv = (float)(c.coarsest << l);
   const float dx = 1.f / inv;
@@ -772,46 +766,52 @@ __device__ __forceinline__ void g2p_one(const Ctx& c, int j) {
   for (int i = 0; i < D; ++i) nv[i] = 0.f;
 #pragma unroll
   for (int i = 0; i < D * D; ++i) G[i] = 0.f;
+  // 3D: one x-slab of 3 rows (9 nodes) at a time keeps fewer gathers in
+  // flight, so G2P fits in 64 registers (4 CTAs per SM)
+#pragma unroll(D == 3 ? 1 : 3)
+  for (int n0 = 0; n0 < 3; ++n0) {
+    const float w0 = n0 == 0 ? W[0][0] : (n0 == 1 ? W[0][1] : W[0][2]);
+    const float g0 = n0 == 0 ? Gw[0][0] : (n0 == 1 ? Gw[0][1] : Gw[0][2]);
 #pragma unroll
-  for (int row = 0; row < ((D == 2) ? 3 : 9); ++row) {
-    const int n0 = (D == 2) ? row : row / 3, n1 = (D == 2) ? 0 : row % 3;
-    float S[D], T[D];
+    for (int n1 = 0; n1 < ((D == 2) ? 1 : 3); ++n1) {
+      float S[D], T[D];
 #pragma unroll
-    for (int i = 0; i < D; ++i) S[i] = T[i] = 0.f;
+      for (int i = 0; i < D; ++i) S[i] = T[i] = 0.f;
 #pragma unroll
-    for (int k = 0; k < 3; ++k) {
-      int I[D];
-      I[0] = base[0] + n0;
-      if (D == 3) I[1] = base[1] + n1;
-      I[D - 1] = base[D - 1] + k;
-      // base lies in [-1, size-1] for an in-domain particle: always in store
-      const float4 nd = __ldg(&V.node[elem_of<D>(V, I)]);
-      const float gv[3] = {nd.x, nd.y, nd.z};
+      for (int k = 0; k < 3; ++k) {
+        int I[D];
+        I[0] = base[0] + n0;
+        if (D == 3) I[1] = base[1] + n1;
+        I[D - 1] = base[D - 1] + k;
+        // base lies in [-1, size-1] for an in-domain particle: always in store
+        const float4 nd = __ldg(&V.node[elem_of<D>(V, I)]);
+        const float gv[3] = {nd.x, nd.y, nd.z};
+#pragma unroll
+        for (int i = 0; i < D; ++i) {
+          S[i] += gv[i] * W[D - 1][k];
+          T[i] += gv[i] * Gw[D - 1][k];
+        }
+      }
+      // row factors: weight, and the gradient components of the other axes
+      float cw, cg[D];
+      if (D == 2) {
+        cw = w0 * kw;
+        cg[0] = g0 * kg;
+        cg[1] = w0 * kg;
+      } else {
+        const float wxy = w0 * W[1][n1];
+        cw = wxy * kw;
+        cg[0] = g0 * W[1][n1] * kg;
+        cg[1] = w0 * Gw[1][n1] * kg;
+        cg[D - 1] = wxy * kg;
+      }
 #pragma unroll
       for (int i = 0; i < D; ++i) {
-        S[i] += gv[i] * W[D - 1][k];
-        T[i] += gv[i] * Gw[D - 1][k];
+        nv[i] += cw * S[i];
+#pragma unroll
+        for (int q = 0; q < D - 1; ++q) G[i * D + q] += cg[q] * S[i];
+        G[i * D + D - 1] += cg[D - 1] * T[i];
       }
-    }
-    // row factors: weight, and the gradient components of the other axes
-    float cw, cg[D];
-    if (D == 2) {
-      cw = W[0][n0] * kw;
-      cg[0] = Gw[0][n0] * kg;
-      cg[1] = W[0][n0] * kg;
-    } else {
-      const float wxy = W[0][n0] * W[1][n1];
-      cw = wxy * kw;
-      cg[0] = Gw[0][n0] * W[1][n1] * kg;
-      cg[1] = W[0][n0] * Gw[1][n1] * kg;
-      cg[D - 1] = wxy * kg;
-    }
-#pragma unroll
-    for (int i = 0; i < D; ++i) {
-      nv[i] += cw * S[i];
-#pragma unroll
-      for (int q = 0; q < D - 1; ++q) G[i * D + q] += cg[q] * S[i];
-      G[i * D + D - 1] += cg[D - 1] * T[i];
     }
   }
 #pragma unroll
@@ -821,6 +821,15 @@ __device__ __forceinline__ void g2p_one(const Ctx& c, int j) {
   }
 #pragma unroll
   for (int i = 0; i < D * D; ++i) __stwb(&c.Q.C[i * N + j], G[i]);
+  // the rest of the particle is loaded only now (fewer live registers
+  // during the gather)
+  float F[D * D];
+#pragma unroll
+  for (int k = 0; k < D * D; ++k) F[k] = __ldg(&c.P.F[k * N + p]);
+  const float mp = __ldg(&c.P.m[p]);
+  const int gp = __ldg(&c.P.g[p]);
+  const int idp = __ldg(&c.P.id[p]);
+  float jp = c.plast == 1 ? __ldg(&c.P.Jp[p]) : 1.f;
   const float s = (c.dt * pw) / (rd * dx);
   float Fn[D * D];
 #pragma unroll
@@ -846,7 +855,7 @@ __device__ __forceinline__ void g2p_one(const Ctx& c, int j) {
 }
 
 template <int D>
-__global__ void __launch_bounds__(256, 3) k_g2p(Batch B) {
+__global__ void __launch_bounds__(256, 4) k_g2p(Batch B) {
   SCENE_CTA(B, MAP_G);
   SCENE_LOOP(j, c.N) g2p_one<D>(c, (int)j);
 }
