@@ -34,22 +34,24 @@ __device__ __forceinline__ void chunk_origin(const LevelDev& V, long long blk, i
 
 // ---------------------------------------------------------------------------
 // P2G (adaptive_gimp.py:230-250).  Per work item (up to CH particles of one
-// 4^d block of one level):
+// 4^d block of one level, in base-cell order: bins store their particles
+// sorted by cell):
 //  1. one thread per particle computes the scaled stress (utils.py:11-16,
 //     adaptive_gimp.py:240), its per-axis GIMP weights and gradients, m,
 //     a = m (v - C (tc+1)) and B = m C, and its base cell inside the block,
-//     and stores them in shared memory;
-//  2. the work item's particles are already in base-cell order (bins store
-//     their particles sorted by cell), so counting them per cell gives each
-//     cell's run of records; the runs are cut into tasks of <= TMAX particles;
+//     and stores them in shared memory at its thread index;
+//  2. each warp cuts its own 32 particles into tasks: runs of one base cell
+//     (found with ballots), at most TMAX long;
 //  3. a lane owns one row of three stencil nodes (the last axis runs along
 //     the row; 3^(d-1) rows per cell) of one task, and a warp serves SLOTS
 //     tasks at once (3 in 3D, 10 in 2D).  All particles of a task share a base
 //     cell, so the lane sums w m and w (a + B n) + S grad w of its three nodes
 //     over the task's particles in registers: one read of a particle record
-//     serves three nodes, and the row's weight products are shared;
-//  4. each lane adds its sums once into the (4+2)^d node tile in shared
-//     memory; the tile is flushed with one float4 atomic per touched node.
+//     serves three nodes, and the row's weight products are shared; the sums
+//     go once into the (4+2)^d node tile in shared memory;
+//  4. after the work item's one barrier the tile is flushed with one float4
+//     atomic per touched node and cleared.  Two tiles alternate between work
+//     items, so the next item's records and sums need no further barrier.
 template <int D, int CH>
 struct P2GLayout {
   static constexpr int NC = 1 << (2 * D);        // cells per block
@@ -66,9 +68,8 @@ struct P2GLayout {
   static constexpr int OFF_WP = OFF_BS + ((2 * D * D + 3) & ~3);
   static constexpr int OFF_WL = OFF_WP + ((6 * (D - 1) + 3) & ~3);
   static constexpr int STRIDE = OFF_WL + 8;  // 3D 44, 2D 28 floats: 16-byte aligned records
-  static constexpr int MAXTASK = NC + CH / TMAX;
   static constexpr size_t bytes() {
-    return sizeof(float) * ((size_t)CH * STRIDE + 4 * TN) + sizeof(int) * (2 * NC + 3 * MAXTASK + 4);
+    return sizeof(float) * ((size_t)CH * STRIDE + 2 * 4 * TN) + sizeof(int) * (CH / 32) * 33;
   }
 };
 
@@ -77,26 +78,20 @@ __global__ void __launch_bounds__(CH, 1024 / CH) k_p2g(Batch B) {
   SCENE_CTA(B, MAP_G);
   using Y = P2GLayout<D, CH>;
   extern __shared__ float dsm[];
-  float* pd = dsm;                              // [CH][STRIDE]
-  float* tile = pd + CH * Y::STRIDE;            // [4][TN]: p_x, p_y, p_z, m
-  int* s_cnt = (int*)(tile + 4 * Y::TN);        // [NC]
-  int* s_off = s_cnt + Y::NC;                   // [NC]
-  int* t_cell = s_off + Y::NC;                  // [MAXTASK]
-  int* t_start = t_cell + Y::MAXTASK;
-  int* t_len = t_start + Y::MAXTASK;
-  int* s_ntask = t_len + Y::MAXTASK;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  float* pd = dsm;                      // [CH][STRIDE]
+  float* tiles = pd + CH * Y::STRIDE;   // [2][4][TN]: p_x, p_y, p_z, m
+  int* starts = (int*)(tiles + 2 * 4 * Y::TN);  // [warps][33]: each warp's task starts
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int nch = c.ctr[CTR_CHUNKS];
   const float pw = (D == 2) ? 0.25f : 0.125f;                                        // 0.5**dim
   const float rd = (D == 2) ? c.radius * c.radius : c.radius * c.radius * c.radius;  // radius**dim
   const float r2 = 2.f * c.radius;
   const float kw = (D == 2) ? 1.f / (4.f * r2 * r2) : 1.f / (8.f * r2 * r2 * r2);
   const float kg = (D == 2) ? 1.f / (2.f * r2 * r2) : 1.f / (4.f * r2 * r2 * r2);
-  // the node tile and the cell counts start at zero; each work item's flush
-  // leaves them at zero again
-  for (int i = threadIdx.x; i < 4 * Y::TN; i += blockDim.x) tile[i] = 0.f;
-  for (int i = threadIdx.x; i < Y::NC; i += blockDim.x) s_cnt[i] = 0;
+  // the tiles start at zero; each flush leaves its tile at zero again
+  for (int i = threadIdx.x; i < 2 * 4 * Y::TN; i += blockDim.x) tiles[i] = 0.f;
   __syncthreads();
+  int tb = 0;
   for (int ch = bid_; ch < nch; ch += nblk_) {
     const int4 wd = c.chunks[ch];
     const int l = wd.x;
@@ -104,10 +99,11 @@ __global__ void __launch_bounds__(CH, 1024 / CH) k_p2g(Batch B) {
     const LevelDev& V = c.lev[l];
     int O[D];
     chunk_origin<D>(V, wd.y, O);
+    float* tile = tiles + tb * 4 * Y::TN;
     // -- 1. per-particle quantities ------------------------------------------
     const int i = threadIdx.x;
     int cell = -1;
-    if (l >= 0 && i < wd.w) {
+    if (i < wd.w) {
       const int p = __ldg(&c.perm[wd.z + i]);
       const long long N = c.N;
       const float inv = (float)(c.coarsest << l);
@@ -179,52 +175,33 @@ __global__ void __launch_bounds__(CH, 1024 / CH) k_p2g(Batch B) {
         }
       }
     }
-    // particles per cell (warp-aggregated shared atomics)
-    {
-      const unsigned grp = __match_any_sync(0xffffffffu, cell);
-      if (cell >= 0 && lane == __ffs(grp) - 1) atomicAdd(&s_cnt[cell], __popc(grp));
-    }
-    __syncthreads();
-    // -- 2. cell offsets and tasks (warp 0) ------------------------------------
-    if (warp == 0) {
-      int run_c = 0, run_t = 0;
-      for (int c0 = 0; c0 < Y::NC; c0 += 32) {
-        const int cc = c0 + lane;
-        const int n = cc < Y::NC ? s_cnt[cc] : 0;
-        const int nt = (n + Y::TMAX - 1) / Y::TMAX;
-        int ic = n, it = nt;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-          const int yc = __shfl_up_sync(0xffffffffu, ic, o), yt = __shfl_up_sync(0xffffffffu, it, o);
-          if (lane >= o) {
-            ic += yc;
-            it += yt;
-          }
-        }
-        if (cc < Y::NC) {
-          const int off = run_c + ic - n;
-          s_off[cc] = off;
-          for (int j = 0, t = run_t + it - nt; j < n; j += Y::TMAX, ++t) {
-            t_cell[t] = cc;
-            t_start[t] = off + j;
-            t_len[t] = min(Y::TMAX, n - j);
-          }
-        }
-        run_c += __shfl_sync(0xffffffffu, ic, 31);
-        run_t += __shfl_sync(0xffffffffu, it, 31);
-      }
-      if (lane == 0) *s_ntask = run_t;
-    }
-    __syncthreads();
+    __syncwarp();
+    // -- 2. this warp's tasks: runs of one base cell, at most TMAX long ---------
+    const int wbase = warp * 32;
+    const int nvalid = max(0, min(32, wd.w - wbase));
+    const bool valid = lane < nvalid;
+    const int prev = __shfl_up_sync(0xffffffffu, cell, 1);
+    const unsigned runs = __ballot_sync(0xffffffffu, valid && (lane == 0 || cell != prev));
+    const int rs = valid ? 31 - __clz(runs & ((2u << lane) - 1u)) : 0;  // start of this lane's run
+    const bool tstart = valid && (lane - rs) % Y::TMAX == 0;
+    const unsigned tmask = __ballot_sync(0xffffffffu, tstart);
+    const int ntask = __popc(tmask);
+    int* ws = starts + warp * 33;  // task k starts at ws[k]; ws[ntask] = nvalid
+    if (tstart) ws[__popc(tmask & ((1u << lane) - 1u))] = lane;
+    if (lane == 0) ws[ntask] = nvalid;
+    __syncwarp();
     // -- 3. tasks: lane <-> row of three nodes ---------------------------------
     {
-      const int ntask = *s_ntask;
       const int q = lane / Y::ROWS, row = lane % Y::ROWS;
       const int n0 = (D == 2) ? row : row / 3, n1 = (D == 2) ? 0 : row % 3;
-      for (int t0 = warp * Y::SLOTS; t0 < ntask; t0 += nwarps * Y::SLOTS) {
+      for (int t0 = 0; t0 < ntask; t0 += Y::SLOTS) {
         const int t = t0 + q;
-        if (q >= Y::SLOTS || t >= ntask) continue;
-        const int cc = t_cell[t], s0 = t_start[t], len = t_len[t];
+        const bool on = q < Y::SLOTS && t < ntask;
+        const int s0 = on ? ws[t] : 0;
+        const int e = on ? ws[t + 1] : 0;
+        const int cc = __shfl_sync(0xffffffffu, cell, s0);
+        if (!on) continue;
+        const int len = e - s0;
         float am[3], ap[3][D];
 #pragma unroll
         for (int k = 0; k < 3; ++k) {
@@ -234,7 +211,7 @@ __global__ void __launch_bounds__(CH, 1024 / CH) k_p2g(Batch B) {
         }
 #pragma unroll 2
         for (int j = 0; j < len; ++j) {
-          const float* R = pd + (s0 + j) * Y::STRIDE;
+          const float* R = pd + (wbase + s0 + j) * Y::STRIDE;
           const float4 ma = *(const float4*)R;
           float bs[2 * D * D];
 #pragma unroll
@@ -305,7 +282,7 @@ __global__ void __launch_bounds__(CH, 1024 / CH) k_p2g(Batch B) {
       }
     }
     __syncthreads();
-    // -- 4. flush ------------------------------------------------------------
+    // -- 4. flush and clear ---------------------------------------------------
     for (int t = threadIdx.x; t < Y::TN; t += blockDim.x) {
       const float4 val = make_float4(tile[t], tile[Y::TN + t], D == 3 ? tile[2 * Y::TN + t] : 0.f, tile[3 * Y::TN + t]);
       if (val.x == 0.f && val.y == 0.f && val.z == 0.f && val.w == 0.f) continue;
@@ -324,8 +301,7 @@ __global__ void __launch_bounds__(CH, 1024 / CH) k_p2g(Batch B) {
       }
       atomicAdd(&V.node[elem_of<D>(V, I)], val);
     }
-    for (int i = threadIdx.x; i < Y::NC; i += blockDim.x) s_cnt[i] = 0;
-    __syncthreads();
+    tb ^= 1;
   }
 }
 
