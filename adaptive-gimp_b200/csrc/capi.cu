@@ -380,6 +380,7 @@ agimp_status agimp_destroy(agimp_sim* s) {
     if (e) cudaEventDestroy(e);
   if (s->rwin) cudaFree(s->rwin);
   if (s->map_dev) cudaFree(s->map_dev);
+  if (s->c.touch_occ) cudaFree(s->c.touch_occ);
   if (s->internal) cudaStreamDestroy(s->internal);
   if (s->ev_in) cudaEventDestroy(s->ev_in);
   if (s->ev_out) cudaEventDestroy(s->ev_out);
@@ -556,6 +557,12 @@ agimp_status agimp_set_level_map(agimp_sim* s, const int8_t* table, int32_t halo
   s->map_dev = nullptr;
   CK(cudaMalloc(&s->map_dev, bytes));
   CK(cudaMemcpy(s->map_dev, host.data(), bytes, cudaMemcpyHostToDevice));
+  if (!s->c.touch_occ) {
+    // base-cell records of the touched blocks (static mode only)
+    const size_t words = (size_t)s->c.lev[s->c.L - 1].nblocks * (s->c.dim == 2 ? 1 : 5);
+    CK(cudaMalloc(&s->c.touch_occ, words * sizeof(uint32_t)));
+    CK(cudaMemset(s->c.touch_occ, 0, words * sizeof(uint32_t)));
+  }
   s->c.map = s->map_dev;
   s->c.map_h = halo;
   s->c.map_n = n;

@@ -88,6 +88,7 @@ struct Ctx {
   int32_t* ctr;
   uint32_t* touch_flag;
   int32_t* touch_list;
+  uint32_t* touch_occ;  // static mode, [finest blocks][1 (2D) or 5 (3D)]: base cells of the block's particles
   int32_t* bin_count;   // [bins]: particles per bin
   int32_t* cell_count;  // [bins][4^d]: particles per (bin, base cell inside the bin's block)
   int32_t* cell_off;    // [bins][4^d]: their offsets inside the bin (particles of a bin are cell-sorted)

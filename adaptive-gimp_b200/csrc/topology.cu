@@ -120,28 +120,50 @@ __device__ __forceinline__ void touch_one(const Ctx& c, int p) {
   }
   if (valid && esc) set_err(c, ERR_ESCAPED);
   if (esc) return;
+  // the finest cell holding the particle and its block (the touched block)
+  const LevelDev& Vf = c.lev[c.L - 1];
+  int pc[D];
+  unsigned b = 0;
+#pragma unroll
+  for (int d = 0; d < D; ++d) {
+    pc[d] = (int)(xp[d] * (float)c.sz);
+    b = b * (unsigned)Vf.nb + (unsigned)((pc[d] >> 2) + 1);
+  }
+  const int key = (int)b;
   // reach of this particle's activations, recorded with its finest block: 1
   // in dynamic mode, L - (level of its level-map cell) in static mode
   unsigned reach = 1;
   if (!c.is_static) {
     const int gl = c.P.g[p];
-    if (gl >= 0 && gl < c.L) {
+    const bool ok = gl >= 0 && gl < c.L;
+    int base[D];
+    long long bk = ok ? gl : -1;
+    if (ok) {
       const float inv = (float)(c.coarsest << gl);
-      int base[D];
 #pragma unroll
-      for (int d = 0; d < D; ++d) base[d] = (int)(xp[d] * inv + 0.5f) - 1;
-#pragma unroll
-      for (int a = 0; a < (1 << D); ++a) {
+      for (int d = 0; d < D; ++d) {
+        base[d] = (int)(xp[d] * inv + 0.5f) - 1;
+        bk = bk * (c.sz + 4) + (base[d] + 2);
+      }
+    }
+    // particles with the same (level, base cell) activate the same 2^d
+    // cells: the lanes of such a group share the activations
+    const int lane = threadIdx.x & 31;
+    const unsigned g = __match_any_sync(__activemask(), bk);
+    const int r = __popc(g & ((1u << lane) - 1u)), n = __popc(g);
+    if (ok)
+      for (int a = r; a < (1 << D); a += n) {
         int I[D];
 #pragma unroll
         for (int d = 0; d < D; ++d) I[d] = base[d] + ((a >> (D - 1 - d)) & 1);
         cell_or<D>(c, gl, I, ACT);
       }
-    }
   } else {
     // The lookups depend on the finest base cell fb, then on (level, base):
     // lanes of a warp that share them would repeat identical lookups and
     // activations, so the first lane of each group does them for the group.
+    // The 4^d cells around fb (adaptive_gimp.py:77-78) are looked up by
+    // k_dilate, once per cell, from the base cells recorded here.
     const unsigned act = __activemask();
     const int lane = threadIdx.x & 31;
     int fb[D];
@@ -153,15 +175,20 @@ __device__ __forceinline__ void touch_one(const Ctx& c, int p) {
     }
     const unsigned g1 = __match_any_sync(act, fk);
     const int lead1 = __ffs(g1) - 1;
-    const int r1 = __popc(g1 & ((1u << lane) - 1u)), n1 = __popc(g1);
     int level = 0;
     if (lane == lead1) level = grid_init<D>(c, fb);
-#pragma unroll 1
-    for (int a = r1; a < (1 << (2 * D)); a += n1) {
-      int I[D];
+    {
+      // fb lies in [T0 - 1, T0 + 3] on every axis (T0: the touched block's
+      // first cell); bit (j_1, .., j_{d-1}) of word j_0 with j = fb - T0 + 1
+      int j[D];
 #pragma unroll
-      for (int d = 0; d < D; ++d) I[d] = fb[d] + ((a >> (2 * (D - 1 - d))) & 3) - 1;
-      grid_init<D>(c, I);
+      for (int d = 0; d < D; ++d) j[d] = fb[d] - (pc[d] & ~3) + 1;
+      const unsigned wi = (D == 2) ? (unsigned)key : (unsigned)key * 5u + (unsigned)j[0];
+      const unsigned bit = (D == 2) ? 1u << (5 * j[0] + j[1]) : 1u << (5 * j[1] + j[D - 1]);
+      const unsigned g3 = __match_any_sync(act, wi);
+      const unsigned bits = __reduce_or_sync(g3, bit);
+      uint32_t* w = &c.touch_occ[wi];
+      if (lane == __ffs(g3) - 1 && (*w & bits) != bits) atomicOr(w, bits);
     }
     level = __shfl_sync(g1, level, lead1);
     reach = (unsigned)(c.L - level);
@@ -184,11 +211,6 @@ __device__ __forceinline__ void touch_one(const Ctx& c, int p) {
     }
   }
   // record the finest block for the active-block lists (first toucher appends)
-  const LevelDev& Vf = c.lev[c.L - 1];
-  unsigned b = 0;
-#pragma unroll
-  for (int d = 0; d < D; ++d) b = b * (unsigned)Vf.nb + (unsigned)((((int)(xp[d] * (float)c.sz)) >> 2) + 1);
-  const int key = (int)b;
   const unsigned grp = __match_any_sync(__activemask(), key);
   const unsigned rmax = __reduce_max_sync(grp, reach);
   if ((int)(threadIdx.x & 31) == __ffs(grp) - 1 && c.touch_flag[key] < rmax &&
@@ -221,6 +243,56 @@ __device__ __forceinline__ int dilate_radius(const Ctx& c, int l, unsigned reach
   const int rho = max(2, 1 << (int)reach);  // reach = L - lv
   const int div = 1 << (c.L - 1 - l);
   return ((rho + div - 1) / div + 9) / 4;
+}
+
+// Static mode: grid_initializer on the 4^d cells f_base + [-1, 2]^d of every
+// particle (adaptive_gimp.py:77-78), once per distinct cell.  k_touch_activate
+// recorded the particles' base cells per touched block (fb - T0 + 1 in
+// [0, 4]^d); a cell X = T0 + r (r in [-2, 5]^d) is looked up when a recorded
+// base cell lies in [X - 2, X + 1] on every axis.
+// Blocks next to each other may both look up a cell of their common border;
+// the second lookup finds the cell already set.
+__device__ __forceinline__ unsigned axis_window(int r) {
+  const int lo = max(0, r - 1), hi = min(4, r + 2);
+  return lo > hi ? 0u : ((2u << hi) - (1u << lo));
+}
+
+// bits j of a 5-bit axis mask m, spread to bit 5 j (one 5-bit row per j)
+__device__ __forceinline__ unsigned spread_rows(unsigned m) {
+  unsigned o = 0;
+#pragma unroll
+  for (int j = 0; j < 5; ++j)
+    if (m >> j & 1u) o |= 1u << (5 * j);
+  return o;
+}
+
+template <int D>
+__device__ __forceinline__ void static_window(const Ctx& c, int key, const int* fb, int lane) {
+  constexpr int W = (D == 2) ? 1 : 5;
+  uint32_t occ[W];
+#pragma unroll
+  for (int w = 0; w < W; ++w) occ[w] = c.touch_occ[(long long)key * W + w];
+  for (int r = lane; r < (1 << (3 * D)); r += 32) {
+    int X[D];
+    unsigned m[D];
+#pragma unroll
+    for (int d = 0; d < D; ++d) {
+      const int rel = ((r >> (3 * (D - 1 - d))) & 7) - 2;
+      X[d] = fb[d] * 4 + rel;
+      m[d] = axis_window(rel);
+    }
+    // recorded base cells inside the window of X
+    const unsigned plane = m[D - 1] * spread_rows(m[D - 2]);
+    bool hit;
+    if (D == 2) {
+      hit = (occ[0] & plane) != 0u;
+    } else {
+      hit = false;
+#pragma unroll
+      for (int j = 0; j < 5; ++j) hit = hit || ((m[0] >> j & 1u) && (occ[j] & plane));
+    }
+    if (hit) grid_init<D>(c, X);
+  }
 }
 
 template <int D>
@@ -270,6 +342,7 @@ __global__ void k_dilate(Batch B) {
         }
       }
     }
+    if (c.is_static) static_window<D>(c, key, fb, lane);
   }
 }
 
@@ -321,7 +394,12 @@ __global__ void k_resolve(Batch B) {
   SCENE_CTA(B, MAP_G);
   // k_dilate has read the touched blocks' reach: clear the flags for the next
   // substep (they are read again only by k_touch_activate)
-  SCENE_LOOP(t, c.ctr[CTR_TOUCH]) c.touch_flag[c.touch_list[t]] = 0u;
+  SCENE_LOOP(t, c.ctr[CTR_TOUCH]) {
+    const int key = c.touch_list[t];
+    c.touch_flag[key] = 0u;
+    if (c.is_static)
+      for (int w = 0; w < ((D == 2) ? 1 : 5); ++w) c.touch_occ[(long long)key * ((D == 2) ? 1 : 5) + w] = 0u;
+  }
   const long long tot = total_elems(c, 0, c.L, D);
   SCENE_LOOP(e, tot) {
     int l, loc;

@@ -87,7 +87,6 @@ __global__ void __launch_bounds__(CH, 1024 / CH) k_p2g(Batch B) {
   const float rd = (D == 2) ? c.radius * c.radius : c.radius * c.radius * c.radius;  // radius**dim
   const float r2 = 2.f * c.radius;
   const float kw = (D == 2) ? 1.f / (4.f * r2 * r2) : 1.f / (8.f * r2 * r2 * r2);
-  const float kg = (D == 2) ? 1.f / (2.f * r2 * r2) : 1.f / (4.f * r2 * r2 * r2);
   // the tiles start at zero; each flush leaves its tile at zero again
   for (int i = threadIdx.x; i < 2 * 4 * Y::TN; i += blockDim.x) tiles[i] = 0.f;
   __syncthreads();
@@ -162,10 +161,19 @@ __global__ void __launch_bounds__(CH, 1024 / CH) k_p2g(Batch B) {
           P[Y::OFF_BS + r * D + b] = mp * Cm[r * D + b];
           P[Y::OFF_BS + D * D + r * D + b] = sc * (acc + (r == b ? diag : 0.f));
         }
+      // axis factors, scaled so that a node's weight is the product of its
+      // W's and the gradient's factors need no constant: axis 0 carries kw,
+      // every G carries kg / kw = 2
 #pragma unroll
       for (int d = 0; d < D; ++d) {
         float W[3], G[3];
         axis_weights(tc[d], c.radius, W, G);
+        const float sw = d == 0 ? kw : 1.f;
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+          W[k] *= sw;
+          G[k] *= 2.f * sw;
+        }
         if (d < D - 1) {
 #pragma unroll
           for (int k = 0; k < 3; ++k) *(float2*)(P + Y::OFF_WP + 6 * d + 2 * k) = make_float2(W[k], G[k]);
@@ -227,46 +235,42 @@ __global__ void __launch_bounds__(CH, 1024 / CH) k_p2g(Batch B) {
           const float4 wl = *(const float4*)(R + Y::OFF_WL);
           const float4 gl = *(const float4*)(R + Y::OFF_WL + 4);
           const float wL[3] = {wl.x, wl.y, wl.z}, gL[3] = {gl.x, gl.y, gl.z};
-          // weight and gradient factors of the row (all axes but the last)
-          float cw, cg[D];
+          // Node k of the row has weight cw wL[k] and gradient
+          // (cg_0 wL[k], .., cg_{d-2} wL[k], cw gL[k]); its momentum term is
+          //   w (a + B n) + S grad w = wL[k] (A + k Bk) + gL[k] s_L
+          // with A = cw (a + B n_row) + sum_{b<d-1} S[:, b] cg_b, Bk = cw B[:, d-1]
+          // and s_L = cw S[:, d-1].
+          float cw, cg[D - 1];
           const float av[3] = {ma.y, ma.z, ma.w};
-          float u[D];
+          float A[D];
           if (D == 2) {
             const float2 wg0 = *(const float2*)(R + Y::OFF_WP + 2 * n0);
-            cw = wg0.x * kw;
-            cg[0] = wg0.y * kg;
-            cg[1] = wg0.x * kg;
+            cw = wg0.x;
+            cg[0] = wg0.y;
 #pragma unroll
-            for (int r = 0; r < D; ++r) u[r] = av[r] + Bm[r * D] * (float)n0;
+            for (int r = 0; r < D; ++r) A[r] = fmaf(cw, fmaf(Bm[r * D], (float)n0, av[r]), Sm[r * D] * cg[0]);
           } else {
             const float2 wg0 = *(const float2*)(R + Y::OFF_WP + 2 * n0);
             const float2 wg1 = *(const float2*)(R + Y::OFF_WP + 6 + 2 * n1);
-            const float wxy = wg0.x * wg1.x;
-            cw = wxy * kw;
-            cg[0] = wg0.y * wg1.x * kg;
-            cg[1] = wg0.x * wg1.y * kg;
-            cg[D - 1] = wxy * kg;
-#pragma unroll
-            for (int r = 0; r < D; ++r) u[r] = av[r] + Bm[r * D] * (float)n0 + Bm[r * D + 1] * (float)n1;
-          }
-#pragma unroll
-          for (int k = 0; k < 3; ++k) {
-            // node n_{d-1} = k of the row
-            const float w = cw * wL[k];
-            float gw[D];
-#pragma unroll
-            for (int b = 0; b < D - 1; ++b) gw[b] = cg[b] * wL[k];
-            gw[D - 1] = cg[D - 1] * gL[k];
-            am[k] += w * ma.x;
+            cw = wg0.x * wg1.x;
+            cg[0] = wg0.y * wg1.x;
+            cg[D - 2] = wg0.x * wg1.y;
 #pragma unroll
             for (int r = 0; r < D; ++r) {
-              const float ur = u[r] + Bm[r * D + D - 1] * (float)k;
-              float sv = 0.f;
-#pragma unroll
-              for (int b = 0; b < D; ++b) sv += Sm[r * D + b] * gw[b];
-              ap[k][r] += w * ur + sv;
+              const float u = fmaf(Bm[r * D + 1], (float)n1, fmaf(Bm[r * D], (float)n0, av[r]));
+              A[r] = fmaf(cw, u, fmaf(Sm[r * D], cg[0], Sm[r * D + 1] * cg[D - 2]));
             }
           }
+          const float cm = cw * ma.x;
+#pragma unroll
+          for (int r = 0; r < D; ++r) {
+            const float bk = cw * Bm[r * D + D - 1], sl = cw * Sm[r * D + D - 1];
+            ap[0][r] = fmaf(gL[0], sl, fmaf(wL[0], A[r], ap[0][r]));
+            ap[1][r] = fmaf(gL[1], sl, fmaf(wL[1], A[r] + bk, ap[1][r]));
+            ap[2][r] = fmaf(gL[2], sl, fmaf(wL[2], fmaf(2.f, bk, A[r]), ap[2][r]));
+          }
+#pragma unroll
+          for (int k = 0; k < 3; ++k) am[k] = fmaf(wL[k], cm, am[k]);
         }
         int ti = 0;
 #pragma unroll
