@@ -46,6 +46,9 @@ agimp_status batch_init(agimp_batch* b) {
   }
   BCK(cudaMalloc(&b->dofs, sizeof(int) * NMAP * (n + 1)));
   b->hofs.assign(NMAP * (n + 1), 0);
+  BCK(cudaStreamCreateWithFlags(&b->side, cudaStreamNonBlocking));
+  BCK(cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming));
+  BCK(cudaEventCreateWithFlags(&b->ev_join, cudaEventDisableTiming));
   if (!b->single) {
     BCK(cudaStreamCreateWithFlags(&b->internal, cudaStreamNonBlocking));
     BCK(cudaEventCreateWithFlags(&b->ev_in, cudaEventDisableTiming));
@@ -70,6 +73,9 @@ void batch_free(agimp_batch* b) {
     if (b->dctx[k]) cudaFree(b->dctx[k]);
   if (b->dofs) cudaFree(b->dofs);
   if (b->internal) cudaStreamDestroy(b->internal);
+  if (b->side) cudaStreamDestroy(b->side);
+  if (b->ev_fork) cudaEventDestroy(b->ev_fork);
+  if (b->ev_join) cudaEventDestroy(b->ev_join);
   if (b->ev_in) cudaEventDestroy(b->ev_in);
   if (b->ev_out) cudaEventDestroy(b->ev_out);
   if (b->ev_done) cudaEventDestroy(b->ev_done);
@@ -148,6 +154,9 @@ static BatchLaunch make_launch(agimp_batch* b, int ph) {
   for (int k = 0; k < NMAP; ++k) bl.nct[k] = b->nct[k];
   bl.chunk = b->tune.chunk;
   bl.single = b->single ? &b->hctx[ph][0] : nullptr;
+  bl.side = b->side;
+  bl.fork = b->ev_fork;
+  bl.join = b->ev_join;
   return bl;
 }
 
@@ -186,7 +195,8 @@ agimp_status batch_step(agimp_batch* b, float dt, int n, cudaStream_t use, cudaE
     const int ph = b->single ? b->sims[0]->par : (int)(b->steps & 1);
     agimp_status st = sync_contexts(b, ph, dt, use);
     if (st != AGIMP_OK) return st;
-    const BatchLaunch bl = make_launch(b, ph);
+    BatchLaunch bl = make_launch(b, ph);
+    if (ev) bl.side = nullptr;  // phase timing: one stream
     if (ev || !b->graphs) {
       launch_substep(bl, use, ev);
       BCK(cudaGetLastError());

@@ -588,6 +588,12 @@ struct BatchLaunch {
   int any_dynamic;   // some scene activates cells from g_p (runs k_mark_hier)
   int any_plastic;   // some scene has snow plasticity (runs k_project)
   const Ctx* single; // host context of a single simulator (surrogate step), else null
+  // second stream of the substep (null: everything on the caller's stream):
+  // k_ghost_tj runs on it beside the binning kernels and P2G, which read no
+  // node mask and only the exact-ACTIVATED cell tests that k_ghost_tj leaves
+  // unchanged; the restriction waits for it
+  cudaStream_t side;
+  cudaEvent_t fork, join;
 };
 
 // The calling CTA's scene: its context (copied to *sc), its rank among the

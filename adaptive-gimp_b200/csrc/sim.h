@@ -66,6 +66,8 @@ struct agimp_batch {
   Key gkey[2];
   long long steps = 0;
   cudaStream_t internal = nullptr;  // used when the caller passes no stream (own batches only)
+  cudaStream_t side = nullptr;      // second stream inside a substep
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   cudaEvent_t ev_in = nullptr, ev_out = nullptr;
   std::string err;
   // batch readback of positions (own batches only): the last step's work is

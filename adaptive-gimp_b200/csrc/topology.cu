@@ -81,21 +81,28 @@ __global__ void k_clear(Batch B) {
 // Per particle: record the finest block holding it (for the active-block
 // lists) and activate cells, dynamically from g_p (adaptive_gimp.py:87-96) or
 // through the level map (adaptive_gimp.py:72-85).
+// the tabulated level map at finest cell I: bits 0-3 the level, bit 6 "no
+// activation"; outside the table: an error and level L-1 without activation
 template <int D>
-__device__ __forceinline__ int grid_init(const Ctx& c, const int* I) {
-  // grid_initializer(sim, I) with the tabulated map: activate_cell(l, I)
-  // (adaptive_gimp.py:68-70) unless bit 6 is set; returns l.
+__device__ __forceinline__ int map_entry(const Ctx& c, const int* I) {
   long long o = 0;
 #pragma unroll
   for (int d = 0; d < D; ++d) {
     int a = I[d] + c.map_h;
     if (a < 0 || a >= c.map_n) {
       set_err(c, ERR_MAP_OOB);
-      return c.L - 1;
+      return (c.L - 1) | 64;
     }
     o = o * c.map_n + a;
   }
-  const int e = c.map[o];
+  return c.map[o];
+}
+
+template <int D>
+__device__ __forceinline__ int grid_init(const Ctx& c, const int* I) {
+  // grid_initializer(sim, I) with the tabulated map: activate_cell(l, I)
+  // (adaptive_gimp.py:68-70) unless bit 6 is set; returns l.
+  const int e = map_entry<D>(c, I);
   const int l = e & 15;
   if (!(e & 64)) {
     int A[D];
@@ -176,7 +183,8 @@ __device__ __forceinline__ void touch_one(const Ctx& c, int p) {
     const unsigned g1 = __match_any_sync(act, fk);
     const int lead1 = __ffs(g1) - 1;
     int level = 0;
-    if (lane == lead1) level = grid_init<D>(c, fb);
+    // fb's own activation is one of its window's (k_dilate): only the level here
+    if (lane == lead1) level = map_entry<D>(c, fb) & 15;
     {
       // fb lies in [T0 - 1, T0 + 3] on every axis (T0: the touched block's
       // first cell); bit (j_1, .., j_{d-1}) of word j_0 with j = fb - T0 + 1
@@ -202,8 +210,9 @@ __device__ __forceinline__ void touch_one(const Ctx& c, int p) {
     }
     const unsigned g2 = __match_any_sync(act, bk);
     const int r2 = __popc(g2 & ((1u << lane) - 1u)), n2 = __popc(g2);
+    // at the finest level base = fb: its 2^d corners are cells of fb's window
 #pragma unroll 1
-    for (int a = r2; a < (1 << D); a += n2) {
+    for (int a = level < c.L - 1 ? r2 : (1 << D); a < (1 << D); a += n2) {
       int I[D];
 #pragma unroll
       for (int d = 0; d < D; ++d) I[d] = (base[d] + ((a >> (D - 1 - d)) & 1)) * (1 << (c.L - 1 - level));
@@ -744,7 +753,14 @@ static void run_topology(const BatchLaunch& bl, cudaStream_t s, cudaEvent_t* ev)
   if (ev) cudaEventRecord(ev[1], s);
   if (bl.any_dynamic) k_mark_hier<D><<<G, 256, 0, s>>>(B);
   k_resolve<D><<<G, 256, 0, s>>>(B);
-  k_ghost_tj<D><<<G, 256, 0, s>>>(B);
+  if (bl.side) {
+    cudaEventRecord(bl.fork, s);
+    cudaStreamWaitEvent(bl.side, bl.fork, 0);
+    k_ghost_tj<D><<<G, 256, 0, bl.side>>>(B);
+    cudaEventRecord(bl.join, bl.side);
+  } else {
+    k_ghost_tj<D><<<G, 256, 0, s>>>(B);
+  }
   if (ev) cudaEventRecord(ev[2], s);
   k_bin<D><<<G, 256, 0, s>>>(B);
   k_offsets<D><<<Go, 1024, 0, s>>>(B);

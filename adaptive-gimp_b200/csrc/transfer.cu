@@ -893,6 +893,7 @@ template <int D>
 void launch_transfer(const BatchLaunch& bl, cudaStream_t s, cudaEvent_t* ev) {
   const int G = bl.nct[MAP_G];
   launch_p2g<D>(bl, s);
+  if (bl.side) cudaStreamWaitEvent(s, bl.join, 0);  // k_ghost_tj's node mask
   if (ev) cudaEventRecord(ev[4], s);
   for (int l = bl.maxL - 1; l >= 1; --l) k_restrict<D><<<G, 256, 0, s>>>(bl.b, l);
   if (ev) cudaEventRecord(ev[5], s);
