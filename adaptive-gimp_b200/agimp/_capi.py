@@ -34,6 +34,8 @@ EXPORTS = (
     "agimp_batch_set_graphs", "agimp_batch_set_tuning", "agimp_batch_get_tuning", "agimp_batch_autotune",
     "agimp_batch_kernels_per_substep", "agimp_batch_profile_substep",
     "agimp_render_mask", "agimp_render_particles", "agimp_get_particles_async", "agimp_batch_positions_async",
+    "agimp_get_level_map", "agimp_lattice_count", "agimp_lattice_fill", "agimp_random_fill",
+    "agimp_set_level_map_rule", "agimp_set_coarse_level_map",
 )
 PHASES = ("blocks", "topology", "binning", "p2g", "restrict", "gridop", "prolong", "g2p")
 
@@ -59,6 +61,23 @@ class Tuning(ctypes.Structure):
 
     def as_dict(self):
         return dict(chunk=self.chunk, ctas_per_sm=self.ctas_per_sm, ms_per_substep=self.ms_per_substep)
+
+
+SHAPE_BOX = 0
+SHAPE_SPHERE = 1
+
+
+class Shape(ctypes.Structure):
+    _fields_ = [("kind", ctypes.c_int32), ("level", ctypes.c_int32), ("lo", ctypes.c_double * 3),
+                ("hi", ctypes.c_double * 3), ("centre", ctypes.c_double * 3), ("radius", ctypes.c_double),
+                ("velocity", ctypes.c_float * 3), ("mass", ctypes.c_float)]
+
+
+class RandomBox(ctypes.Structure):
+    _fields_ = [("count", ctypes.c_int64), ("lo", ctypes.c_float * 3), ("size", ctypes.c_float * 3),
+                ("velocity", ctypes.c_float * 3), ("mass", ctypes.c_float), ("n_bands", ctypes.c_int32),
+                ("band_lo", ctypes.c_float * 4), ("band_hi", ctypes.c_float * 4), ("band_level", ctypes.c_int32 * 4),
+                ("level", ctypes.c_int32)]
 
 
 class AgimpError(RuntimeError):
@@ -137,6 +156,15 @@ def load(path: str | None = None):
     L.agimp_batch_positions_async.argtypes = [vp, vp, vp]
     L.agimp_render_mask.argtypes = [vp, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, vp, ctypes.c_int32, vp]
     L.agimp_render_particles.argtypes = [vp, ctypes.c_int32, ctypes.c_float, vp, ctypes.c_int32, vp, ctypes.c_int32, vp]
+    L.agimp_get_level_map.argtypes = [vp, vp, ip, ctypes.c_int32, vp]
+    L.agimp_lattice_count.argtypes = [ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_uint64,
+                                      ctypes.POINTER(Shape), ctypes.c_int32, ctypes.POINTER(ctypes.c_int64),
+                                      ctypes.c_int32]
+    L.agimp_lattice_fill.argtypes = [vp, ctypes.c_int32, ctypes.c_int32, ctypes.c_uint64, ctypes.POINTER(Shape),
+                                     ctypes.c_int32, vp]
+    L.agimp_random_fill.argtypes = [vp, ctypes.c_uint64, ctypes.POINTER(RandomBox), ctypes.c_int32, vp]
+    L.agimp_set_level_map_rule.argtypes = [vp, ctypes.c_int32, vp]
+    L.agimp_set_coarse_level_map.argtypes = [vp, vp, ctypes.c_int32, vp]
     _lib = L
     return L
 

@@ -14,7 +14,7 @@ ROOT = os.path.dirname(PKG)
 CSRC = os.path.join(ROOT, "csrc")
 INCLUDE = os.path.join(os.path.dirname(ROOT), "include")
 LIB = os.path.join(PKG, "libagimp.so")
-SOURCES = ["capi.cu", "batch.cu", "topology.cu", "transfer.cu", "refine.cu", "noalloc.cu", "mlp.cu", "render.cu"]
+SOURCES = ["capi.cu", "batch.cu", "topology.cu", "transfer.cu", "refine.cu", "noalloc.cu", "mlp.cu", "render.cu", "init.cu"]
 HEADERS = ["common.cuh", "umma.cuh", "sim.h"]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

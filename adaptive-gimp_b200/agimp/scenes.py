@@ -72,6 +72,8 @@ def initialize_mask5(sim, I):
 
 REFERENCE_MASKS = {1: initialize_mask1, 2: initialize_mask2, 3: initialize_mask3, 4: initialize_mask4,
                    5: initialize_mask5}
+for _k, _f in REFERENCE_MASKS.items():
+    _f.device_rule = _k  # the library tabulates these on the device (agimp_set_level_map_rule)
 
 
 def band_level_map(boxes, dim, level, coarsest_size, near=2, mid=4, floor_y=0.25):
@@ -101,6 +103,7 @@ def band_level_map(boxes, dim, level, coarsest_size, near=2, mid=4, floor_y=0.25
         lv = coarse_lv[tuple(np.moveaxis(C, -1, 0))]
         return np.where(inr, lv, level - 1), inr
 
+    grid_initializer.coarse_levels = coarse_lv.astype(np.int8)  # expanded on the device
     return grid_initializer
 
 
@@ -280,7 +283,7 @@ def _place_boxes(rng, sides, tries=200):
     return placed
 
 
-def make_batch_config(seed=0, n_scenes=256, scale=1.0):
+def make_batch_config(seed=0, n_scenes=256, scale=1.0, device=False):
     """Config 4: independent 2D scenes for one batch.  Each scene draws its
     level count from {2, 3, 4}, its finest resolution from {256, 512}, 1-3
     boxes and a particle count from a lognormal clipped to [2k, 60k] (times
@@ -304,6 +307,14 @@ def make_batch_config(seed=0, n_scenes=256, scale=1.0):
             w = float(np.sqrt(a * r))
             sides.append((min(w, 0.7), min(a / w, 0.7)))
         boxes = _place_boxes(rng, sides)
+        if device:
+            from . import device_init as di
+            out.append(DeviceScene(
+                "config4_scene%03d" % i, 2, L, c, [di.box(lo, hi, L - 1) for lo, hi in boxes],
+                seed * 100003 + i, 1e-4, 1000, dict(E=1e4 / RHO[1], nu=0.2, gravity=(0.0, -9.8), boundary_mode="sticky"),
+                grid_initializer=band_level_map([(tuple(lo), tuple(hi)) for lo, hi in boxes], 2, L, c),
+                description="%d levels %d^2..%d^2, %d boxes" % (L, c, fin, len(boxes))))
+            continue
         xs = [fill_lattice(rng, 2, fin, *box_region(lo, hi)) for lo, hi in boxes]
         x = np.concatenate(xs) if xs else np.zeros((0, 2), np.float32)
         n = len(x)
@@ -313,3 +324,82 @@ def make_batch_config(seed=0, n_scenes=256, scale=1.0):
                          grid_initializer=band_level_map([(tuple(lo), tuple(hi)) for lo, hi in boxes], 2, L, c),
                          description="%d levels %d^2..%d^2, %d boxes, %d particles" % (L, c, fin, len(boxes), n)))
     return out
+
+
+# ---------------------------------------------------------------------------
+# The same configurations generated on the GPU (agimp_lattice_fill): shapes and
+# materials as above, lattice jitter from Philox keyed by the seed instead of
+# numpy's generator, so the particles are another draw of the same scene.
+# (Config 2's random boxes use the same numpy draws for their sizes, places and
+# velocities, minus the jitter draws the host version makes between them.)
+
+
+@dataclass
+class DeviceScene:
+    name: str
+    dim: int
+    level: int
+    coarsest: int
+    shapes: list
+    seed: int
+    dt: float
+    steps: int
+    sim_kwargs: dict = field(default_factory=dict)
+    grid_initializer: object = None
+    refine_every: int = 0
+    refine_band: int = 3
+    description: str = ""
+    per_axis: int = 2
+    _n: int = -1
+
+    @property
+    def n(self):
+        if self._n < 0:
+            from . import device_init as di
+            self._n = di.lattice_count(self.dim, self.coarsest << (self.level - 1), self.shapes, self.seed,
+                                       self.per_axis)
+        return self._n
+
+    def build(self, **over):
+        """Construct an AdaptiveGIMP whose particles are generated on the GPU."""
+        from . import device_init as di
+        from .simulator import AdaptiveGIMP
+        kw = dict(self.sim_kwargs)
+        kw.update(over)
+        return AdaptiveGIMP(self.dim, self.level, self.coarsest, self.n,
+                            di.lattice_initializer(self.shapes, self.seed, self.per_axis), self.grid_initializer, **kw)
+
+
+def make_device_config(k, seed=0, scale=1.0):
+    """Configurations 1, 2, 3 and 5 with their particles generated on the GPU."""
+    from . import device_init as di
+    host = make_config(k, seed, scale=min(scale, 1e-3)) if k in (1, 2, 3, 5) else None
+    if host is None:
+        raise ValueError("device scenes: configs 1, 2, 3 and 5 (config 4: make_batch_config(device=True))")
+    L, c = host.level, host.coarsest
+    if k == 1:
+        shapes = [di.box((0.3 - 0.1 * scale, 0.5 - 0.1 * scale), (0.3 + 0.1 * scale, 0.5 + 0.1 * scale), L - 1),
+                  di.box((0.6 - 0.1 * scale, 0.7 - 0.1 * scale), (0.6 + 0.1 * scale, 0.7 + 0.1 * scale), L - 1)]
+        boxes = [((0.3 - 0.1 * scale, 0.5 - 0.1 * scale), (0.3 + 0.1 * scale, 0.5 + 0.1 * scale)),
+                 ((0.6 - 0.1 * scale, 0.7 - 0.1 * scale), (0.6 + 0.1 * scale, 0.7 + 0.1 * scale))]
+        gi = band_level_map(boxes, 2, L, c)
+    elif k == 2:
+        rng = np.random.default_rng(seed)
+        shapes = []
+        for _ in range(3):
+            side = rng.uniform(0.1, 0.25, 2) * scale
+            lo = rng.uniform(0.1, 0.9 - side)
+            vel = rng.uniform(-1, 1, 2).astype(np.float32)
+            shapes.append(di.box(lo, lo + side, L - 1, velocity=vel))
+        gi = None
+    elif k == 3:
+        shapes = [di.sphere((0.5, 0.6, 0.5), 0.15 * scale, L - 1, velocity=(0.0, -3.0, 0.0))]
+        gi = None
+    else:
+        r = 0.12 * scale
+        shapes = [di.sphere((0.35, 0.5, 0.5), r, L - 1, velocity=(2.0, 0.0, 0.0)),
+                  di.sphere((0.65, 0.5, 0.5), r, L - 1, velocity=(-2.0, 0.0, 0.0))]
+        gi = None
+    return DeviceScene(host.name + "_device", host.dim, L, c, shapes, seed, host.dt, host.steps, dict(host.sim_kwargs),
+                       grid_initializer=gi, refine_every=host.refine_every, refine_band=host.refine_band,
+                       description=host.description + " (particles generated on the GPU)")

@@ -285,8 +285,18 @@ class AdaptiveGIMP:
         self.grid_initializer = grid_initializer
         self.static_adaptivity = grid_initializer is not None
         if self.static_adaptivity:
-            table, H = tabulate_level_map(grid_initializer, dim, level, coarsest_size)
-            self.set_level_map(table, H)
+            # initializers that describe themselves are tabulated on the device
+            # (init.py's masks by rule number, maps constant per coarsest cell);
+            # any other Python callable is tabulated here
+            rule = getattr(grid_initializer, "device_rule", None)
+            coarse = getattr(grid_initializer, "coarse_levels", None)
+            if rule is not None and (rule != 3 or level >= 3) and (rule in (1, 3) or level >= 4):
+                self.set_level_map_rule(rule)
+            elif coarse is not None and np.shape(coarse) == (coarsest_size,) * dim:
+                self.set_coarse_level_map(coarse)
+            else:
+                table, H = tabulate_level_map(grid_initializer, dim, level, coarsest_size)
+                self.set_level_map(table, H)
 
     # -- lifetime ----------------------------------------------------------
     def close(self):
@@ -316,6 +326,31 @@ class AdaptiveGIMP:
         _capi.check(self._L.agimp_set_level_map(self._h, _ptr(t), int(halo), AGIMP_MEM_HOST, None), self._h,
                     "set level map")
         self.static_adaptivity = True
+
+    def set_level_map_rule(self, rule, stream=None):
+        """initialize_mask<rule> of init.py:34-98, tabulated on the device."""
+        st = stream if stream is not None else _torch_stream()
+        _capi.check(self._L.agimp_set_level_map_rule(self._h, int(rule), st), self._h, "level map rule")
+        self.static_adaptivity = True
+
+    def set_coarse_level_map(self, coarse_levels, stream=None):
+        """A level map constant per coarsest cell (coarsest_size^dim levels),
+        expanded to the finest cells on the device."""
+        c = np.ascontiguousarray(coarse_levels, np.int8)
+        st = stream if stream is not None else _torch_stream()
+        _capi.check(self._L.agimp_set_coarse_level_map(self._h, _ptr(c), AGIMP_MEM_HOST, st), self._h,
+                    "coarse level map")
+        self.static_adaptivity = True
+
+    def get_level_map(self):
+        """The selected level map: (table int8 [(finest + 2 halo)]*dim, halo)."""
+        H = ctypes.c_int32()
+        _capi.check(self._L.agimp_get_level_map(self._h, None, ctypes.byref(H), AGIMP_MEM_HOST, None), self._h,
+                    "level map")
+        n = self.finest_size + 2 * H.value
+        t = np.empty((n,) * self.dim, np.int8)
+        _capi.check(self._L.agimp_get_level_map(self._h, _ptr(t), None, AGIMP_MEM_HOST, None), self._h, "level map")
+        return t, H.value
 
     def clear_level_map(self):
         _capi.check(self._L.agimp_clear_level_map(self._h), self._h, "clear level map")

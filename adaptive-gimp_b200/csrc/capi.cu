@@ -172,6 +172,28 @@ int gs_blocks(long long n) {
 
 }  // namespace
 
+namespace agimp {
+// Makes the device table (ownership passes to the simulator) its level map
+// and switches the substep to static activation.
+agimp_status install_level_map(agimp_sim* s, int8_t* dev_table, int halo, int n) {
+  CK(cudaDeviceSynchronize());  // substeps in flight may read the old map
+  if (s->map_dev) cudaFree(s->map_dev);
+  s->map_dev = dev_table;
+  if (!s->c.touch_occ) {
+    // base-cell records of the touched blocks (static mode only)
+    const size_t words = (size_t)s->c.lev[s->c.L - 1].nblocks * (s->c.dim == 2 ? 1 : 5);
+    CK(cudaMalloc(&s->c.touch_occ, words * sizeof(uint32_t)));
+    CK(cudaMemset(s->c.touch_occ, 0, words * sizeof(uint32_t)));
+  }
+  s->c.map = s->map_dev;
+  s->c.map_h = halo;
+  s->c.map_n = n;
+  s->c.is_static = 1;
+  drop_graphs(s);
+  return AGIMP_OK;
+}
+}  // namespace agimp
+
 extern "C" {
 
 int agimp_abi_version(void) { return AGIMP_ABI_VERSION; }
@@ -552,23 +574,29 @@ agimp_status agimp_set_level_map(agimp_sim* s, const int8_t* table, int32_t halo
     if (e < 0 || (e & 15) >= s->c.L || (e & ~(15 | 64)))
       return fail(s, AGIMP_INVALID_ARG, "level map entry out of range at " + std::to_string(i));
   }
-  CK(cudaStreamSynchronize(0));
-  if (s->map_dev) cudaFree(s->map_dev);
-  s->map_dev = nullptr;
-  CK(cudaMalloc(&s->map_dev, bytes));
-  CK(cudaMemcpy(s->map_dev, host.data(), bytes, cudaMemcpyHostToDevice));
-  if (!s->c.touch_occ) {
-    // base-cell records of the touched blocks (static mode only)
-    const size_t words = (size_t)s->c.lev[s->c.L - 1].nblocks * (s->c.dim == 2 ? 1 : 5);
-    CK(cudaMalloc(&s->c.touch_occ, words * sizeof(uint32_t)));
-    CK(cudaMemset(s->c.touch_occ, 0, words * sizeof(uint32_t)));
+  int8_t* table_dev = nullptr;
+  CK(cudaMalloc(&table_dev, bytes));
+  const cudaError_t e = cudaMemcpy(table_dev, host.data(), bytes, cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) {
+    cudaFree(table_dev);
+    return cuda_fail(s, e, "level map upload");
   }
-  s->c.map = s->map_dev;
-  s->c.map_h = halo;
-  s->c.map_n = n;
-  s->c.is_static = 1;
-  drop_graphs(s);
   (void)stream;
+  return install_level_map(s, table_dev, halo, n);
+}
+
+agimp_status agimp_get_level_map(agimp_sim* s, int8_t* table, int32_t* halo, int32_t memory, void* stream) {
+  if (!s || (memory != AGIMP_MEM_DEVICE && memory != AGIMP_MEM_HOST)) return fail(s, AGIMP_INVALID_ARG, "bad args");
+  if (!s->c.is_static || !s->map_dev) return fail(s, AGIMP_INVALID_ARG, "no level map selected");
+  if (halo) *halo = s->c.map_h;
+  if (!table) return AGIMP_OK;
+  CK(cudaSetDevice(s->device));
+  StreamUse su(s, stream);
+  size_t bytes = 1;
+  for (int d = 0; d < s->c.dim; ++d) bytes *= (size_t)s->c.map_n;
+  CK(cudaMemcpyAsync(table, s->map_dev, bytes, memory == AGIMP_MEM_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice,
+                     su.use));
+  if (memory == AGIMP_MEM_HOST) CK(cudaStreamSynchronize(su.use));
   return AGIMP_OK;
 }
 

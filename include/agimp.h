@@ -144,6 +144,9 @@ agimp_status agimp_get_particles_async(agimp_sim* s, float* x, float* v, float* 
  * activation from g_p (adaptive_gimp.py:87-96). */
 agimp_status agimp_set_level_map(agimp_sim* s, const int8_t* table, int32_t halo, int32_t memory, void* stream);
 agimp_status agimp_clear_level_map(agimp_sim* s);
+/* Readback of the selected level map: *halo, and when table is not null the
+ * (finest + 2 halo)^dim entries in the layout agimp_set_level_map takes. */
+agimp_status agimp_get_level_map(agimp_sim* s, int8_t* table, int32_t* halo, int32_t memory, void* stream);
 
 /* Replaces AdaptiveGIMP.substep(dt0) (adaptive_gimp.py:323-352), run n_steps
  * times back to back.  Asynchronous on `stream`.  With graphs enabled (the
@@ -313,6 +316,69 @@ int32_t agimp_batch_kernels_per_substep(const agimp_batch* b);
 agimp_status agimp_batch_positions_async(agimp_batch* b, float* x, void* stream);
 /* As agimp_profile_substep, for one substep of the whole batch. */
 agimp_status agimp_batch_profile_substep(agimp_batch* b, float dt, float* ms, int32_t n, void* stream);
+
+/* ---- Scene initialisers on the device.  The reference fills x_p, v_p, F_p,
+ * m_p, g_p with Taichi kernels (init.py:3-32 initialize_particle,
+ * run_3d.py:14-32 init_p) and tabulates its grid initializer through
+ * activate_cell (init.py:34-98).  These write the simulator's state (and its
+ * level map) on the GPU from a small description, so a large scene needs no
+ * host arrays and no upload.  Every particle gets F = I, C = 0, Jp = 1, and
+ * its index in the generation order as the caller's index (readback returns
+ * particles in that order).  Random numbers: Philox4x32-10 (Salmon et al.,
+ * SC 2011) keyed by the 64-bit seed, counter = the particle's (or lattice
+ * point's) index: the result does not depend on the launch shape. */
+#define AGIMP_SHAPE_BOX 0
+#define AGIMP_SHAPE_SPHERE 1
+typedef struct agimp_shape {
+  int32_t kind;        /* AGIMP_SHAPE_BOX: lo <= x < hi; AGIMP_SHAPE_SPHERE: |x - centre|^2 < radius^2 */
+  int32_t level;       /* g_p of its particles */
+  double lo[3], hi[3]; /* box corners */
+  double centre[3], radius;
+  float velocity[3];
+  float mass;
+} agimp_shape;
+/* Points of a jittered sub-lattice inside the shapes (the synthetic
+ * benchmark scenes): per_axis points per finest cell and axis, at
+ * (start + i + 1/2) h with h = 1 / (finest per_axis), i over the shape's
+ * bounding box [floor(lo / h), ceil(hi / h)); with jitter, each moved by
+ * -h/2 + h u per axis (u uniform in [0, 1), 53 bits, counter (k, shape,
+ * 0 / 1) for lattice point k of the shape); kept when the moved point lies
+ * inside its shape.  Shapes one after another, each in row-major lattice
+ * order (first axis slowest).  Positions are computed in double and rounded
+ * to float once.  Count first (to create the simulator), then fill: the
+ * fill requires exactly n_particles points.  At most 64 shapes. */
+agimp_status agimp_lattice_count(int32_t dim, int32_t finest, int32_t per_axis, int32_t jitter, uint64_t seed,
+                                 const agimp_shape* shapes, int32_t n_shapes, int64_t* count, int32_t device);
+agimp_status agimp_lattice_fill(agimp_sim* s, int32_t per_axis, int32_t jitter, uint64_t seed,
+                                const agimp_shape* shapes, int32_t n_shapes, void* stream);
+/* init.py:3-32 / run_3d.py:14-32: `count` particles per box, consecutive
+ * boxes in order (the reference's two halves of the particle range), at
+ * x = u size + lo in float (u uniform in [0, 1)^dim, 24 bits, counter
+ * (index, 0, 0, 0)); g_p = band_level[k] of the first band k with
+ * band_lo[k] <= u_d <= band_hi[k] on every axis, else `level` (the
+ * reference's `if all(0.2 <= xy <= 0.8)` chain).  The counts must sum to
+ * n_particles.  At most 16 boxes. */
+typedef struct agimp_random_box {
+  int64_t count;
+  float lo[3], size[3];
+  float velocity[3];
+  float mass;
+  int32_t n_bands; /* 0..4 */
+  float band_lo[4], band_hi[4];
+  int32_t band_level[4];
+  int32_t level;
+} agimp_random_box;
+agimp_status agimp_random_fill(agimp_sim* s, uint64_t seed, const agimp_random_box* boxes, int32_t n_boxes,
+                               void* stream);
+/* initialize_mask1..5 (init.py:34-98) tabulated on the device: the same table
+ * agimp_set_level_map takes, over finest cells [-halo, finest + halo)^dim with
+ * halo = max(2, 2^(level-1)).  Rules 2, 4 and 5 use level 3 and need 4 levels,
+ * rule 3 needs 3. */
+agimp_status agimp_set_level_map_rule(agimp_sim* s, int32_t rule, void* stream);
+/* A level map constant on each coarsest cell: a finest cell inside the domain
+ * gets coarse_levels[its coarsest cell] (activating), the halo level-1 without
+ * activation.  coarse_levels: coarsest_size^dim int8, first axis slowest. */
+agimp_status agimp_set_coarse_level_map(agimp_sim* s, const int8_t* coarse_levels, int32_t memory, void* stream);
 
 #ifdef __cplusplus
 }
