@@ -58,7 +58,9 @@ struct P2GLayout {
   static constexpr int ROWS = (D == 2) ? 3 : 9;   // node rows per stencil
   static constexpr int SLOTS = 32 / ROWS;         // tasks served by one warp at once
   static constexpr int TN = (D == 2) ? 36 : 216;  // nodes of the (4+2)^d tile
-  static constexpr int TMAX = 16;                 // particles per task
+  // particles per task: in 3D a run over the whole warp fills the 3 slots
+  // (11 + 11 + 10); in 2D runs are short (4 per base cell at the finest level)
+  static constexpr int TMAX = (D == 3) ? 11 : 16;
   // per-particle record:
   //   [0, 4)          m, a_0 .. a_{d-1}                 a = m (v - C (tc + 1))
   //   [4, 4 + 2d^2)   B = m C (row-major), then the scaled stress S (row-major)
