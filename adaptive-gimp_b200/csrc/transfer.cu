@@ -716,6 +716,13 @@ __device__ __forceinline__ void g2p_one(const Ctx& c, int j) {
   const long long N = c.N;
   const int p = __ldg(&c.perm[j]);
   const int l = __ldg(&c.P.fl[p]);
+  // the fields read after the gather start moving into L1 now (no registers held)
+#pragma unroll
+  for (int k = 0; k < D * D; ++k) asm volatile("prefetch.global.L1 [%0];" ::"l"(&c.P.F[k * N + p]));
+  asm volatile("prefetch.global.L1 [%0];" ::"l"(&c.P.m[p]));
+  asm volatile("prefetch.global.L1 [%0];" ::"l"(&c.P.g[p]));
+  asm volatile("prefetch.global.L1 [%0];" ::"l"(&c.P.id[p]));
+  if (c.plast == 1) asm volatile("prefetch.global.L1 [%0];" ::"l"(&c.P.Jp[p]));
   if (l < 0) {
     copy_particle<D>(c, p, j);
     return;
