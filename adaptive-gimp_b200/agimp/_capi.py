@@ -35,7 +35,7 @@ EXPORTS = (
     "agimp_batch_kernels_per_substep", "agimp_batch_profile_substep",
     "agimp_render_mask", "agimp_render_particles", "agimp_get_particles_async", "agimp_batch_positions_async",
     "agimp_get_level_map", "agimp_lattice_count", "agimp_lattice_fill", "agimp_random_fill",
-    "agimp_set_level_map_rule", "agimp_set_coarse_level_map",
+    "agimp_set_level_map_rule", "agimp_set_coarse_level_map", "agimp_render_scene3d", "agimp_cell_lines",
 )
 PHASES = ("blocks", "topology", "binning", "p2g", "restrict", "gridop", "prolong", "g2p")
 
@@ -78,6 +78,15 @@ class RandomBox(ctypes.Structure):
                 ("velocity", ctypes.c_float * 3), ("mass", ctypes.c_float), ("n_bands", ctypes.c_int32),
                 ("band_lo", ctypes.c_float * 4), ("band_hi", ctypes.c_float * 4), ("band_level", ctypes.c_int32 * 4),
                 ("level", ctypes.c_int32)]
+
+
+class View3D(ctypes.Structure):
+    _fields_ = [("eye", ctypes.c_float * 3), ("right", ctypes.c_float * 3), ("up", ctypes.c_float * 3),
+                ("forward", ctypes.c_float * 3), ("tan_half_fov", ctypes.c_float), ("radius", ctypes.c_float),
+                ("color", ctypes.c_float * 3), ("floor", ctypes.c_int32), ("floor_color", ctypes.c_float * 3),
+                ("ambient", ctypes.c_float * 3), ("n_lights", ctypes.c_int32),
+                ("light_pos", (ctypes.c_float * 3) * 4), ("light_color", (ctypes.c_float * 3) * 4),
+                ("background", ctypes.c_float * 3)]
 
 
 class AgimpError(RuntimeError):
@@ -165,6 +174,8 @@ def load(path: str | None = None):
     L.agimp_random_fill.argtypes = [vp, ctypes.c_uint64, ctypes.POINTER(RandomBox), ctypes.c_int32, vp]
     L.agimp_set_level_map_rule.argtypes = [vp, ctypes.c_int32, vp]
     L.agimp_set_coarse_level_map.argtypes = [vp, vp, ctypes.c_int32, vp]
+    L.agimp_render_scene3d.argtypes = [vp, ctypes.c_int32, ctypes.POINTER(View3D), vp, ctypes.c_int32, vp]
+    L.agimp_cell_lines.argtypes = [vp, vp, ctypes.c_int64, ctypes.POINTER(ctypes.c_int64), ctypes.c_int32, vp]
     _lib = L
     return L
 

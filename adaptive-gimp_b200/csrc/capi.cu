@@ -401,6 +401,9 @@ agimp_status agimp_destroy(agimp_sim* s) {
   for (cudaEvent_t e : {s->ev_state, s->ev_read[0], s->ev_read[1]})
     if (e) cudaEventDestroy(e);
   if (s->rwin) cudaFree(s->rwin);
+  if (s->rkey) cudaFree(s->rkey);
+  if (s->rdir) cudaFree(s->rdir);
+  if (s->rslot) cudaFree(s->rslot);
   if (s->map_dev) cudaFree(s->map_dev);
   if (s->c.touch_occ) cudaFree(s->c.touch_occ);
   if (s->internal) cudaStreamDestroy(s->internal);
@@ -805,6 +808,25 @@ agimp_status agimp_render_particles(agimp_sim* s, int32_t res, float radius, con
   CK(cudaSetDevice(s->device));
   StreamUse su(s, stream);
   return render_particles(s, res, radius, colors, colors_memory, img, memory, su.use);
+}
+
+agimp_status agimp_render_scene3d(agimp_sim* s, int32_t res, const agimp_view3d* view, float* img, int32_t memory,
+                                  void* stream) {
+  if (!s) return AGIMP_INVALID_ARG;
+  CK(cudaSetDevice(s->device));
+  StreamUse su(s, stream);
+  return render_scene3d(s, res, view, img, memory, su.use);
+}
+
+agimp_status agimp_cell_lines(agimp_sim* s, float* vertices, int64_t capacity, int64_t* count, int32_t memory,
+                              void* stream) {
+  if (!s) return AGIMP_INVALID_ARG;
+  CK(cudaSetDevice(s->device));
+  StreamUse su(s, stream);
+  long long n = 0;
+  const agimp_status st = cell_lines(s, vertices, capacity, &n, memory, su.use);
+  if (count) *count = n;
+  return st;
 }
 
 // ---------------------------------------------------------------------------

@@ -37,6 +37,10 @@ struct agimp_sim {
   size_t rimg_floats = 0;
   int* rwin = nullptr;          // headless drawing: particle covering each pixel
   size_t rwin_n = 0;
+  unsigned long long* rkey = nullptr;  // 3D drawing: nearest sphere hit per pixel (depth, particle)
+  float* rdir = nullptr;               // 3D drawing: ray direction per pixel
+  int* rslot = nullptr;                // 3D drawing: storage slot of each caller particle index
+  size_t rkey_n = 0, rslot_n = 0;
 };
 
 // Several simulators (scenes) stepped together: one launch per kernel serves
@@ -97,6 +101,8 @@ agimp_status batch_autotune(agimp_batch* b, float dt, int trials, agimp_tuning* 
 agimp_status batch_set_tuning(agimp_batch* b, const agimp_tuning* t);
 // headless drawing (render.cu)
 agimp_status render_mask(agimp_sim* s, int res, int show_ghost, int show_node, float* img, int memory, cudaStream_t st);
+agimp_status render_scene3d(agimp_sim* s, int res, const agimp_view3d* v, float* img, int memory, cudaStream_t st);
+agimp_status cell_lines(agimp_sim* s, float* vert, long long cap, long long* count, int memory, cudaStream_t st);
 agimp_status render_particles(agimp_sim* s, int res, float radius, const float* colors, int colors_memory, float* img,
                               int memory, cudaStream_t st);
 }  // namespace agimp

@@ -271,6 +271,39 @@ agimp_status agimp_render_mask(agimp_sim* s, int32_t res, int32_t show_ghost, in
 agimp_status agimp_render_particles(agimp_sim* s, int32_t res, float radius, const float* colors,
                                     int32_t colors_memory, float* img, int32_t memory, void* stream);
 
+/* GUI3D.show (gui_3d.py:50-64) without a window: x_p as spheres of one
+ * radius and colour (scene.particles), optionally the unit floor quad y = 0
+ * (scene.mesh of bound_box), lit by point lights (scene.point_light) and an
+ * ambient term, seen from a pinhole camera.  Each pixel casts a ray through
+ * its centre; the nearest sphere (exact intersection; ties to the lower
+ * caller index) or the floor (two-sided) is shaded with Lambert terms, no
+ * shadows or specular (GGUI's own shaders are not reproduced).  The camera
+ * basis is orthonormal: ray = normalise(forward + sx right + sy up) with
+ * sx = (2 (col + 1/2) / res - 1) tan_half_fov, sy = (1 - 2 (row + 1/2) / res)
+ * tan_half_fov.  img: [res][res][3] f32, row 0 at the top.  Spheres that reach
+ * the camera's plane are not drawn.  Allocates its scratch on first use. */
+typedef struct agimp_view3d {
+  float eye[3], right[3], up[3], forward[3];
+  float tan_half_fov; /* tan(vertical field of view / 2) */
+  float radius;       /* sphere radius (scene.particles radius) */
+  float color[3];     /* sphere colour */
+  int32_t floor;      /* draw the floor quad [0,1] x {0} x [0,1] */
+  float floor_color[3];
+  float ambient[3];
+  int32_t n_lights;   /* 0..4 */
+  float light_pos[4][3], light_color[4][3];
+  float background[3];
+} agimp_view3d;
+agimp_status agimp_render_scene3d(agimp_sim* s, int32_t res, const agimp_view3d* view, float* img, int32_t memory,
+                                  void* stream);
+/* GUI3D._draw_lines (gui_3d.py:35-47): for every cell whose mask is exactly
+ * ACTIVATED, at every level, the 24 vertices [24][3] (f32) of its 12 edges in
+ * the reference's stencil order (corner k = dI_0 + 2 dI_1 + 4 dI_2 at
+ * (I + dI) dx).  Cells come in no fixed order.  Writes at most `capacity`
+ * vertices and returns in *count the number of vertices of all cells.  3D only. */
+agimp_status agimp_cell_lines(agimp_sim* s, float* vertices, int64_t capacity, int64_t* count, int32_t memory,
+                              void* stream);
+
 /* ---- Launch tuning (no counterpart in the reference: Taichi picks its own
  * launch sizes).  Results do not depend on it beyond the order of float
  * additions. */

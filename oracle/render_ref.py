@@ -83,3 +83,107 @@ def splat_particles(img, x, colors, radius):
         sub = img[i0:i1 + 1, j0:j1 + 1]
         sub[cov] = np.float32(colors[k])
     return img
+
+
+# ---------------------------------------------------------------------------
+# 3D: the library's stated picture of GUI3D.show (gui_3d.py:50-64): ray-cast
+# spheres and floor with Lambert point lights, every operation in float32 in
+# the kernel's order (dot products ((a0 b0 + a1 b1) + a2 b2)).
+
+def _dot3(a, b):
+    f = np.float32
+    return (f(a[0]) * f(b[0]) + f(a[1]) * f(b[1])) + f(a[2]) * f(b[2])
+
+
+def rays3d(view, res):
+    f = np.float32
+    col = np.arange(res, dtype=np.float32)[None, :].repeat(res, 0)
+    row = np.arange(res, dtype=np.float32)[:, None].repeat(res, 1)
+    fr, th = f(res), f(view["tan_half_fov"])
+    sx = ((f(2) * (col + f(0.5))) / fr - f(1)) * th
+    sy = (f(1) - (f(2) * (row + f(0.5))) / fr) * th
+    d = [(f(view["forward"][k]) + sx * f(view["right"][k])) + sy * f(view["up"][k]) for k in range(3)]
+    inv = f(1) / np.sqrt(_dot3(d, d))
+    return [dk * inv for dk in d]  # three [res][res] arrays
+
+
+def _shade(view, base, p, n):
+    f = np.float32
+    out = [f(base[k]) * f(view["ambient"][k]) + np.zeros_like(p[0]) for k in range(3)]
+    for lp, lc in view["lights"]:
+        L = [f(lp[k]) - p[k] for k in range(3)]
+        inv = f(1) / np.sqrt(_dot3(L, L))
+        L = [Lk * inv for Lk in L]
+        ndl = np.maximum(_dot3(n, L), f(0))
+        out = [out[k] + (f(base[k]) * f(lc[k])) * ndl for k in range(3)]
+    return out
+
+
+def render_scene3d(x, res, view):
+    """x [N][3] f32 in caller order; view: dict of eye, right, up, forward,
+    tan_half_fov, radius, color, floor, floor_color, ambient, lights
+    [(pos, colour)], background.  Returns [res][res][3] f32, row 0 on top."""
+    f = np.float32
+    d = rays3d(view, res)
+    R = f(view["radius"])
+    eye = [f(v) for v in view["eye"]]
+    best_t = np.full((res, res), np.inf, np.float32)
+    best_i = np.full((res, res), -1, np.int64)
+    for i, c in enumerate(np.asarray(x, np.float32)):
+        w = [f(c[k]) - eye[k] for k in range(3)]
+        oc = [-wk for wk in w]
+        cz = _dot3(w, view["forward"])
+        if not cz > R:
+            continue
+        cc = _dot3(oc, oc) - R * R
+        b = _dot3(oc, d)
+        disc = b * b - cc
+        with np.errstate(invalid="ignore"):
+            t = -b - np.sqrt(disc)
+        hit = (disc >= 0) & (t > 0) & ((t < best_t) | ((t == best_t) & (i < best_i)))
+        best_t = np.where(hit, t, best_t)
+        best_i = np.where(hit, i, best_i)
+    img = np.zeros((res, res, 3), np.float32)
+    for k in range(3):
+        img[..., k] = f(view["background"][k])
+    tf = np.full((res, res), np.inf, np.float32)
+    if view["floor"]:
+        with np.errstate(divide="ignore", invalid="ignore"):
+            t = (-eye[1]) / d[1]
+        hf = [eye[k] + t * d[k] for k in range(3)]
+        ok = (d[1] != 0) & (t > 0) & (hf[0] >= 0) & (hf[0] <= 1) & (hf[2] >= 0) & (hf[2] <= 1)
+        tf = np.where(ok, t, tf)
+        use = tf < best_t
+        if use.any():
+            p = [hf[0][use], np.zeros(use.sum(), np.float32), hf[2][use]]
+            ny = f(1) if eye[1] >= 0 else f(-1)
+            n = [np.zeros_like(p[0]), np.full_like(p[0], ny), np.zeros_like(p[0])]
+            out = _shade(view, view["floor_color"], p, n)
+            for k in range(3):
+                img[..., k][use] = out[k]
+    sph = ~(tf < best_t) & np.isfinite(best_t)
+    if sph.any():
+        t = best_t[sph]
+        cen = np.asarray(x, np.float32)[best_i[sph]]
+        p = [eye[k] + t * d[k][sph] for k in range(3)]
+        n = [(p[k] - cen[:, k]) / R for k in range(3)]
+        out = _shade(view, view["color"], p, n)
+        for k in range(3):
+            img[..., k][sph] = out[k]
+    return img
+
+
+STENCIL = (0, 1, 2, 3, 4, 5, 6, 7, 0, 2, 1, 3, 4, 6, 5, 7, 0, 4, 1, 5, 2, 6, 3, 7)  # gui_3d.py:30-32
+
+
+def cell_lines(cell_masks, lo, coarsest):
+    """GUI3D._draw_lines over read-back 3D cell masks (level l array indexed
+    from `lo`): 24 vertices per exactly-ACTIVATED cell, cells in index order."""
+    out = []
+    for l, cm in enumerate(cell_masks):
+        dx = np.float32(np.float32(1.0 / coarsest) / np.float32(2 ** l))
+        for I in np.argwhere(cm == ACT):
+            I = I + lo
+            corners = [np.float32(I + np.array([(k >> a) & 1 for a in range(3)])) * dx for k in range(8)]
+            out.extend(corners[k] for k in STENCIL)
+    return np.asarray(out, np.float32).reshape(-1, 3)

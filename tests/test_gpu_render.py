@@ -64,3 +64,44 @@ def test_particles_and_device_output():
     gui = HeadlessGUI(res)
     np.testing.assert_array_equal(gui.show(sim), got)
     sim.close()
+
+
+def _view_dict(v):
+    return dict(eye=tuple(v.eye), right=tuple(v.right), up=tuple(v.up), forward=tuple(v.forward),
+                tan_half_fov=v.tan_half_fov, radius=v.radius, color=tuple(v.color), floor=bool(v.floor),
+                floor_color=tuple(v.floor_color), ambient=tuple(v.ambient),
+                lights=[(tuple(v.light_pos[i]), tuple(v.light_color[i])) for i in range(v.n_lights)],
+                background=tuple(v.background))
+
+
+@pytest.mark.parametrize("res,radius,floor", [(96, 0.02, True), (160, 0.05, False)])
+def test_scene3d_matches_restatement(res, radius, floor):
+    # a small 3D scene stepped a few substeps (particles in bin order on the
+    # device) rendered with GUI3D's camera and lights
+    from agimp import scenes
+    from agimp.render import render_scene3d, view3d
+    sc = scenes.make_config(3, scale=0.25)
+    sim = sc.build()
+    for i in range(5):
+        if i % sc.refine_every == 0:
+            sim.refine_levels(sc.refine_band)
+        sim.substep(sc.dt)
+    v = view3d(radius=radius, floor=floor, ambient=(0.05, 0.05, 0.05))
+    got = render_scene3d(sim, res, v)
+    exp = R.render_scene3d(sim.x_p.to_numpy(), res, _view_dict(v))
+    np.testing.assert_array_equal(got, exp)
+    assert (got > 0).any(axis=2).sum() > res  # spheres (and floor) are drawn
+    sim.close()
+
+
+def test_cell_lines_match_restatement():
+    from agimp import scenes
+    from agimp.render import cell_lines
+    sc, sim = _scene(3, 0.25, 12)
+    got = cell_lines(sim)
+    cells = [sim.cell_mask[l].read(LO, (sim.coarsest_size << l) + 12) for l in range(sim.level)]
+    exp = R.cell_lines(cells, LO, sim.coarsest_size)
+    assert got.shape == exp.shape and len(got) > 24
+    key = lambda v: sorted(map(bytes, v.reshape(-1, 24 * 3)))  # cells in any order
+    assert key(got) == key(exp)
+    sim.close()

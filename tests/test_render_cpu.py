@@ -43,3 +43,45 @@ def test_restated_particle_circles():
     assert (img[9, 9] == [1, 0, 0]).all()      # drawn in the other order
     assert (img[11, 8] == [0, 1, 0]).all()
     assert (img[0, 0] == 0).all()
+
+
+def _view(res_fov=55.0):
+    from agimp.render import camera_basis
+    r, u, f = camera_basis((0.5, 1.0, 1.95), (0.5, 0.3, 0.5))
+    return dict(eye=(0.5, 1.0, 1.95), right=r, up=u, forward=f,
+                tan_half_fov=np.float32(np.tan(np.radians(res_fov) / 2)), radius=0.02, color=(0.5, 0.5, 0.5),
+                floor=True, floor_color=(0.0, 0.0, 0.9), ambient=(0.0, 0.0, 0.0),
+                lights=[((0.5, 1.5, 0.5), (0.5, 0.5, 0.5)), ((0.5, 1.5, 1.5), (0.5, 0.5, 0.5))],
+                background=(0.0, 0.0, 0.0))
+
+
+def test_restated_scene3d_sphere_and_floor():
+    v = _view()
+    v["radius"] = 0.1
+    res = 64
+    # a sphere at the look-at point appears at the image centre, lit from above
+    img = R.render_scene3d(np.array([[0.5, 0.3, 0.5]], np.float32), res, v)
+    c = img[res // 2, res // 2]
+    assert c[0] == c[1] == c[2] and c[0] > 0.05
+    # the floor (blue) is seen below it (the camera at z = 1.95 sees past its
+    # near edge z = 1 at the bottom rows), the background (black) above it
+    col = img[:, res // 2]
+    floor_rows = np.nonzero((col[:, 2] > 0) & (col[:, 0] == 0))[0]
+    assert len(floor_rows) > res // 4 and floor_rows.min() > res // 2 - 8 and floor_rows.max() < res - 4
+    assert (img[1, res // 2] == 0).all()
+    # no particles: only the floor
+    empty = R.render_scene3d(np.zeros((0, 3), np.float32), res, v)
+    assert (empty[..., 0] == 0).all() and (empty[..., 2] > 0).sum() > res * res // 10
+
+
+def test_restated_cell_lines():
+    cm0 = np.zeros((2 + 12, 2 + 12, 2 + 12), np.int32)
+    cm0[4 + 1, 4 + 0, 4 + 1] = R.ACT  # cell (1, 0, 1) of level 0, coarsest 2
+    cm1 = np.zeros((4 + 12,) * 3, np.int32)
+    cm1[4 + 3, 4 + 3, 4 + 3] = R.GHO  # not drawn
+    v = R.cell_lines([cm0, cm1], -4, 2)
+    assert v.shape == (24, 3)
+    # first edge: corner 0 -> corner 1 (dI = (0,0,0) -> (1,0,0)), dx = 0.5
+    np.testing.assert_array_equal(v[0], [0.5, 0.0, 0.5])
+    np.testing.assert_array_equal(v[1], [1.0, 0.0, 0.5])
+    np.testing.assert_array_equal(v[-1], [1.0, 0.5, 1.0])  # corner 7
