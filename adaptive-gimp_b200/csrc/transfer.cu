@@ -23,12 +23,15 @@
 
 namespace agimp {
 
+// first stored cell of block `blk` (block indices are 32-bit: 32-bit division)
 template <int D>
 __device__ __forceinline__ void chunk_origin(const LevelDev& V, long long blk, int* O) {
+  unsigned b = (unsigned)blk;
+  const unsigned nb = (unsigned)V.nb;
 #pragma unroll
   for (int d = D - 1; d >= 0; --d) {
-    O[d] = (int)(blk % V.nb) * 4 - HALO;
-    blk /= V.nb;
+    O[d] = (int)(b % nb) * 4 - HALO;
+    b /= nb;
   }
 }
 
@@ -49,9 +52,12 @@ __device__ __forceinline__ void chunk_origin(const LevelDev& V, long long blk, i
 //     over the task's particles in registers: one read of a particle record
 //     serves three nodes, and the row's weight products are shared; the sums
 //     go once into the (4+2)^d node tile in shared memory;
-//  4. after the work item's one barrier the tile is flushed with one float4
-//     atomic per touched node and cleared.  Two tiles alternate between work
-//     items, so the next item's records and sums need no further barrier.
+//  4. a CTA takes a contiguous range of work items, so consecutive items of
+//     one block (a dense block holds many) keep summing into the same tile;
+//     when the next item is another block, the tile is flushed after one
+//     barrier with one float4 atomic per touched node and cleared.  Two tiles
+//     alternate between blocks, so the next block's records and sums need no
+//     further barrier.
 template <int D, int CH>
 struct P2GLayout {
   static constexpr int NC = 1 << (2 * D);        // cells per block
@@ -93,10 +99,18 @@ __global__ void __launch_bounds__(CH, 1024 / CH) k_p2g(Batch B) {
   for (int i = threadIdx.x; i < 2 * 4 * Y::TN; i += blockDim.x) tiles[i] = 0.f;
   __syncthreads();
   int tb = 0;
-  for (int ch = bid_; ch < nch; ch += nblk_) {
+  const int per = (nch + nblk_ - 1) / nblk_;
+  const int c0 = bid_ * per, c1 = min(nch, c0 + per);
+  for (int ch = c0; ch < c1; ++ch) {
     const int4 wd = c.chunks[ch];
     const int l = wd.x;
     if (l < 0) continue;  // particles without a level: no transfer (uniform over the CTA)
+    // the tile is flushed when the next work item of this CTA is another block
+    bool last = ch + 1 == c1;
+    if (!last) {
+      const int4 nx = c.chunks[ch + 1];
+      last = nx.x != wd.x || nx.y != wd.y;
+    }
     const LevelDev& V = c.lev[l];
     int O[D];
     chunk_origin<D>(V, wd.y, O);
@@ -287,6 +301,7 @@ __global__ void __launch_bounds__(CH, 1024 / CH) k_p2g(Batch B) {
         }
       }
     }
+    if (!last) continue;  // the same block follows: keep summing into this tile
     __syncthreads();
     // -- 4. flush and clear ---------------------------------------------------
     for (int t = threadIdx.x; t < Y::TN; t += blockDim.x) {
