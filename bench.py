@@ -266,6 +266,20 @@ def timed_steps(sim, scene, a, stream, dist=None, clocks=None):
     return e0.elapsed_time(e1)
 
 
+def job_totals(dist, device, times_ms, units):
+    """Whole-job figures over the ranks: each entry of `times_ms` is replaced
+    by its maximum over the ranks (the slowest rank's time) and `units` by
+    their sum (ranks may hold scenes of different sizes).  Without a process
+    group (one rank) the inputs come back unchanged."""
+    import torch
+    t = torch.tensor(list(times_ms), dtype=torch.float64, device=device)
+    u = torch.tensor([float(units)], dtype=torch.float64, device=device)
+    if dist:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        dist.all_reduce(u, op=dist.ReduceOp.SUM)
+    return [float(v) for v in t.tolist()], float(u.item())
+
+
 def surrogate_report(a, scene, sim, ms, local, tuning):
     """Plain (SVD return map) run of the same scene for comparison: its
     throughput and the surrogate run's position error against it."""
@@ -327,11 +341,8 @@ def run_agimp(a):
         stats = sim.stats()
         # per-phase timing of single substeps (direct launches, CUDA events)
         prof = [sim.profile_substep(scene.dt, stream=st) for _ in range(5)]
-    ms_t = torch.tensor([ms], device="cuda")
-    if dist:
-        dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
-    ms_max = float(ms_t.item())
-    value = world * scene.n * a.steps / (ms_max / 1e3)
+    (ms_max,), units = job_totals(dist, "cuda", [ms], scene.n * a.steps)
+    value = units / (ms_max / 1e3)
     phases = {k: statistics.median(p[k] for p in prof) for k in prof[0]}
     d = scene.dim
     jp = scene.sim_kwargs.get("plasticity") == "snow"
@@ -470,11 +481,8 @@ def run_batch(a):
             errs.append(float(np.abs(s.x_p.to_numpy().astype(np.float64) - b.x_p.to_numpy()).max()))
     for s in alone:
         s.close()
-    ms_t = torch.tensor([ms, ms_alone], device="cuda")
-    if dist:
-        dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
-    ms_max, ms_alone_max = (float(v) for v in ms_t.tolist())
-    value = world * n_tot * a.steps / (ms_max / 1e3)
+    (ms_max, ms_alone_max), units = job_totals(dist, "cuda", [ms, ms_alone], n_tot * a.steps)
+    value = units / (ms_max / 1e3)
     phases = {k: statistics.median(p[k] for p in prof) for k in prof[0]}
     b_p2g, b_g2p = BYTES[(2, False)]
     hbm, src = peaks()
@@ -500,7 +508,7 @@ def run_batch(a):
                                   "boxes, lognormal 2k-60k particles, static level maps, one launch per kernel "
                                   "for all scenes under a CUDA graph"},
         "tuning": tuning,
-        "one_at_a_time": {"value": world * n_tot * a.steps / (ms_alone_max / 1e3),
+        "one_at_a_time": {"value": units / (ms_alone_max / 1e3),
                           "ms_per_step": ms_alone_max / a.steps, "speedup_of_batch": ms_alone_max / ms_max,
                           "position_error_vs_batch": {"max_over_scenes": max(errs), "median": float(np.median(errs)),
                                                       "unit": "domain lengths"}},
