@@ -51,7 +51,8 @@ def test_default_params_are_reference_constants():
 @pytest.mark.parametrize("field,value", [("dim", 4), ("level", 0), ("level", 9), ("coarsest_size", 12),
                                          ("coarsest_size", 2), ("n_particles", -1), ("radius", 0.75),
                                          ("n_colliders", 5), ("plasticity", 7),
-                                         ("invalid_nodes", 2)])
+                                         ("invalid_nodes", 2), ("n_particles", 2 ** 30 + 1),
+                                         ("coarsest_size", 8192)])  # finest 16384 > 8192
 def test_create_rejects_invalid_params(field, value):
     from agimp import _capi
     lib = _capi.load()

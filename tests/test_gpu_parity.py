@@ -192,3 +192,17 @@ def test_static_reference_mask_via_scalar_initializer():
     np.testing.assert_array_equal(sim.fl_p.to_numpy(), z["s0_fl"])
     assert scale_rel(sim.x_p.to_numpy(), z["s0_x"]) <= RTOL_PART
     sim.close()
+
+
+def test_create_rejects_lattices_beyond_32bit_indices():
+    # a 3D level of 2048^3 cells stores 515^3 blocks of 64 cells: more than
+    # 2^31 elements, which the kernels' 32-bit element indices cannot address
+    import ctypes
+
+    from agimp import _capi
+    lib = _capi.load()
+    p = _capi.Params()
+    lib.agimp_default_params(ctypes.byref(p), 3, 1, 2048, 10)
+    h = ctypes.c_void_p()
+    assert lib.agimp_create(ctypes.byref(p), 0, ctypes.byref(h)) == 2  # AGIMP_CAPACITY
+    assert not h.value
