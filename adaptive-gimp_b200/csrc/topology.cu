@@ -208,15 +208,18 @@ __device__ __forceinline__ void touch_one(const Ctx& c, int p) {
       base[d] = (int)(xp[d] * inv + 0.5f) - 1;
       bk = bk * (c.sz + 4) + (base[d] + 2);
     }
-    const unsigned g2 = __match_any_sync(act, bk);
-    const int r2 = __popc(g2 & ((1u << lane) - 1u)), n2 = __popc(g2);
-    // at the finest level base = fb: its 2^d corners are cells of fb's window
+    // at the finest level base = fb: its 2^d corners are cells of fb's window,
+    // so a warp whose particles all map to the finest level skips this part
+    if (!__all_sync(act, level == c.L - 1)) {
+      const unsigned g2 = __match_any_sync(act, bk);
+      const int r2 = __popc(g2 & ((1u << lane) - 1u)), n2 = __popc(g2);
 #pragma unroll 1
-    for (int a = level < c.L - 1 ? r2 : (1 << D); a < (1 << D); a += n2) {
-      int I[D];
+      for (int a = level < c.L - 1 ? r2 : (1 << D); a < (1 << D); a += n2) {
+        int I[D];
 #pragma unroll
-      for (int d = 0; d < D; ++d) I[d] = (base[d] + ((a >> (D - 1 - d)) & 1)) * (1 << (c.L - 1 - level));
-      grid_init<D>(c, I);
+        for (int d = 0; d < D; ++d) I[d] = (base[d] + ((a >> (D - 1 - d)) & 1)) * (1 << (c.L - 1 - level));
+        grid_init<D>(c, I);
+      }
     }
   }
   // record the finest block for the active-block lists (first toucher appends)
