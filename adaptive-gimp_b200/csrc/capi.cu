@@ -312,6 +312,7 @@ agimp_status agimp_create(const agimp_params* p, int32_t device, agimp_sim** out
     long long cells = 1;
     for (int d = 0; d < D; ++d) cells *= c.sz;
     AL(c.occ, cells);
+    AL(c.occ2, cells);
   }
   cudaMemset(c.nmask, 0, Vf.nblocks * per * sizeof(uint32_t));
   AL(c.ctr, CTR_COUNT);

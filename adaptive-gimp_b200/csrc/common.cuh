@@ -104,7 +104,8 @@ struct Ctx {
   // substep's bin order (the host swaps P and Q between substeps).
   Particles P, Q;
   const int8_t* map;
-  uint8_t* occ;  // refinement scratch over the finest cells
+  uint8_t* occ;   // refinement scratch over the finest cells
+  uint8_t* occ2;  // its second buffer (the distance transform's passes alternate)
   // surrogate return map and training-pair recorder (extension)
   int sur;                   // 1: G2P hands particles that need a projection to the MLP
   int rec_stride;            // recorder: particles whose new slot is a multiple of this
