@@ -149,8 +149,9 @@ class Clocks:
 
 
 def refine_kernels(scene):
-    kmax = min(scene.refine_band * ((1 << (scene.level - 1)) - 1) + 1, 250)
-    return 5 + (kmax - 1)
+    """Kernels of one refinement: bounding box (2), occupancy (2), one
+    distance-transform pass per axis, level assignment."""
+    return 5 + scene.dim
 
 
 def run_steps(sim, scene, first, count, stream=None):
