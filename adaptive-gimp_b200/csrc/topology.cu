@@ -784,7 +784,7 @@ void launch_substep(const BatchLaunch& bl, cudaStream_t s, cudaEvent_t* ev) {
 
 int kernels_per_substep(const BatchLaunch& bl) {
   const int topo = 10 - (bl.any_dynamic ? 0 : 1);
-  return topo + 3 + (bl.any_plastic ? 1 : 0) + 2 * (bl.maxL - 1);
+  return topo + 2 + (bl.maxL == 1 ? 1 : 0) + (bl.any_plastic ? 1 : 0) + 2 * (bl.maxL - 1);
 }
 
 }  // namespace agimp

@@ -3,7 +3,9 @@
 // Reference steps (adaptive_gimp.py, g1n0st/adaptive-gimp):
 //   230-250 p2g               -> k_p2g      (all levels in one launch)
 //   289-301 grid_restriction  -> k_restrict (one launch per level, fine->coarse)
-//   277-287 grid_op           -> k_gridop   (all levels in one launch)
+//   277-287 grid_op           -> level 0 in the last k_restrict, level l in
+//                                k_prolong(l); k_gridop (all levels) only
+//                                when every scene has one level
 //   303-321 grid_prolongation -> k_prolong  (one launch per level, coarse->fine)
 //   252-275 g2p               -> k_g2p      (all levels in one launch)
 //
@@ -326,14 +328,103 @@ __global__ void __launch_bounds__(CH, 1024 / CH) k_p2g(Batch B) {
   }
 }
 
+// grid_op (adaptive_gimp.py:277-287) of node I of level l, stored at idx: an
+// activated node's momentum becomes its velocity (gravity, walls, colliders);
+// with inv_norm the other nodes with mass are divided by it.  I lies in
+// [0, size]^d.
+template <int D>
+__device__ __forceinline__ void gridop_node(const Ctx& c, int l, const int* I, long long idx) {
+  const LevelDev& V = c.lev[l];
+  const float4 nd = V.node[idx];
+  if (!(nd.w > 0.f)) return;
+  if (!is_activated(nm_get<D>(c, l, I))) {
+    if (c.inv_norm) V.node[idx] = make_float4(nd.x / nd.w, nd.y / nd.w, D == 3 ? nd.z / nd.w : nd.z, nd.w);
+    return;
+  }
+  float vv[3] = {nd.x, nd.y, nd.z};
+  const int s = c.L - 1 - l;
+  bool band = false;
+#pragma unroll
+  for (int d = 0; d < D; ++d) {
+    vv[d] = vv[d] / nd.w;
+    vv[d] = vv[d] + c.grav[d] * c.dt;
+    const int P = I[d] * (1 << s);
+    if (P < c.gap || P > c.sz - c.gap) {
+      band = true;
+      if (c.bmode == 0) vv[d] = 0.f;
+    }
+  }
+  if (c.bmode == 1 && band)
+#pragma unroll
+    for (int d = 0; d < D; ++d) vv[d] = 0.f;
+  if (c.ncol) {
+    const double ldx = 1.0 / (double)(c.coarsest << l);
+    for (int k = 0; k < c.ncol; ++k) {
+      bool in = true;
+#pragma unroll
+      for (int d = 0; d < D; ++d) {
+        const double pos = (double)I[d] * ldx;
+        in = in && pos >= c.col[k][d] && pos <= c.col[k][3 + d];
+      }
+      if (in)
+#pragma unroll
+        for (int d = 0; d < D; ++d) vv[d] = 0.f;
+    }
+  }
+  V.node[idx] = make_float4(vv[0], vv[1], vv[2], nd.w);
+}
+
 // ---------------------------------------------------------------------------
-// grid_restriction(l) as a gather over coarse nodes K of level l-1.
+// grid_restriction(l) as a gather over coarse nodes K of level l-1: the
+// restricted sum onto node K (stored at blk, loc)
+template <int D>
+__device__ __forceinline__ void restrict_node(const Ctx& c, int l, const int* K, const LevelDev& Vc,
+                                              const LevelDev& Vf, long long blk, int loc, int lsz) {
+  float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
+  bool any = false;
+#pragma unroll
+  for (int a = 0; a < ((D == 2) ? 9 : 27); ++a) {
+    int I[D], nrm = 0;
+    int t = a;
+    bool ok = true;
+#pragma unroll
+    for (int d = D - 1; d >= 0; --d) {
+      const int dI = t % 3 - 1;
+      t /= 3;
+      I[d] = 2 * K[d] - dI;
+      nrm += dI != 0;
+      ok = ok && I[d] >= 0 && I[d] <= lsz;
+    }
+    if (!ok) continue;
+    const uint32_t nm = nm_get<D>(c, l, I);
+    if (!((is_activated(nm) && nrm == 0) || is_tj(nm) || is_ghost(nm))) continue;
+    const float w = (nrm == 0) ? 1.f : (nrm == 1) ? 0.5f : (nrm == 2) ? 0.25f : 0.125f;
+    const float4 f = Vf.node[elem_of<D>(Vf, I)];
+    acc.x += f.x * w;
+    acc.y += f.y * w;
+    acc.z += f.z * w;
+    acc.w += f.w * w;
+    any = true;
+  }
+  if (!any) return;
+  float4* dst = &Vc.node[(blk << (2 * D)) | loc];
+  float4 o = *dst;
+  o.x += acc.x;
+  o.y += acc.y;
+  o.z += acc.z;
+  o.w += acc.w;
+  *dst = o;
+}
+
+// The last restriction (into level 0) also applies grid_op to level 0, whose
+// momentum no later pass reads; in a scene of one level it only does that.
 template <int D>
 __global__ void k_restrict(Batch B, int l) {
   SCENE_CTA(B, MAP_G);
-  if (l >= c.L) return;
+  const bool restrict_l = l < c.L;
+  if (!restrict_l && l != 1) return;
   const LevelDev& Vc = c.lev[l - 1];
-  const LevelDev& Vf = c.lev[l];
+  const LevelDev& Vf = c.lev[restrict_l ? l : l - 1];
   const long long tot = (long long)c.ctr[CTR_LEVEL + l - 1] << (2 * D);
   const int lsz = Vf.size, l0sz = Vc.size;
   SCENE_LOOP(e, tot) {
@@ -344,46 +435,16 @@ __global__ void k_restrict(Batch B, int l) {
     bool inr = true;
 #pragma unroll
     for (int d = 0; d < D; ++d) inr = inr && K[d] >= 0 && K[d] <= l0sz;
-    if (!inr || !is_valid(nm_get<D>(c, l - 1, K))) continue;
-    float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
-    bool any = false;
-#pragma unroll
-    for (int a = 0; a < ((D == 2) ? 9 : 27); ++a) {
-      int I[D], nrm = 0;
-      int t = a;
-      bool ok = true;
-#pragma unroll
-      for (int d = D - 1; d >= 0; --d) {
-        const int dI = t % 3 - 1;
-        t /= 3;
-        I[d] = 2 * K[d] - dI;
-        nrm += dI != 0;
-        ok = ok && I[d] >= 0 && I[d] <= lsz;
-      }
-      if (!ok) continue;
-      const uint32_t nm = nm_get<D>(c, l, I);
-      if (!((is_activated(nm) && nrm == 0) || is_tj(nm) || is_ghost(nm))) continue;
-      const float w = (nrm == 0) ? 1.f : (nrm == 1) ? 0.5f : (nrm == 2) ? 0.25f : 0.125f;
-      const float4 f = Vf.node[elem_of<D>(Vf, I)];
-      acc.x += f.x * w;
-      acc.y += f.y * w;
-      acc.z += f.z * w;
-      acc.w += f.w * w;
-      any = true;
-    }
-    if (!any) continue;
-    float4* dst = &Vc.node[(blk << (2 * D)) | loc];
-    float4 o = *dst;
-    o.x += acc.x;
-    o.y += acc.y;
-    o.z += acc.z;
-    o.w += acc.w;
-    *dst = o;
+    if (!inr) continue;
+    if (restrict_l && is_valid(nm_get<D>(c, l - 1, K))) restrict_node<D>(c, l, K, Vc, Vf, blk, loc, lsz);
+    if (l == 1) gridop_node<D>(c, 0, K, (blk << (2 * D)) | loc);
   }
 }
 
 // ---------------------------------------------------------------------------
-// grid_op (adaptive_gimp.py:277-287) for all levels.
+// grid_op for every level at once.  Only substeps whose scenes all have one
+// level launch it; otherwise the last restriction applies grid_op to level 0
+// and each prolongation to its own level (see there).
 template <int D>
 __global__ void k_gridop(Batch B) {
   SCENE_CTA(B, MAP_G);
@@ -398,45 +459,7 @@ __global__ void k_gridop(Batch B) {
     bool inr = true;
 #pragma unroll
     for (int d = 0; d < D; ++d) inr = inr && I[d] >= 0 && I[d] <= V.size;
-    if (!inr) continue;
-    const long long idx = (blk << (2 * D)) | loc;
-    const float4 nd = V.node[idx];
-    if (!(nd.w > 0.f)) continue;
-    if (!is_activated(nm_get<D>(c, l, I))) {
-      if (c.inv_norm) V.node[idx] = make_float4(nd.x / nd.w, nd.y / nd.w, D == 3 ? nd.z / nd.w : nd.z, nd.w);
-      continue;
-    }
-    float vv[3] = {nd.x, nd.y, nd.z};
-    const int s = c.L - 1 - l;
-    bool band = false;
-#pragma unroll
-    for (int d = 0; d < D; ++d) {
-      vv[d] = vv[d] / nd.w;
-      vv[d] = vv[d] + c.grav[d] * c.dt;
-      const int P = I[d] * (1 << s);
-      if (P < c.gap || P > c.sz - c.gap) {
-        band = true;
-        if (c.bmode == 0) vv[d] = 0.f;
-      }
-    }
-    if (c.bmode == 1 && band)
-#pragma unroll
-      for (int d = 0; d < D; ++d) vv[d] = 0.f;
-    if (c.ncol) {
-      const double ldx = 1.0 / (double)(c.coarsest << l);
-      for (int k = 0; k < c.ncol; ++k) {
-        bool in = true;
-#pragma unroll
-        for (int d = 0; d < D; ++d) {
-          const double pos = (double)I[d] * ldx;
-          in = in && pos >= c.col[k][d] && pos <= c.col[k][3 + d];
-        }
-        if (in)
-#pragma unroll
-          for (int d = 0; d < D; ++d) vv[d] = 0.f;
-      }
-    }
-    V.node[idx] = make_float4(vv[0], vv[1], vv[2], nd.w);
+    if (inr) gridop_node<D>(c, l, I, (blk << (2 * D)) | loc);
   }
 }
 
@@ -465,6 +488,9 @@ __global__ void k_prolong(Batch B, int l) {
       even = even && (J[d] & 1) == 0;
     }
     if (!inr) continue;
+    // this level's grid_op first: level l's momentum is no longer read (the
+    // restrictions are done) and its coarser neighbour is final
+    gridop_node<D>(c, l, J, (blk << (2 * D)) | loc);
     const uint32_t nm = nm_get<D>(c, l, J);
     const bool tg = is_tj(nm) || is_ghost(nm);
     if (!tg && !even) continue;
@@ -921,7 +947,9 @@ void launch_transfer(const BatchLaunch& bl, cudaStream_t s, cudaEvent_t* ev) {
   if (ev) cudaEventRecord(ev[4], s);
   for (int l = bl.maxL - 1; l >= 1; --l) k_restrict<D><<<G, 256, 0, s>>>(bl.b, l);
   if (ev) cudaEventRecord(ev[5], s);
-  k_gridop<D><<<G, 256, 0, s>>>(bl.b);
+  // with more than one level grid_op runs inside the restriction into level 0
+  // and the prolongations
+  if (bl.maxL == 1) k_gridop<D><<<G, 256, 0, s>>>(bl.b);
   if (ev) cudaEventRecord(ev[6], s);
   for (int l = 1; l < bl.maxL; ++l) k_prolong<D><<<G, 256, 0, s>>>(bl.b, l);
   if (ev) cudaEventRecord(ev[7], s);

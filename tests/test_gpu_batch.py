@@ -83,9 +83,10 @@ def test_batch_matches_scenes_stepped_alone():
             assert np.abs(a["v"] - b["v"]).max() <= 1e-3 * max(1.0, np.abs(a["v"]).max())
         assert together[k].stats()["substeps"] == steps
     # 10 topology and binning kernels (k_mark_hier included: one scene is
-    # dynamic), P2G, grid_op, G2P, the return map (one scene has snow
-    # plasticity), and a restriction and a prolongation per level above 0
-    assert batch.kernels_per_substep() == 10 + 4 + 2 * (max(s.level for s in sc) - 1)
+    # dynamic), P2G, G2P, the return map (one scene has snow plasticity), and
+    # a restriction and a prolongation per level above 0 (grid_op runs inside
+    # them)
+    assert batch.kernels_per_substep() == 10 + 3 + 2 * (max(s.level for s in sc) - 1)
     batch.close()
     for s in alone + together:
         s.close()
