@@ -627,6 +627,9 @@ agimp_status agimp_substep(agimp_sim* s, float dt, int32_t n_steps, void* stream
 
 agimp_status agimp_refine_levels(agimp_sim* s, int32_t band, void* stream) {
   if (!s || band < 1 || band > 32) return fail(s, AGIMP_INVALID_ARG, "band must be in [1, 32]");
+  // depths are kept in bytes: the deepest threshold, band (2^(L-1) - 1), must stay below 250
+  if ((long long)band * ((1ll << (s->c.L - 1)) - 1) >= 250)
+    return fail(s, AGIMP_INVALID_ARG, "band * (2^(levels-1) - 1) must be below 250");
   CK(cudaSetDevice(s->device));
   StreamUse su(s, stream);
   wait_readback(s, s->par, su.use);  // g_p of the state being read is rewritten

@@ -511,6 +511,109 @@ __host__ __device__ __forceinline__ void polar_rot(const float* F, float* R) {
   }
 }
 
+// Fixed-corotated Kirchhoff stress (utils.py:11-16) as a symmetric matrix:
+//   tau = 2 mu (F - R) F^T + la J (J - 1) I,  R = U V^T,
+// passed as tmu = 2 mu and diag = la J (J - 1).  tau is symmetric, and its
+// entries are written in the order xx, xy, yy (2D) / xx, xy, yy, xz, yz, zz (3D).
+//
+// 3D near rotations (det F > 0, |F F^T - I|_F < 0.1, which holds in the snow
+// range, singular values within a few percent of 1): with the left polar
+// decomposition F = P R, R F^T = P = (F F^T)^(1/2), so
+//   (F - R) F^T = F F^T - (F F^T)^(1/2) = (I + E) - (I + E)^(1/2),  E = F F^T - I,
+// a power series in E: E/2 + E^2/8 - E^3/16 + 5 E^4/128 - 7 E^5/256 + ...
+// (the binomial series of the matrix square root, Higham, "Functions of
+// Matrices", SIAM 2008, ch. 6), summed by Horner's rule to the E^5 term: the
+// first omitted term, 21 E^6 / 1024, is below 2.1e-8 for |E| < 0.1.  Every
+// product is a polynomial in E (symmetric, commuting), so each needs only its
+// 6 upper entries.  Elsewhere (inverted or strongly stretched F) R comes from
+// polar_rot.  In 2D the closed-form polar rotation is cheap and used always.
+template <int D>
+__host__ __device__ __forceinline__ void kirchhoff_sym(const float* F, float tmu, float diag, float* tau) {
+  if (D == 2) {
+    float R[4];
+    polar_rot<2>(F, R);
+    float t[4];
+#pragma unroll
+    for (int r = 0; r < 2; ++r)
+#pragma unroll
+      for (int b = 0; b < 2; ++b) {
+        float acc = 0.f;
+#pragma unroll
+        for (int k = 0; k < 2; ++k) acc += (tmu * (F[r * 2 + k] - R[r * 2 + k])) * F[b * 2 + k];
+        t[r * 2 + b] = acc;
+      }
+    tau[0] = t[0] + diag;
+    tau[1] = 0.5f * (t[1] + t[2]);
+    tau[2] = t[3] + diag;
+    return;
+  }
+  // E = F F^T - I, upper entries (xx, xy, yy, xz, yz, zz)
+  float e[6];
+  e[0] = fmaf(F[0], F[0], fmaf(F[1], F[1], F[2] * F[2])) - 1.f;
+  e[1] = fmaf(F[0], F[3], fmaf(F[1], F[4], F[2] * F[5]));
+  e[2] = fmaf(F[3], F[3], fmaf(F[4], F[4], F[5] * F[5])) - 1.f;
+  e[3] = fmaf(F[0], F[6], fmaf(F[1], F[7], F[2] * F[8]));
+  e[4] = fmaf(F[3], F[6], fmaf(F[4], F[7], F[5] * F[8]));
+  e[5] = fmaf(F[6], F[6], fmaf(F[7], F[7], F[8] * F[8])) - 1.f;
+  const float fro2 = e[0] * e[0] + e[2] * e[2] + e[5] * e[5] + 2.f * (e[1] * e[1] + e[3] * e[3] + e[4] * e[4]);
+  if (fro2 < 0.01f && det<3>(F) > 0.f) {
+    // T <- c I + E T, starting from T = c4 I + c5 E
+    float t[6];
+    const float c5 = -7.f / 256.f, c4 = 5.f / 128.f, c3 = -1.f / 16.f, c2 = 1.f / 8.f, c1 = 0.5f;
+#pragma unroll
+    for (int i = 0; i < 6; ++i) t[i] = c5 * e[i];
+    t[0] += c4;
+    t[2] += c4;
+    t[5] += c4;
+    auto sym_mul = [](const float* a, const float* b, float* o) {
+      // o = a b for symmetric commuting a, b (upper entries)
+      o[0] = fmaf(a[0], b[0], fmaf(a[1], b[1], a[3] * b[3]));
+      o[1] = fmaf(a[0], b[1], fmaf(a[1], b[2], a[3] * b[4]));
+      o[2] = fmaf(a[1], b[1], fmaf(a[2], b[2], a[4] * b[4]));
+      o[3] = fmaf(a[0], b[3], fmaf(a[1], b[4], a[3] * b[5]));
+      o[4] = fmaf(a[1], b[3], fmaf(a[2], b[4], a[4] * b[5]));
+      o[5] = fmaf(a[3], b[3], fmaf(a[4], b[4], a[5] * b[5]));
+    };
+    const float cs[3] = {c3, c2, c1};
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      float o[6];
+      sym_mul(e, t, o);
+#pragma unroll
+      for (int i = 0; i < 6; ++i) t[i] = o[i];
+      t[0] += cs[k];
+      t[2] += cs[k];
+      t[5] += cs[k];
+    }
+    float x[6];
+    sym_mul(e, t, x);
+#pragma unroll
+    for (int i = 0; i < 6; ++i) tau[i] = tmu * x[i];
+  } else {
+    float R[9];
+    polar_rot<3>(F, R);
+    float t[9];
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+#pragma unroll
+      for (int b = 0; b < 3; ++b) {
+        float acc = 0.f;
+#pragma unroll
+        for (int k = 0; k < 3; ++k) acc += (tmu * (F[r * 3 + k] - R[r * 3 + k])) * F[b * 3 + k];
+        t[r * 3 + b] = acc;
+      }
+    tau[0] = t[0];
+    tau[1] = 0.5f * (t[1] + t[3]);
+    tau[2] = t[4];
+    tau[3] = 0.5f * (t[2] + t[6]);
+    tau[4] = 0.5f * (t[5] + t[7]);
+    tau[5] = t[8];
+  }
+  tau[0] += diag;
+  tau[2] += diag;
+  tau[5] += diag;
+}
+
 // True when every singular value of F provably lies in [lo, hi] and det F > 0
 // (Gershgorin discs of F^T F inside [lo^2, hi^2]): a clamp of the singular
 // values to [lo, hi] then leaves F unchanged.
@@ -562,6 +665,20 @@ __host__ __device__ __forceinline__ void axis_weights(float t, float r, float* W
   G[0] = g00;
   G[1] = g01 + g10;
   G[2] = g11;
+}
+
+// axis_weights for the reference's radius r = 0.5 (adaptive_gimp.py:48) and
+// t in [-0.5, 0.5] (every in-domain particle): none of the clamps binds, and
+// the per-axis sums reduce to W = ((1/2 - t)^2, 3/2 - 2 t^2, (1/2 + t)^2),
+// G = (t - 1/2, -2 t, t + 1/2).
+__host__ __device__ __forceinline__ void axis_weights_half(float t, float* W, float* G) {
+  const float a = 0.5f - t, b = 0.5f + t;
+  W[0] = a * a;
+  W[1] = fmaf(-2.f * t, t, 1.5f);
+  W[2] = b * b;
+  G[0] = -a;
+  G[1] = -2.f * t;
+  G[2] = b;
 }
 
 // ---------------------------------------------------------------------------

@@ -27,6 +27,9 @@ namespace {
 // 16 MiB of cell depths: finest^dim <= 16,777,216 (3D up to 256^3, 2D up to 4096^2)
 constexpr long long NOALLOC_MAX_CELLS = 16ll << 20;
 constexpr int NOALLOC_HEADER = 256;  // bounding box: int lo[3], hi[3]
+// longest line of a distance-transform pass: the finest size (2D at most
+// 4096, 3D at most 256 under the cell limit)
+constexpr int NOALLOC_MAX_LINE = 4096;
 static __device__ __align__(256) uint8_t g_noalloc_scratch[NOALLOC_HEADER + NOALLOC_MAX_CELLS];
 
 constexpr int NOALLOC_MAX_DEVICES = 64;
@@ -85,22 +88,51 @@ __device__ __forceinline__ long long na_idx(const NA& a, const int* cell) {
   return o;
 }
 
+// bounding box of the particles' finest cells: a fixed grid of CTAs, each
+// reducing its share of the particles across its warps in shared memory, then
+// one atomic per CTA and bound
 template <int D>
-__global__ void k_na_bb(NA a) {
-  const long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  int cell[D];
-  const bool ok = p < a.n && na_cell<D>(a, p, cell);
+__global__ void __launch_bounds__(256) k_na_bb(NA a) {
+  __shared__ int s_lo[8][D], s_hi[8][D];
+  int lo[D], hi[D];
 #pragma unroll
   for (int d = 0; d < D; ++d) {
-    int lo = ok ? cell[d] : INT_MAX, hi = ok ? cell[d] : -1;
+    lo[d] = INT_MAX;
+    hi[d] = -1;
+  }
+  GS_LOOP(p, a.n) {
+    int cell[D];
+    if (na_cell<D>(a, p, cell))
+#pragma unroll
+      for (int d = 0; d < D; ++d) {
+        lo[d] = min(lo[d], cell[d]);
+        hi[d] = max(hi[d], cell[d]);
+      }
+  }
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int d = 0; d < D; ++d) {
 #pragma unroll
     for (int o = 16; o; o >>= 1) {
-      lo = min(lo, __shfl_xor_sync(0xffffffffu, lo, o));
-      hi = max(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+      lo[d] = min(lo[d], __shfl_xor_sync(0xffffffffu, lo[d], o));
+      hi[d] = max(hi[d], __shfl_xor_sync(0xffffffffu, hi[d], o));
     }
-    if ((threadIdx.x & 31) == 0 && hi >= 0) {
-      atomicMin(&a.bb[d], lo);
-      atomicMax(&a.bb[3 + d], hi);
+    if (lane == 0) {
+      s_lo[warp][d] = lo[d];
+      s_hi[warp][d] = hi[d];
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x < D) {
+    const int d = threadIdx.x;
+    int mn = INT_MAX, mx = -1;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
+      mn = min(mn, s_lo[w][d]);
+      mx = max(mx, s_hi[w][d]);
+    }
+    if (mx >= 0) {
+      atomicMin(&a.bb[d], mn);
+      atomicMax(&a.bb[3 + d], mx);
     }
   }
 }
@@ -128,35 +160,50 @@ __global__ void k_na_mark(NA a) {
   if (p < a.n && na_cell<D>(a, p, cell)) a.depth[na_idx<D>(a, cell)] = 1;
 }
 
+// One pass of the separable distance transform of refine.cu along `axis`,
+// in place: a CTA takes one line of the bounding box at a time and reads it
+// into shared memory before writing it back, so the pass needs no second
+// buffer (lines are at most NOALLOC_MAX_LINE cells long).  With f_0 = 0 on
+// empty and K on occupied cells (the first pass reads occupancy 0 / 1),
+//   f_a(c) = min over x' on the line of c of max(f_{a-1}(c|x'), |x - x'|),
+// positions outside the box counting as empty, so after the last axis every
+// cell holds min(K, its Chebyshev distance to the nearest empty cell).
 template <int D>
-__global__ void k_na_erode(NA a, int k) {
+__global__ void __launch_bounds__(256) k_na_dt_line(NA a, int axis, int K, int first) {
+  __shared__ uint8_t line[NOALLOC_MAX_LINE];
   int lo[D], n[D];
   const long long vol = na_vol<D>(a, lo, n);
-  GS_LOOP(i, vol) {
-    long long t = i;
+  if (vol == 0) return;
+  const int nx = n[axis];
+  const long long nlines = vol / nx;
+  long long stride = 1;
+  for (int d = D - 1; d > axis; --d) stride *= a.sz;
+  for (long long li = blockIdx.x; li < nlines; li += gridDim.x) {
+    // the line's first cell: li runs over the other axes' box coordinates
     int cell[D];
+    long long t = li;
 #pragma unroll
     for (int d = D - 1; d >= 0; --d) {
+      if (d == axis) {
+        cell[d] = lo[d];
+        continue;
+      }
       cell[d] = lo[d] + (int)(t % n[d]);
       t /= n[d];
     }
-    uint8_t* me = &a.depth[na_idx<D>(a, cell)];
-    if (*me != k) continue;
-    bool all = true;
-#pragma unroll
-    for (int q = 0; q < ((D == 2) ? 9 : 27); ++q) {
-      int c[D];
-      int tt = q;
-      bool in = true;
-#pragma unroll
-      for (int d = D - 1; d >= 0; --d) {
-        c[d] = cell[d] + tt % 3 - 1;
-        tt /= 3;
-        in = in && c[d] >= lo[d] && c[d] < lo[d] + n[d];
-      }
-      if (!in || a.depth[na_idx<D>(a, c)] < k) all = false;
+    uint8_t* base = a.depth + na_idx<D>(a, cell);
+    for (int x = threadIdx.x; x < nx; x += blockDim.x) {
+      const int v = base[x * stride];
+      line[x] = (uint8_t)(first ? (v ? K : 0) : v);
     }
-    if (all) *me = (uint8_t)(k + 1);
+    __syncthreads();
+    for (int x = threadIdx.x; x < nx; x += blockDim.x) {
+      auto val = [&](int q) -> int { return (q < 0 || q >= nx) ? 0 : line[q]; };
+      int best = val(x);
+      for (int o = 1; o < best; ++o) best = min(best, max(min(val(x - o), val(x + o)), o));
+      base[x * stride] = (uint8_t)best;
+    }
+    __syncthreads();
   }
 }
 
@@ -180,13 +227,14 @@ template <int D>
 void na_launch(const NA& a, int sms, cudaStream_t s) {
   const int Gp = (int)((a.n + 255) / 256);
   const int G = sms * 8;
-  int kmax = a.band * ((1 << (a.L - 1)) - 1) + 1;
-  if (kmax > 250) kmax = 250;
+  // the largest depth the rule compares is band (2^(L-1) - 1); the entry
+  // point keeps it below 250, so K fits the uint8 cells
+  const int K = a.band * ((1 << (a.L - 1)) - 1) + 1;
   k_na_bb_init<<<1, 32, 0, s>>>(a);
-  k_na_bb<D><<<Gp, 256, 0, s>>>(a);
+  k_na_bb<D><<<sms * 2, 256, 0, s>>>(a);  // 256 threads: 8 warps (s_lo / s_hi)
   k_na_clear<D><<<G, 256, 0, s>>>(a);
   k_na_mark<D><<<Gp, 256, 0, s>>>(a);
-  for (int k = 1; k < kmax; ++k) k_na_erode<D><<<G, 256, 0, s>>>(a, k);
+  for (int k = 0; k < D; ++k) k_na_dt_line<D><<<G, 256, 0, s>>>(a, D - 1 - k, K, k == 0);
   k_na_assign<D><<<Gp, 256, 0, s>>>(a);
 }
 
@@ -199,6 +247,8 @@ extern "C" agimp_status agimp_refine_levels_noalloc(const float* x, int64_t n, i
   if ((dim != 2 && dim != 3) || level < 1 || level > MAXL || coarsest_size < 4 ||
       (coarsest_size & (coarsest_size - 1)) || band < 1 || band > 32 || n < 0 || (n > 0 && (!x || !g)))
     return AGIMP_INVALID_ARG;
+  // depths are kept in bytes: the deepest threshold must stay below 250
+  if ((long long)band * ((1ll << (level - 1)) - 1) >= 250) return AGIMP_INVALID_ARG;
   const long long sz = (long long)coarsest_size << (level - 1);
   long long cells = 1;
   for (int d = 0; d < dim; ++d) {

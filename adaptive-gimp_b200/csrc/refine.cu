@@ -188,8 +188,8 @@ static void run_refine(const Ctx& c, int band, cudaStream_t s) {
   if (c.N == 0) return;
   const int Gp = (c.N + 255) / 256;
   const int G = c.sms * 8;
-  int kmax = band * ((1 << (c.L - 1)) - 1) + 1;
-  if (kmax > 250) kmax = 250;
+  // agimp_refine_levels keeps band (2^(L-1) - 1) below 250: K fits the uint8 cells
+  const int kmax = band * ((1 << (c.L - 1)) - 1) + 1;
   k_bb_init<<<1, 32, 0, s>>>(c);
   k_bb<D><<<c.sms * 2, 256, 0, s>>>(c);  // 256 threads: 8 warps (s_lo / s_hi)
   k_occ_clear<D><<<G, 256, 0, s>>>(c);

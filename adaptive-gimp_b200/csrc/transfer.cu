@@ -38,23 +38,54 @@ __device__ __forceinline__ void chunk_origin(const LevelDev& V, long long blk, i
 }
 
 // ---------------------------------------------------------------------------
+// Packed f32x2 arithmetic (sm_100 fma/mul/add .f32x2): each half is rounded
+// exactly like the scalar fmaf / multiply / add, at one instruction per pair.
+__device__ __forceinline__ unsigned long long pk2(float2 a) {
+  unsigned long long r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a.x), "f"(a.y));
+  return r;
+}
+__device__ __forceinline__ float2 upk2(unsigned long long r) {
+  float2 a;
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(a.x), "=f"(a.y) : "l"(r));
+  return a;
+}
+__device__ __forceinline__ float2 ffma2(float2 a, float2 b, float2 c) {
+  unsigned long long d;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(pk2(a)), "l"(pk2(b)), "l"(pk2(c)));
+  return upk2(d);
+}
+__device__ __forceinline__ float2 fmul2(float2 a, float2 b) {
+  unsigned long long d;
+  asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(pk2(a)), "l"(pk2(b)));
+  return upk2(d);
+}
+__device__ __forceinline__ float2 fadd2(float2 a, float2 b) {
+  unsigned long long d;
+  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(pk2(a)), "l"(pk2(b)));
+  return upk2(d);
+}
+__device__ __forceinline__ float2 dup2(float a) { return make_float2(a, a); }
+
+// ---------------------------------------------------------------------------
 // P2G (adaptive_gimp.py:230-250).  Per work item (up to CH particles of one
 // 4^d block of one level, in base-cell order: bins store their particles
 // sorted by cell):
-//  1. one thread per particle computes the scaled stress (utils.py:11-16,
-//     adaptive_gimp.py:240), its per-axis GIMP weights and gradients, m,
-//     a = m (v - C (tc+1)) and B = m C, and its base cell inside the block,
-//     and stores them in shared memory at its thread index;
-//  2. each warp cuts its own 32 particles into tasks: runs of one base cell
-//     (found with ballots), at most TMAX long;
-//  3. a lane owns one row of three stencil nodes (the last axis runs along
-//     the row; 3^(d-1) rows per cell) of one task, and a warp serves SLOTS
-//     tasks at once (3 in 3D, 10 in 2D).  All particles of a task share a base
-//     cell, so the lane sums w m and w (a + B n) + S grad w of its three nodes
-//     over the task's particles in registers: one read of a particle record
-//     serves three nodes, and the row's weight products are shared; the sums
-//     go once into the (4+2)^d node tile in shared memory;
-//  4. a CTA takes a contiguous range of work items, so consecutive items of
+//  1. one thread per particle computes the scaled Kirchhoff stress S
+//     (utils.py:11-16, adaptive_gimp.py:240; symmetric, kirchhoff_sym), its
+//     per-axis GIMP weights and gradients, m, a = m (v - C (tc+1)) and
+//     B = m C, and its base cell inside the block, and stores them in shared
+//     memory at its thread index;
+//  2. each warp cuts its own 32 particles into SLOTS contiguous ranges of
+//     equal length (3 of 11/11/10 in 3D, 10 of 3-4 in 2D); a lane owns one row
+//     of three stencil nodes (the last axis runs along the row; 3^(d-1) rows
+//     per cell) of one range and walks its particles.  While the base cell
+//     stays the same it sums w m and w (a + B n) + S grad w of its three
+//     nodes in registers (one read of a particle record serves three nodes,
+//     and the row's weight products are shared); when the cell changes, and
+//     at the end, the sums go into the (4+2)^d node tile in shared memory.
+//     Equal ranges keep every slot busy for the same number of steps;
+//  3. a CTA takes a contiguous range of work items, so consecutive items of
 //     one block (a dense block holds many) keep summing into the same tile;
 //     when the next item is another block, the tile is flushed after one
 //     barrier with one float4 atomic per touched node and cleared.  Two tiles
@@ -64,45 +95,64 @@ template <int D, int CH>
 struct P2GLayout {
   static constexpr int NC = 1 << (2 * D);        // cells per block
   static constexpr int ROWS = (D == 2) ? 3 : 9;   // node rows per stencil
-  static constexpr int SLOTS = 32 / ROWS;         // tasks served by one warp at once
+  static constexpr int SLOTS = 32 / ROWS;         // particle ranges served by one warp at once
   static constexpr int TN = (D == 2) ? 36 : 216;  // nodes of the (4+2)^d tile
-  // particles per task: in 3D a run over the whole warp fills the 3 slots
-  // (11 + 11 + 10); in 2D runs are short (4 per base cell at the finest level)
-  static constexpr int TMAX = (D == 3) ? 11 : 16;
-  // per-particle record:
-  //   [0, 4)          m, a_0 .. a_{d-1}                 a = m (v - C (tc + 1))
-  //   [4, 4 + 2d^2)   B = m C (row-major), then the scaled stress S (row-major)
-  //   [OFF_WP, ..)    {W_k[n], G_k[n]} pairs, n = 0..2, for the axes k < d-1
-  //   [OFF_WL, +4)    W_{d-1}[0..2] (last axis), then [OFF_WL + 4, +4) G_{d-1}[0..2]
-  static constexpr int OFF_BS = 4;
-  static constexpr int OFF_WP = OFF_BS + ((2 * D * D + 3) & ~3);
-  static constexpr int OFF_WL = OFF_WP + ((6 * (D - 1) + 3) & ~3);
-  static constexpr int STRIDE = OFF_WL + 8;  // 3D 44, 2D 28 floats: 16-byte aligned records
-  static constexpr size_t bytes() {
-    return sizeof(float) * ((size_t)CH * STRIDE + 2 * 4 * TN) + sizeof(int) * (CH / 32) * 33;
-  }
+  // per-particle record (floats; pairs that the row sums read together sit at
+  // even offsets):
+  //  3D  0 a_x a_y a_z m | 4 Bx0 By0 Bx1 By1 | 8 Bx2 By2 Bz0 Bz1 | 12 Sxx Sxy Sxy Syy |
+  //     16 Sxz Syz Szz Bz2 | 20 (W0 G0)[0] (W0 G0)[1] | 24 (W0 G0)[2] (W1 G1)[0] |
+  //     28 (W1 G1)[1] (W1 G1)[2] | 32 W2[0..2] cell | 36 G2[0..2] -
+  //  2D  0 a_x a_y m cell | 4 Bx0 By0 Bx1 By1 | 8 Sxx Sxy Sxy Syy |
+  //     12 (W0 G0)[0] (W0 G0)[1] | 16 (W0 G0)[2] - - | 20 W1[0..2] - | 24 G1[0..2] -
+  static constexpr int STRIDE = (D == 3) ? 40 : 28;  // 16-byte aligned records
+  static constexpr int OFF_WP = (D == 3) ? 20 : 12;  // (W, G) pairs of the axes before the last
+  static constexpr int OFF_WL = (D == 3) ? 32 : 20;  // last axis: W[0..2], then G[0..2] at +4
+  static constexpr int OFF_CELL = (D == 3) ? 35 : 3;
+  static constexpr size_t bytes() { return sizeof(float) * ((size_t)CH * STRIDE + 2 * 4 * TN); }
 };
+
+// A lane's three node sums of one base cell into the node tile ([4][TN]:
+// p_x, p_y, p_z, m).
+template <int D>
+__device__ __forceinline__ void p2g_row_flush(float* tile, int TN, int cc, int n0, int n1, const float2* axy,
+                                              const float* az, const float* am) {
+  int ti;
+  if (D == 2)
+    ti = (((cc >> 2) & 3) + n0) * 6 + (cc & 3);
+  else
+    ti = ((((cc >> 4) & 3) + n0) * 6 + ((cc >> 2) & 3) + n1) * 6 + (cc & 3);
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    atomicAdd(&tile[ti + k], axy[k].x);
+    atomicAdd(&tile[TN + ti + k], axy[k].y);
+    if (D == 3) atomicAdd(&tile[2 * TN + ti + k], az[k]);
+    atomicAdd(&tile[3 * TN + ti + k], am[k]);
+  }
+}
 
 template <int D, int CH>
 __global__ void __launch_bounds__(CH, 1024 / CH) k_p2g(Batch B) {
   SCENE_CTA(B, MAP_G);
   using Y = P2GLayout<D, CH>;
-  extern __shared__ float dsm[];
-  float* pd = dsm;                      // [CH][STRIDE]
+  extern __shared__ float4 dsm4[];
+  float* pd = (float*)dsm4;             // [CH][STRIDE]
   float* tiles = pd + CH * Y::STRIDE;   // [2][4][TN]: p_x, p_y, p_z, m
-  int* starts = (int*)(tiles + 2 * 4 * Y::TN);  // [warps][33]: each warp's task starts
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int nch = c.ctr[CTR_CHUNKS];
   const float pw = (D == 2) ? 0.25f : 0.125f;                                        // 0.5**dim
   const float rd = (D == 2) ? c.radius * c.radius : c.radius * c.radius * c.radius;  // radius**dim
   const float r2 = 2.f * c.radius;
   const float kw = (D == 2) ? 1.f / (4.f * r2 * r2) : 1.f / (8.f * r2 * r2 * r2);
+  const bool half = c.radius == 0.5f;
   // the tiles start at zero; each flush leaves its tile at zero again
   for (int i = threadIdx.x; i < 2 * 4 * Y::TN; i += blockDim.x) tiles[i] = 0.f;
   __syncthreads();
   int tb = 0;
   const int per = (nch + nblk_ - 1) / nblk_;
   const int c0 = bid_ * per, c1 = min(nch, c0 + per);
+  // this lane's slot and node row
+  const int q = lane / Y::ROWS, row = lane % Y::ROWS;
+  const int n0 = (D == 2) ? row : row / 3, n1 = (D == 2) ? 0 : row % 3;
   for (int ch = c0; ch < c1; ++ch) {
     const int4 wd = c.chunks[ch];
     const int l = wd.x;
@@ -117,9 +167,8 @@ __global__ void __launch_bounds__(CH, 1024 / CH) k_p2g(Batch B) {
     int O[D];
     chunk_origin<D>(V, wd.y, O);
     float* tile = tiles + tb * 4 * Y::TN;
-    // -- 1. per-particle quantities ------------------------------------------
+    // -- 1. per-particle records -----------------------------------------------
     const int i = threadIdx.x;
-    int cell = -1;
     if (i < wd.w) {
       const int p = __ldg(&c.perm[wd.z + i]);
       const long long N = c.N;
@@ -139,7 +188,7 @@ __global__ void __launch_bounds__(CH, 1024 / CH) k_p2g(Batch B) {
       const float mp = __ldg(&c.P.m[p]);
       const float jp = c.plast == 1 ? __ldg(&c.P.Jp[p]) : 1.f;
       float tc[D];
-      cell = 0;
+      int cell = 0;
 #pragma unroll
       for (int d = 0; d < D; ++d) {
         const float xs = xp[d] * inv;
@@ -153,13 +202,10 @@ __global__ void __launch_bounds__(CH, 1024 / CH) k_p2g(Batch B) {
         mu *= h;
         la *= h;
       }
-      float Rm[D * D];
-      polar_rot<D>(F, Rm);
       const float J = det<D>(F);
-      const float tmu = 2.f * mu;
-      const float diag = la * J * (J - 1.f);
+      float tau[(D == 2) ? 3 : 6];
+      kirchhoff_sym<D>(F, 2.f * mu, la * J * (J - 1.f), tau);
       const float sc = (-c.dt * pw) / (rd * dx);
-      float* P = pd + i * Y::STRIDE;
       float a[D];
 #pragma unroll
       for (int r = 0; r < D; ++r) {
@@ -168,144 +214,142 @@ __global__ void __launch_bounds__(CH, 1024 / CH) k_p2g(Batch B) {
         for (int b = 0; b < D; ++b) cd += Cm[r * D + b] * (tc[b] + 1.f);
         a[r] = mp * (vp[r] - cd);
       }
-      *(float4*)P = make_float4(mp, a[0], a[1], D == 3 ? a[D - 1] : 0.f);
-#pragma unroll
-      for (int r = 0; r < D; ++r)
-#pragma unroll
-        for (int b = 0; b < D; ++b) {
-          float acc = 0.f;
-#pragma unroll
-          for (int k = 0; k < D; ++k) acc += (tmu * (F[r * D + k] - Rm[r * D + k])) * F[b * D + k];
-          P[Y::OFF_BS + r * D + b] = mp * Cm[r * D + b];
-          P[Y::OFF_BS + D * D + r * D + b] = sc * (acc + (r == b ? diag : 0.f));
-        }
       // axis factors, scaled so that a node's weight is the product of its
       // W's and the gradient's factors need no constant: axis 0 carries kw,
       // every G carries kg / kw = 2
+      float W[D][3], G[D][3];
 #pragma unroll
       for (int d = 0; d < D; ++d) {
-        float W[3], G[3];
-        axis_weights(tc[d], c.radius, W, G);
+        if (half)
+          axis_weights_half(tc[d], W[d], G[d]);
+        else
+          axis_weights(tc[d], c.radius, W[d], G[d]);
         const float sw = d == 0 ? kw : 1.f;
 #pragma unroll
         for (int k = 0; k < 3; ++k) {
-          W[k] *= sw;
-          G[k] *= 2.f * sw;
+          W[d][k] *= sw;
+          G[d][k] *= 2.f * sw;
         }
-        if (d < D - 1) {
-#pragma unroll
-          for (int k = 0; k < 3; ++k) *(float2*)(P + Y::OFF_WP + 6 * d + 2 * k) = make_float2(W[k], G[k]);
-        } else {
-          *(float4*)(P + Y::OFF_WL) = make_float4(W[0], W[1], W[2], 0.f);
-          *(float4*)(P + Y::OFF_WL + 4) = make_float4(G[0], G[1], G[2], 0.f);
-        }
+      }
+      float4* P4 = (float4*)(pd + i * Y::STRIDE);
+      const float cf = __int_as_float(cell);
+      if (D == 3) {
+        P4[0] = make_float4(a[0], a[1], a[D - 1], mp);
+        P4[1] = make_float4(mp * Cm[0], mp * Cm[D], mp * Cm[1], mp * Cm[D + 1]);
+        P4[2] = make_float4(mp * Cm[2 % (D * D)], mp * Cm[(D + 2) % (D * D)], mp * Cm[(2 * D) % (D * D)],
+                            mp * Cm[(2 * D + 1) % (D * D)]);
+        P4[3] = make_float4(sc * tau[0], sc * tau[1], sc * tau[1], sc * tau[2]);
+        P4[4] = make_float4(sc * tau[3 % (D == 3 ? 6 : 3)], sc * tau[4 % (D == 3 ? 6 : 3)],
+                            sc * tau[5 % (D == 3 ? 6 : 3)], mp * Cm[(D * D - 1)]);
+        P4[5] = make_float4(W[0][0], G[0][0], W[0][1], G[0][1]);
+        P4[6] = make_float4(W[0][2], G[0][2], W[1][0], G[1][0]);
+        P4[7] = make_float4(W[1][1], G[1][1], W[1][2], G[1][2]);
+        P4[8] = make_float4(W[D - 1][0], W[D - 1][1], W[D - 1][2], cf);
+        P4[9] = make_float4(G[D - 1][0], G[D - 1][1], G[D - 1][2], 0.f);
+      } else {
+        P4[0] = make_float4(a[0], a[1], mp, cf);
+        P4[1] = make_float4(mp * Cm[0], mp * Cm[D], mp * Cm[1], mp * Cm[D + 1 < D * D ? D + 1 : 0]);
+        P4[2] = make_float4(sc * tau[0], sc * tau[1], sc * tau[1], sc * tau[2]);
+        P4[3] = make_float4(W[0][0], G[0][0], W[0][1], G[0][1]);
+        P4[4] = make_float4(W[0][2], G[0][2], 0.f, 0.f);
+        P4[5] = make_float4(W[D - 1][0], W[D - 1][1], W[D - 1][2], 0.f);
+        P4[6] = make_float4(G[D - 1][0], G[D - 1][1], G[D - 1][2], 0.f);
       }
     }
     __syncwarp();
-    // -- 2. this warp's tasks: runs of one base cell, at most TMAX long ---------
+    // -- 2. this warp's particles: SLOTS equal ranges, lane <-> node row ---------
     const int wbase = warp * 32;
     const int nvalid = max(0, min(32, wd.w - wbase));
-    const bool valid = lane < nvalid;
-    const int prev = __shfl_up_sync(0xffffffffu, cell, 1);
-    const unsigned runs = __ballot_sync(0xffffffffu, valid && (lane == 0 || cell != prev));
-    const int rs = valid ? 31 - __clz(runs & ((2u << lane) - 1u)) : 0;  // start of this lane's run
-    const bool tstart = valid && (lane - rs) % Y::TMAX == 0;
-    const unsigned tmask = __ballot_sync(0xffffffffu, tstart);
-    const int ntask = __popc(tmask);
-    int* ws = starts + warp * 33;  // task k starts at ws[k]; ws[ntask] = nvalid
-    if (tstart) ws[__popc(tmask & ((1u << lane) - 1u))] = lane;
-    if (lane == 0) ws[ntask] = nvalid;
-    __syncwarp();
-    // -- 3. tasks: lane <-> row of three nodes ---------------------------------
-    {
-      const int q = lane / Y::ROWS, row = lane % Y::ROWS;
-      const int n0 = (D == 2) ? row : row / 3, n1 = (D == 2) ? 0 : row % 3;
-      for (int t0 = 0; t0 < ntask; t0 += Y::SLOTS) {
-        const int t = t0 + q;
-        const bool on = q < Y::SLOTS && t < ntask;
-        const int s0 = on ? ws[t] : 0;
-        const int e = on ? ws[t + 1] : 0;
-        const int cc = __shfl_sync(0xffffffffu, cell, s0);
-        if (!on) continue;
-        const int len = e - s0;
-        float am[3], ap[3][D];
+    if (q < Y::SLOTS) {
+      const int j0 = (q * nvalid) / Y::SLOTS, j1 = ((q + 1) * nvalid) / Y::SLOTS;
+      const float2 nn0 = dup2((float)n0), nn1 = dup2((float)n1);
+      float2 axy[3];
+      float az[3], am[3];
 #pragma unroll
-        for (int k = 0; k < 3; ++k) {
-          am[k] = 0.f;
-#pragma unroll
-          for (int d = 0; d < D; ++d) ap[k][d] = 0.f;
-        }
+      for (int k = 0; k < 3; ++k) {
+        axy[k] = make_float2(0.f, 0.f);
+        az[k] = am[k] = 0.f;
+      }
+      int cur = -1;
 #pragma unroll 2
-        for (int j = 0; j < len; ++j) {
-          const float* R = pd + (wbase + s0 + j) * Y::STRIDE;
-          const float4 ma = *(const float4*)R;
-          float bs[2 * D * D];
+      for (int j = j0; j < j1; ++j) {
+        const float* R = pd + (wbase + j) * Y::STRIDE;
+        const float4 q0 = *(const float4*)R;
+        const int cc = __float_as_int(R[Y::OFF_CELL]);
+        if (cc != cur) {
+          if (cur >= 0) p2g_row_flush<D>(tile, Y::TN, cur, n0, n1, axy, az, am);
 #pragma unroll
-          for (int k = 0; k < (2 * D * D + 3) / 4; ++k) {
-            const float4 v = *(const float4*)(R + Y::OFF_BS + 4 * k);
-            if (4 * k + 0 < 2 * D * D) bs[4 * k + 0] = v.x;
-            if (4 * k + 1 < 2 * D * D) bs[4 * k + 1] = v.y;
-            if (4 * k + 2 < 2 * D * D) bs[4 * k + 2] = v.z;
-            if (4 * k + 3 < 2 * D * D) bs[4 * k + 3] = v.w;
+          for (int k = 0; k < 3; ++k) {
+            axy[k] = make_float2(0.f, 0.f);
+            az[k] = am[k] = 0.f;
           }
-          const float* Bm = bs;
-          const float* Sm = bs + D * D;
-          const float4 wl = *(const float4*)(R + Y::OFF_WL);
-          const float4 gl = *(const float4*)(R + Y::OFF_WL + 4);
-          const float wL[3] = {wl.x, wl.y, wl.z}, gL[3] = {gl.x, gl.y, gl.z};
-          // Node k of the row has weight cw wL[k] and gradient
-          // (cg_0 wL[k], .., cg_{d-2} wL[k], cw gL[k]); its momentum term is
-          //   w (a + B n) + S grad w = wL[k] (A + k Bk) + gL[k] s_L
-          // with A = cw (a + B n_row) + sum_{b<d-1} S[:, b] cg_b, Bk = cw B[:, d-1]
-          // and s_L = cw S[:, d-1].
-          float cw, cg[D - 1];
-          const float av[3] = {ma.y, ma.z, ma.w};
-          float A[D];
-          if (D == 2) {
-            const float2 wg0 = *(const float2*)(R + Y::OFF_WP + 2 * n0);
-            cw = wg0.x;
-            cg[0] = wg0.y;
+          cur = cc;
+        }
+        const float4 wl = *(const float4*)(R + Y::OFF_WL);
+        const float4 gl = *(const float4*)(R + Y::OFF_WL + 4);
+        const float wL[3] = {wl.x, wl.y, wl.z}, gL[3] = {gl.x, gl.y, gl.z};
+        // Node k of the row has weight cw wL[k] and gradient
+        // (cg_0 wL[k], .., cg_{d-2} wL[k], cw gL[k]); its momentum term is
+        //   w (a + B n) + S grad w = wL[k] (A + k Bk) + gL[k] s_L
+        // with A = cw (a + B n_row) + sum_{b<d-1} S[:, b] cg_b, Bk = cw B[:, d-1]
+        // and s_L = cw S[:, d-1]; the mass term is wL[k] cw m.
+        if (D == 3) {
+          const float4 b1 = *(const float4*)(R + 4);   // Bx0 By0 Bx1 By1
+          const float4 b2 = *(const float4*)(R + 8);   // Bx2 By2 Bz0 Bz1
+          const float4 s1 = *(const float4*)(R + 12);  // Sxx Sxy Sxy Syy
+          const float4 s2 = *(const float4*)(R + 16);  // Sxz Syz Szz Bz2
+          const float2 wg0 = *(const float2*)(R + Y::OFF_WP + 2 * n0);
+          const float2 wg1 = *(const float2*)(R + Y::OFF_WP + 6 + 2 * n1);
+          const float cw = wg0.x * wg1.x, cg0 = wg0.y * wg1.x, cg1 = wg0.x * wg1.y;
+          const float2 cw2 = dup2(cw);
+          // x, y channels as pairs
+          const float2 uxy = ffma2(make_float2(b1.z, b1.w), nn1, ffma2(make_float2(b1.x, b1.y), nn0,
+                                                                       make_float2(q0.x, q0.y)));
+          const float2 Axy = ffma2(cw2, uxy, ffma2(make_float2(s1.x, s1.y), dup2(cg0),
+                                                   fmul2(make_float2(s1.z, s1.w), dup2(cg1))));
+          const float2 bkxy = fmul2(cw2, make_float2(b2.x, b2.y));
+          const float2 slxy = fmul2(cw2, make_float2(s2.x, s2.y));
+          const float2 A1xy = fadd2(Axy, bkxy), A2xy = ffma2(dup2(2.f), bkxy, Axy);
+          axy[0] = ffma2(dup2(gL[0]), slxy, ffma2(dup2(wL[0]), Axy, axy[0]));
+          axy[1] = ffma2(dup2(gL[1]), slxy, ffma2(dup2(wL[1]), A1xy, axy[1]));
+          axy[2] = ffma2(dup2(gL[2]), slxy, ffma2(dup2(wL[2]), A2xy, axy[2]));
+          // z channel (S symmetric: S[z][0] = Sxz, S[z][1] = Syz) and mass
+          const float uz = fmaf(b2.w, (float)n1, fmaf(b2.z, (float)n0, q0.z));
+          const float Az = fmaf(cw, uz, fmaf(s2.x, cg0, s2.y * cg1));
+          const float bkz = cw * s2.w, slz = cw * s2.z;
+          az[0] = fmaf(gL[0], slz, fmaf(wL[0], Az, az[0]));
+          az[1] = fmaf(gL[1], slz, fmaf(wL[1], Az + bkz, az[1]));
+          az[2] = fmaf(gL[2], slz, fmaf(wL[2], fmaf(2.f, bkz, Az), az[2]));
+          const float cm = cw * q0.w;
 #pragma unroll
-            for (int r = 0; r < D; ++r) A[r] = fmaf(cw, fmaf(Bm[r * D], (float)n0, av[r]), Sm[r * D] * cg[0]);
-          } else {
-            const float2 wg0 = *(const float2*)(R + Y::OFF_WP + 2 * n0);
-            const float2 wg1 = *(const float2*)(R + Y::OFF_WP + 6 + 2 * n1);
-            cw = wg0.x * wg1.x;
-            cg[0] = wg0.y * wg1.x;
-            cg[D - 2] = wg0.x * wg1.y;
-#pragma unroll
-            for (int r = 0; r < D; ++r) {
-              const float u = fmaf(Bm[r * D + 1], (float)n1, fmaf(Bm[r * D], (float)n0, av[r]));
-              A[r] = fmaf(cw, u, fmaf(Sm[r * D], cg[0], Sm[r * D + 1] * cg[D - 2]));
-            }
-          }
-          const float cm = cw * ma.x;
-#pragma unroll
-          for (int r = 0; r < D; ++r) {
-            const float bk = cw * Bm[r * D + D - 1], sl = cw * Sm[r * D + D - 1];
-            ap[0][r] = fmaf(gL[0], sl, fmaf(wL[0], A[r], ap[0][r]));
-            ap[1][r] = fmaf(gL[1], sl, fmaf(wL[1], A[r] + bk, ap[1][r]));
-            ap[2][r] = fmaf(gL[2], sl, fmaf(wL[2], fmaf(2.f, bk, A[r]), ap[2][r]));
-          }
+          for (int k = 0; k < 3; ++k) am[k] = fmaf(wL[k], cm, am[k]);
+        } else {
+          const float4 b1 = *(const float4*)(R + 4);  // Bx0 By0 Bx1 By1
+          const float4 s1 = *(const float4*)(R + 8);  // Sxx Sxy Sxy Syy
+          const float2 wg0 = *(const float2*)(R + Y::OFF_WP + 2 * n0);
+          const float cw = wg0.x, cg0 = wg0.y;
+          const float2 cw2 = dup2(cw);
+          const float2 uxy = ffma2(make_float2(b1.x, b1.y), nn0, make_float2(q0.x, q0.y));
+          const float2 Axy = ffma2(cw2, uxy, fmul2(make_float2(s1.x, s1.y), dup2(cg0)));
+          const float2 bkxy = fmul2(cw2, make_float2(b1.z, b1.w));
+          const float2 slxy = fmul2(cw2, make_float2(s1.z, s1.w));
+          const float2 A1xy = fadd2(Axy, bkxy), A2xy = ffma2(dup2(2.f), bkxy, Axy);
+          axy[0] = ffma2(dup2(gL[0]), slxy, ffma2(dup2(wL[0]), Axy, axy[0]));
+          axy[1] = ffma2(dup2(gL[1]), slxy, ffma2(dup2(wL[1]), A1xy, axy[1]));
+          axy[2] = ffma2(dup2(gL[2]), slxy, ffma2(dup2(wL[2]), A2xy, axy[2]));
+          const float cm = cw * q0.z;
 #pragma unroll
           for (int k = 0; k < 3; ++k) am[k] = fmaf(wL[k], cm, am[k]);
         }
-        int ti = 0;
-#pragma unroll
-        for (int d = 0; d < D - 1; ++d) ti = ti * 6 + ((cc >> (2 * (D - 1 - d))) & 3) + (d == 0 ? n0 : n1);
-        ti = ti * 6 + (cc & 3);
-#pragma unroll
-        for (int k = 0; k < 3; ++k) {
-          if (am[k] != 0.f) atomicAdd(&tile[3 * Y::TN + ti + k], am[k]);
-#pragma unroll
-          for (int d = 0; d < D; ++d)
-            if (ap[k][d] != 0.f) atomicAdd(&tile[d * Y::TN + ti + k], ap[k][d]);
-        }
       }
+      if (cur >= 0) p2g_row_flush<D>(tile, Y::TN, cur, n0, n1, axy, az, am);
     }
+    // the next work item's step 1 overwrites this warp's records, which lanes
+    // of this warp may still be reading above
+    __syncwarp();
     if (!last) continue;  // the same block follows: keep summing into this tile
     __syncthreads();
-    // -- 4. flush and clear ---------------------------------------------------
+    // -- 3. flush and clear ---------------------------------------------------
     for (int t = threadIdx.x; t < Y::TN; t += blockDim.x) {
       const float4 val = make_float4(tile[t], tile[Y::TN + t], D == 3 ? tile[2 * Y::TN + t] : 0.f, tile[3 * Y::TN + t]);
       if (val.x == 0.f && val.y == 0.f && val.z == 0.f && val.w == 0.f) continue;

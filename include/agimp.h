@@ -161,7 +161,9 @@ agimp_status agimp_set_graphs(agimp_sim* s, int32_t enable);
  * init.py:17-29 / run_3d.py:151-156): recompute g_p from the current positions.
  * A particle whose finest cell is within `band` finest cells (Chebyshev) of an
  * empty finest cell gets the finest level, within band*3 the next coarser,
- * band*7 the next, ..., deeper particles level 0. */
+ * band*7 the next, ..., deeper particles level 0.  Depths are kept in bytes:
+ * band * (2^(levels-1) - 1) must be below 250 (band in [1, 32]), else
+ * AGIMP_INVALID_ARG. */
 agimp_status agimp_refine_levels(agimp_sim* s, int32_t band, void* stream);
 
 /* Readback of cell_mask[l], ad_grid_m[l], ad_grid_v[l] (adaptive_gimp.py:35-42)
@@ -199,7 +201,8 @@ agimp_status agimp_profile_substep(agimp_sim* s, float dt, float* ms, int32_t n,
  * and its scratch is a static 16 MiB device array inside libagimp.so, held by
  * every GPU that loads the library until exit, which limits it to
  * finest^dim <= 16,777,216 cells (3D 256^3, 2D 4096^2); larger grids return
- * AGIMP_CAPACITY.  The first call on a device looks up the array's device
+ * AGIMP_CAPACITY.  band and level obey agimp_refine_levels' limit
+ * (band * (2^(level-1) - 1) below 250).  The first call on a device looks up the array's device
  * address with that device current; make that first call before any stream
  * capture.  All calls share the array: calls that overlap on the GPU race.
  * Asynchronous on `stream`. */

@@ -22,6 +22,29 @@ void h_svd(int dim, const float* A, float* U, float* S, float* V, int n) {
   }
 }
 void h_axis_weights(float t, float r, float* W, float* G) { axis_weights(t, r, W, G); }
+void h_axis_weights_half(float t, float* W, float* G) { axis_weights_half(t, W, G); }
+// symmetric Kirchhoff stress expanded to full dim x dim matrices
+void h_kirchhoff(int dim, const float* F, float mu, float la, float* tau, int n) {
+  for (int i = 0; i < n; ++i) {
+    if (dim == 2) {
+      const float* f = F + 4 * i;
+      const float J = det<2>(f);
+      float t[3];
+      kirchhoff_sym<2>(f, 2.f * mu, la * J * (J - 1.f), t);
+      float* o = tau + 4 * i;
+      o[0] = t[0]; o[1] = t[1]; o[2] = t[1]; o[3] = t[2];
+    } else {
+      const float* f = F + 9 * i;
+      const float J = det<3>(f);
+      float t[6];
+      kirchhoff_sym<3>(f, 2.f * mu, la * J * (J - 1.f), t);
+      float* o = tau + 9 * i;
+      o[0] = t[0]; o[1] = t[1]; o[2] = t[3];
+      o[3] = t[1]; o[4] = t[2]; o[5] = t[4];
+      o[6] = t[3]; o[7] = t[4]; o[8] = t[5];
+    }
+  }
+}
 void h_within(int dim, const float* F, float lo, float hi, int* out, int n) {
   for (int i = 0; i < n; ++i)
     out[i] = dim == 2 ? singular_values_within<2>(F + 4 * i, lo, hi) : singular_values_within<3>(F + 9 * i, lo, hi);

@@ -1,11 +1,12 @@
 """Generate golden vectors by running the reference's own source.
 
 Runs the reference project's adaptive_gimp.py, utils.py and init.py (read from
-a checkout of g1n0st/adaptive-gimp, default /root/reference) under the
+a checkout of g1n0st/adaptive-gimp given by --ref or the AGIMP_REFERENCE
+environment variable) under the
 Taichi-semantics shim in tests/golden/taichi_shim, on small seeded scenes, and
 writes one compressed .npz per scene into tests/golden/.
 
-    python tests/golden/make_golden.py [--ref PATH] [--only NAME]
+    python tests/golden/make_golden.py --ref PATH [--only NAME]
 
 The fixtures hold the inputs (particle state, prescribed levels, the level
 map tabulated from the reference's grid_initializer), and after every substep
@@ -180,6 +181,19 @@ def _dyn3(ti, ag, init):
     return dict(dim=3, level=3, coarsest=8, x=x, v=v, g=g, mask=None, dt=1e-4, steps=2)
 
 
+@scene("dynamic3d_large")
+def _dyn3_large(ti, ag, init):
+    # a few thousand particles on a 3-level octree (16^3 .. 64^3): a wide block
+    # whose core is prescribed the coarsest level (several coarse cells
+    # across, so some survive the culling), hit by a smaller falling block
+    rng = np.random.default_rng(13)
+    x, v, u = scene_boxes(rng, 3000, [((0.18, 0.08, 0.18), (0.82, 0.6, 0.82)), ((0.35, 0.66, 0.35), (0.6, 0.9, 0.6))],
+                          [(0.0, 2.0, 0.0), (1.0, -8.0, 0.5)])
+    v = v + (rng.standard_normal(v.shape) * 1.0).astype(np.float32)
+    g = band_levels(u, [0.22, 0.08])
+    return dict(dim=3, level=3, coarsest=16, x=x, v=v, g=g, mask=None, dt=5e-5, steps=3)
+
+
 def run_scene(ti, ag, init, name, spec, out_dir):
     dim, L, c = spec["dim"], spec["level"], spec["coarsest"]
     x, v, g = spec["x"], spec["v"], spec["g"]
@@ -215,10 +229,13 @@ def run_scene(ti, ag, init, name, spec, out_dir):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", default=os.environ.get("AGIMP_REFERENCE"),
+                    help="checkout of the reference (default: $AGIMP_REFERENCE)")
     ap.add_argument("--only", default=None)
     ap.add_argument("--out", default=HERE)
     a = ap.parse_args()
+    if not a.ref:
+        ap.error("give the reference checkout with --ref or AGIMP_REFERENCE")
     ti, ag, init = load_reference(a.ref)
     for name, fn in SCENES.items():
         if a.only and name != a.only:

@@ -116,6 +116,38 @@ def test_axis_weights_reproduce_reference_stencil(h):
             np.testing.assert_allclose(g, ref[k, 1:], atol=1e-6)
 
 
+def test_axis_weights_half_match_general_form(h):
+    """The closed form for radius 1/2 equals the clamped general form on
+    t in [-0.5, 0.5] (to rounding)."""
+    for t in np.linspace(-0.5, 0.5, 1001):
+        W, G, Wh, Gh = (np.zeros(3, np.float32) for _ in range(4))
+        h.h_axis_weights(ctypes.c_float(t), ctypes.c_float(0.5), f32p(W), f32p(G))
+        h.h_axis_weights_half(ctypes.c_float(t), f32p(Wh), f32p(Gh))
+        np.testing.assert_allclose(Wh, W, atol=4e-7)
+        np.testing.assert_allclose(Gh, G, atol=4e-7)
+
+
+@pytest.mark.parametrize("dim,spread", [(2, 0.3), (3, 0.004), (3, 0.02), (3, 0.05), (3, 0.3)])
+def test_kirchhoff_stress_matches_oracle(h, dim, spread):
+    """The P2G stress (series path near rotations, polar path elsewhere,
+    inverted F included) against the oracle's SVD-based get_stress
+    (utils.py:11-16) in f64, relative to the deviatoric part's size."""
+    rng = np.random.default_rng(7)
+    F = rand_F(rng, 1500, dim, spread)
+    mu, la = 1000.0, 600.0
+    tau = np.zeros_like(F)
+    h.h_kirchhoff(dim, f32p(F), ctypes.c_float(mu), ctypes.c_float(la), f32p(tau), len(F))
+    worst = 0.0
+    for f, t in zip(F, tau):
+        U, S, V = O.svd(f)
+        if abs(S[-1]) < 1e-3 * abs(S[0]):
+            continue  # rotation ill-defined
+        ref = O.stress(f.astype(np.float64), mu, la, f64=True)
+        scale = 2 * mu * np.abs(f - U @ V.T).max() * np.abs(f).max() + la * abs(np.linalg.det(f)) + 1e-3 * mu
+        worst = max(worst, np.abs(t - ref).max() / scale)
+    assert worst < 2e-5, worst
+
+
 @pytest.mark.parametrize("dim", [2, 3])
 def test_snow_skip_is_sound(h, dim):
     """Whenever the skip test passes, every singular value is inside the clamp
