@@ -18,16 +18,17 @@ ERR_OOB = 1
 ERR_ESCAPED = 2
 ERR_MAP_OOB = 4
 ERR_NOBIN = 8
+ERR_WAIT = 16
 
 # every symbol include/agimp.h declares
 EXPORTS = (
     "agimp_abi_version", "agimp_status_string", "agimp_default_params", "agimp_create", "agimp_destroy",
     "agimp_last_error", "agimp_set_particles", "agimp_get_particles", "agimp_set_level_map",
-    "agimp_clear_level_map", "agimp_substep", "agimp_set_graphs", "agimp_refine_levels", "agimp_get_grid",
+    "agimp_clear_level_map", "agimp_get_bins", "agimp_substep", "agimp_set_graphs", "agimp_refine_levels", "agimp_get_grid",
     "agimp_get_node_mask", "agimp_errors", "agimp_get_stats", "agimp_kernels_per_substep",
     "agimp_profile_substep", "agimp_refine_levels_noalloc",
     "agimp_mlp_num_params", "agimp_mlp_create", "agimp_mlp_destroy", "agimp_mlp_set_params", "agimp_mlp_get_params",
-    "agimp_mlp_forward", "agimp_mlp_errors", "agimp_mlp_grad", "agimp_mlp_train_step", "agimp_mlp_reset_optimizer",
+    "agimp_mlp_forward", "agimp_mlp_errors", "agimp_wait_selftest", "agimp_mlp_grad", "agimp_mlp_train_step", "agimp_mlp_reset_optimizer",
     "agimp_set_surrogate", "agimp_set_recorder", "agimp_recorded",
     "agimp_set_tuning", "agimp_get_tuning", "agimp_autotune",
     "agimp_batch_create", "agimp_batch_destroy", "agimp_batch_last_error", "agimp_batch_substep",
@@ -127,6 +128,7 @@ def load(path: str | None = None):
     L.agimp_get_node_mask.argtypes = [vp, vp, ctypes.c_int32, vp]
     L.agimp_errors.argtypes = [vp, ctypes.POINTER(ctypes.c_uint32), ctypes.c_int32]
     L.agimp_get_stats.argtypes = [vp, ctypes.POINTER(Stats)]
+    L.agimp_get_bins.argtypes = [vp, vp, ctypes.c_int32, vp]
     L.agimp_kernels_per_substep.argtypes = [vp]
     L.agimp_kernels_per_substep.restype = ctypes.c_int32
     L.agimp_profile_substep.argtypes = [vp, ctypes.c_float, fp, ctypes.c_int32, vp]
@@ -139,6 +141,7 @@ def load(path: str | None = None):
     L.agimp_mlp_get_params.argtypes = [vp, vp, ctypes.c_int32, vp]
     L.agimp_mlp_forward.argtypes = [vp, vp, vp, ctypes.c_int64, vp]
     L.agimp_mlp_errors.argtypes = [vp, ctypes.POINTER(ctypes.c_uint32), ctypes.c_int32]
+    L.agimp_wait_selftest.argtypes = [ctypes.c_int32, ctypes.c_int32, ctypes.c_uint32, ctypes.POINTER(ctypes.c_uint32)]
     L.agimp_mlp_grad.argtypes = [vp, vp, vp, ctypes.c_int64, vp, vp, vp]
     L.agimp_mlp_train_step.argtypes = [vp, vp, vp, ctypes.c_int64, ctypes.c_float, vp, vp]
     L.agimp_mlp_reset_optimizer.argtypes = [vp]

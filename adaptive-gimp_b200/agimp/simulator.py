@@ -384,6 +384,15 @@ class AdaptiveGIMP:
         _capi.check(self._L.agimp_errors(self._h, ctypes.byref(bits), 1 if clear else 0), self._h, "errors")
         return bits.value
 
+    def bin_keys(self):
+        """The bins of the last substep, one uint64 key per particle (the
+        reference's pid[l] lists, adaptive_gimp.py:208-216): level in bits
+        60-63, floor(base / 4) + 1 per axis in 20-bit fields (first axis
+        highest), all ones for particles without a level."""
+        out = np.zeros(self.n_particles, np.uint64)
+        _capi.check(self._L.agimp_get_bins(self._h, _ptr(out), AGIMP_MEM_HOST, None), self._h, "get bins")
+        return out
+
     def stats(self):
         st = _capi.Stats()
         _capi.check(self._L.agimp_get_stats(self._h, ctypes.byref(st)), self._h, "stats")

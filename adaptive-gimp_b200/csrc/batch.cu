@@ -221,6 +221,7 @@ agimp_status batch_step(agimp_batch* b, float dt, int n, cudaStream_t use, cudaE
     for (agimp_sim* s : b->sims) {
       s->par ^= 1;  // the new state is in the other buffer
       s->substeps += 1;
+      s->bins_valid = true;
     }
     b->steps += 1;
   }
@@ -397,6 +398,7 @@ agimp_status batch_autotune(agimp_batch* b, float dt, int trials, agimp_tuning* 
       agimp_sim* s = v.s;
       s->par = v.par;
       s->substeps = v.substeps;
+      s->bins_valid = false;  // the restored state was not binned by the last substep
       size_t o = 0;
       for_each_array(s, s->buf[v.par], [&](void* p, size_t nb) {
         cudaMemcpyAsync(p, v.data + o, nb, cudaMemcpyDeviceToDevice, use);

@@ -115,6 +115,39 @@ __global__ void k_i32_out(const int32_t* __restrict__ src, const int32_t* __rest
     dst[id[i]] = src[i];
 }
 
+// Bin key of every particle in the last substep (adaptive_gimp.py:208-216:
+// particle p goes to pid[fl_p] at block base // 4 of level fl_p): the level in
+// bits 60-63 and per axis the block coordinate plus one (floor(base / 4) + 1,
+// the stored block index) in a 20-bit field, first axis highest; ~0 for
+// particles without a level.  Slot j of the current state came from slot
+// perm[j] of the binned state, whose bin_of holds the bin.
+template <int D>
+__global__ void k_get_bins(Ctx c, const int32_t* __restrict__ id, unsigned long long* __restrict__ out) {
+  long long nbins = 0;
+  for (int q = 0; q < c.L; ++q) nbins += c.ctr[CTR_LEVEL + q];
+  for (long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x; j < c.N; j += (long long)gridDim.x * blockDim.x) {
+    const long long b = (long long)(c.bin_of[c.perm[j]] >> (2 * D));
+    unsigned long long key = ~0ull;
+    if (b < nbins) {
+      int l = 0;
+      long long r = b;
+      while (l < c.L - 1 && r >= c.ctr[CTR_LEVEL + l]) {
+        r -= c.ctr[CTR_LEVEL + l];
+        ++l;
+      }
+      unsigned blk = (unsigned)c.lev[l].blist[r];
+      const unsigned nb = (unsigned)c.lev[l].nb;
+      key = (unsigned long long)l << 60;
+#pragma unroll
+      for (int d = D - 1; d >= 0; --d) {
+        key |= (unsigned long long)(blk % nb) << (20 * (D - 1 - d));
+        blk /= nb;
+      }
+    }
+    out[id[j]] = key;
+  }
+}
+
 __global__ void k_iota(int32_t* __restrict__ id, long long n) {
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
     id[i] = (int32_t)i;
@@ -353,7 +386,6 @@ agimp_status agimp_create(const agimp_params* p, int32_t device, agimp_sim** out
     cudaMemset(P.g, 0, (N + 1) * sizeof(int32_t));
     cudaMemset(P.fl, 0xff, (N + 1) * sizeof(int32_t));
   }
-  if (N) k_iota<<<gs_blocks(N), 256>>>(s->buf[0].id, N);
   s->staging_floats = std::max<size_t>((size_t)1 << 20, (size_t)(D * D * N));
   AL(s->staging, s->staging_floats);
   {
@@ -371,6 +403,9 @@ agimp_status agimp_create(const agimp_params* p, int32_t device, agimp_sim** out
     agimp_destroy(s);
     return AGIMP_CUDA_ERROR;
   }
+  // storage slot i starts with caller particle i (on the simulator's own
+  // stream; the synchronisation below orders it before any use)
+  if (N) k_iota<<<gs_blocks(N), 256, 0, s->internal>>>(s->buf[0].id, N);
   s->self = new agimp_batch();
   s->self->sims.push_back(s);
   s->self->single = true;
@@ -471,6 +506,7 @@ agimp_status agimp_set_particles(agimp_sim* s, const float* x, const float* v, c
   CK(cudaSetDevice(s->device));
   StreamUse su(s, stream);
   wait_readback(s, s->par, su.use);  // the upload overwrites the state being read
+  s->bins_valid = false;
   const int D = s->c.dim;
   const Particles& P = s->buf[s->par];
   agimp_status r;
@@ -501,6 +537,34 @@ agimp_status agimp_get_particles(agimp_sim* s, float* x, float* v, float* F, flo
   if (Jp && (r = download_soa(s, P.Jp, Jp, 1, memory, su.use))) return r;
   if (g && (r = copy_i32(s, P.g, g, 0, memory, su.use))) return r;
   if (fl && (r = copy_i32(s, P.fl, fl, 0, memory, su.use))) return r;
+  return AGIMP_OK;
+}
+
+agimp_status agimp_get_bins(agimp_sim* s, uint64_t* keys, int32_t memory, void* stream) {
+  if (!s || !keys || (memory != AGIMP_MEM_DEVICE && memory != AGIMP_MEM_HOST))
+    return fail(s, AGIMP_INVALID_ARG, "bad args");
+  if (!s->bins_valid) return fail(s, AGIMP_NOT_READY, "no substep has binned the current state");
+  CK(cudaSetDevice(s->device));
+  StreamUse su(s, stream);
+  const long long N = s->c.N;
+  if (N == 0) return AGIMP_OK;
+  Ctx& c = cur(s);
+  unsigned long long* dst = (unsigned long long*)keys;
+  unsigned long long* tmp = nullptr;
+  if (memory == AGIMP_MEM_HOST) {
+    CK(cudaMallocAsync((void**)&tmp, N * sizeof(unsigned long long), su.use));
+    dst = tmp;
+  }
+  if (c.dim == 2)
+    k_get_bins<2><<<gs_blocks(N), 256, 0, su.use>>>(c, c.P.id, dst);
+  else
+    k_get_bins<3><<<gs_blocks(N), 256, 0, su.use>>>(c, c.P.id, dst);
+  CK(cudaGetLastError());
+  if (memory == AGIMP_MEM_HOST) {
+    CK(cudaMemcpyAsync(keys, tmp, N * sizeof(unsigned long long), cudaMemcpyDeviceToHost, su.use));
+    CK(cudaFreeAsync(tmp, su.use));
+    CK(cudaStreamSynchronize(su.use));
+  }
   return AGIMP_OK;
 }
 

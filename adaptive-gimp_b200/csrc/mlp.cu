@@ -515,6 +515,25 @@ void launch_mlp_forward_dev(const void* packed, const float* P, const float* X, 
                                                              ERR_MLP);
 }
 
+// Self-test of the bounded completion wait of the tensor-core kernels
+// (umma::mbar_wait): one CTA waits on an mbarrier of one expected arrival.
+// With arrive = 1 a thread arrives first and the wait succeeds; with
+// arrive = 0 nothing ever arrives, the wait gives up after max_polls polls,
+// the kernel records ERR_MLP in *err and returns normally, so the context
+// stays usable.  This is how a lost tensor-core completion surfaces.
+__global__ void k_wait_selftest(uint32_t* err, uint32_t max_polls, int arrive) {
+  __shared__ uint64_t mbar;
+  if (threadIdx.x == 0) {
+    umma::mbar_init(&mbar, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  if (arrive && threadIdx.x == 0)
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(umma::smem_u32(&mbar)) : "memory");
+  const bool ok = umma::mbar_wait(&mbar, 0, max_polls);
+  if (!ok && threadIdx.x == 0) atomicOr(err, ERR_MLP);
+}
+
 }  // namespace agimp
 
 using namespace agimp;
@@ -686,6 +705,24 @@ agimp_status agimp_mlp_errors(agimp_mlp* m, uint32_t* bits, int32_t clear) {
   *bits = (uint32_t)v;
   if (clear) cudaMemset(m->err, 0, sizeof(int32_t));
   return AGIMP_OK;
+}
+
+agimp_status agimp_wait_selftest(int32_t device, int32_t arrive, uint32_t max_polls, uint32_t* bits) {
+  if (!bits || max_polls == 0) return AGIMP_INVALID_ARG;
+  if (cudaSetDevice(device) != cudaSuccess) return AGIMP_CUDA_ERROR;
+  uint32_t* d = nullptr;
+  if (cudaMalloc(&d, sizeof(uint32_t)) != cudaSuccess) return AGIMP_OUT_OF_MEMORY;
+  uint32_t v = 0;
+  bool good = cudaMemset(d, 0, sizeof(uint32_t)) == cudaSuccess;
+  if (good) {
+    k_wait_selftest<<<1, 128>>>(d, max_polls, arrive);
+    good = cudaGetLastError() == cudaSuccess && cudaDeviceSynchronize() == cudaSuccess &&
+           cudaMemcpy(&v, d, sizeof(v), cudaMemcpyDeviceToHost) == cudaSuccess;
+  }
+  cudaFree(d);
+  if (!good) return AGIMP_CUDA_ERROR;
+  *bits = v ? AGIMP_ERR_WAIT : 0u;
+  return v ? AGIMP_DEVICE_TIMEOUT : AGIMP_OK;
 }
 
 }  // extern "C"

@@ -23,6 +23,7 @@ struct agimp_sim {
   size_t staging_floats = 0;
   int8_t* map_dev = nullptr;
   long long substeps = 0;
+  bool bins_valid = false;  // perm / bin_of hold the binning of the current state's last substep
   agimp_batch* self = nullptr;  // the simulator as a batch of one (its substep path)
   // asynchronous readback: the state is ready after ev_state; a copy of
   // buffer k is in flight until ev_read[k]

@@ -58,6 +58,8 @@ def parse():
     ap.add_argument("--scale", type=float, default=1.0, help="body scale of the scene (profiling cases)")
     ap.add_argument("--cpu-seconds", type=float, default=20.0, help="budget of the CPU baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--parity-substeps", type=int, default=100,
+                    help="substeps of the full scene compared with the f32 / f64 oracle in the CPU leg (0: none)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--surrogate", default=None, metavar="NPZ",
                     help="snow return map through this trained surrogate (agimp.train_surrogate output); the line "
@@ -154,6 +156,41 @@ def refine_kernels(scene):
     return 5 + scene.dim
 
 
+def scene_config(scene, world=1):
+    """The `config` object of a single-scene line: the workload and every
+    interpretation of the configuration as a structured key (both arms print
+    the same object)."""
+    import numpy as np
+
+    from agimp import scenes
+    sk = scene.sim_kwargs
+    k = int(scene.name[6]) if scene.name.startswith("config") and scene.name[6].isdigit() else None
+    rho = scenes.RHO.get(k)
+    d = scene.dim
+    vel = np.unique(np.asarray(scene.v, np.float32), axis=0)
+    mat = {"model": "fixed-corotated" + (" + snow plasticity" if sk.get("plasticity") == "snow" else ""),
+           "E": sk["E"] * rho if rho else sk["E"], "rho": rho, "E_over_rho": sk["E"], "nu": sk["nu"]}
+    if sk.get("plasticity") == "snow":
+        mat.update(theta_c=sk.get("theta_c", 2.5e-2), theta_s=sk.get("theta_s", 7.5e-3),
+                   hardening=sk.get("hardening", 10.0))
+    return {
+        "workload": scene.name, "particles": scene.n, "levels": scene.level,
+        "coarsest": scene.coarsest, "finest": scene.coarsest << (scene.level - 1), "dt": scene.dt,
+        "refine_every": scene.refine_every, "parallelism": "replicas" if world > 1 else "single",
+        "material": mat,
+        "gravity": list(sk.get("gravity", ())),
+        "initial_velocity": vel.tolist() if len(vel) <= 4 else "per body",
+        "colliders": [list(c) for c in sk.get("colliders", ())],
+        "boundary": sk.get("boundary_mode", "ref_slip"),
+        "invalid_nodes": sk.get("invalid_nodes", "raw"),
+        "refinement": ({"rule": "free-surface depth (Chebyshev, finest cells)", "band": scene.refine_band,
+                        "every": scene.refine_every} if scene.refine_every else "static level map"),
+        "l2": "inputs exceed L2 (particle state %.0f MB)" % (scene.n * (4 * (2 * d + 2 * d * d + 2)) / 1e6),
+        "seed": 0,
+        "description": scene.description,
+    }
+
+
 def run_steps(sim, scene, first, count, stream=None):
     for i in range(first, first + count):
         if scene.refine_every and i % scene.refine_every == 0:
@@ -205,6 +242,60 @@ def cpu_oracle_run(scene, seconds, threads, steps_cap=None, warmup=1):
     return n * done / el, done, el
 
 
+def cpu_parity_leg(a, scene, local, tuning):
+    """The CPU baseline, and from the same oracle run the long-horizon parity
+    of the GPU path.  The full scene runs from its initial state for
+    --parity-substeps substeps (refinement included) on the GPU, on the f32
+    oracle (OpenMP on all host threads; after one warm-up substep, the
+    substeps finished within --cpu-seconds are the timed CPU sample) and on
+    the f64 oracle; positions, velocities and per-level grid momentum are
+    compared (oracle/parity.py).  Returns (cpu_baseline, parity or None)."""
+    import parity as PY
+    from agimp.simulator import tabulate_level_map
+    threads = os.cpu_count() or 1
+    steps = max(0, a.parity_substeps)
+    lm = (tabulate_level_map(scene.grid_initializer, scene.dim, scene.level, scene.coarsest)
+          if scene.grid_initializer is not None else None)
+    par = None
+    if steps:
+        sim = scene.build(device=local)
+        sim.set_tuning(tuning["chunk"], tuning["ctas_per_sm"])
+        run_steps(sim, scene, 0, steps)
+        gpu = {"x": sim.x_p.to_numpy(), "v": sim.v_p.to_numpy(), "g": sim.g_p.to_numpy()}
+        errors = sim.errors()
+        boxes = PY.grid_boxes(gpu["x"], scene.coarsest, scene.level)
+        grids = [(sim.ad_grid_m[l].read(lo, n), sim.ad_grid_v[l].read(lo, n)) for l, (lo, n) in enumerate(boxes)]
+        sim.close()
+    o32 = PY.make_oracle(scene, False, lm)
+    PY.step(o32, scene, 0, threads)  # warm-up
+    if steps:
+        t0 = time.perf_counter()
+        done, el = PY.timed_run(o32, scene, 1, steps - 1, threads, a.cpu_seconds)
+        total32 = time.perf_counter() - t0
+    else:
+        done, el = 0, 0.0
+        t0 = time.perf_counter()
+        while True:
+            PY.step(o32, scene, 1 + done, threads)
+            done += 1
+            el = time.perf_counter() - t0
+            if el >= a.cpu_seconds:
+                break
+    cpu = {"value": scene.n * done / el, "unit": METRIC, "cores": threads, "kind": "port",
+           "sample": "%s: %d substeps of the full %d-particle scene after 1 warm-up, %.1f s, OpenMP%s"
+                     % (scene.name, done, scene.n, el,
+                        ", the first substeps of the parity run" if steps else "")}
+    if steps:
+        t1 = time.perf_counter()
+        o64 = PY.make_oracle(scene, True, lm)
+        PY.run(o64, scene, 0, steps, threads)
+        par = PY.report(gpu, grids, o32, o64, scene.x, boxes, steps)
+        par["gpu_device_errors"] = errors
+        par["oracle_seconds"] = {"f32": round(total32, 1), "f64": round(time.perf_counter() - t1, 1)}
+        par["grid_boxes"] = [[lo, n] for lo, n in boxes]
+    return cpu, par
+
+
 def run_reference(a):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -227,15 +318,15 @@ def run_reference(a):
                     "restatement of its algorithm (oracle/oracle.cpp) with OpenMP on all host threads"}))
         return
     scene = scenes.make_config(a.config, scale=a.scale)
-    val, done, el = cpu_oracle_run(scene, budget, threads, steps_cap=a.steps, warmup=min(a.warmup, 1))
+    warm = min(a.warmup, 10)
+    val, done, el = cpu_oracle_run(scene, budget, threads, steps_cap=a.steps, warmup=warm)
     sample = "%s: %d substeps of the full %d-particle scene after %d warm-up, %.1f s" % (
-        scene.name, done, scene.n, min(a.warmup, 1), el)
+        scene.name, done, scene.n, warm, el)
     out = {
         "impl": "reference", "metric": METRIC, "value": val, "unit": METRIC, "n_gpus": a.gpus, "steps": done,
-        "warmup": min(a.warmup, 1), "ms_per_step": 1e3 * el / done, "higher_is_better": True, "scaling": "weak",
+        "warmup": warm, "ms_per_step": 1e3 * el / done, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": scene.name, "particles": scene.n, "levels": scene.level,
-                   "finest": scene.coarsest << (scene.level - 1), "description": scene.description},
+        "config": scene_config(scene, a.gpus),
         "cpu_baseline": {"value": val, "unit": METRIC, "cores": threads, "kind": "port", "sample": sample},
         "e2e": {"value": val, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "note": "the reference is Taichi code and Taichi cannot be installed offline; this arm runs the CPU "
@@ -364,11 +455,7 @@ def run_agimp(a):
         "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
         "ms_per_step": ms_max / a.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32", "data": "synthetic",
-        "config": {"workload": scene.name, "particles": scene.n, "levels": scene.level,
-                   "finest": scene.coarsest << (scene.level - 1), "dt": scene.dt,
-                   "refine_every": scene.refine_every, "parallelism": "replicas" if world > 1 else "single",
-                   "l2": "inputs exceed L2 (particle state %.0f MB)" % (scene.n * (4 * (2 * d + 2 * d * d + 2)) / 1e6),
-                   "description": scene.description},
+        "config": scene_config(scene, world),
         "roofline": roof,
         "phases_ms": phases,
         "tuning": tuning,
@@ -388,11 +475,9 @@ def run_agimp(a):
     if not a.no_e2e:
         out["e2e"] = e2e_run(a, scene, local, a.surrogate and (mlp, xmax, a.sur_tol), tuning)
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
-        threads = os.cpu_count() or 1
-        val, done, el = cpu_oracle_run(scene, a.cpu_seconds, threads)
-        out["cpu_baseline"] = {"value": val, "unit": METRIC, "cores": threads, "kind": "port",
-                               "sample": "%s: %d substeps of the full %d-particle scene after 1 warm-up, %.1f s, "
-                                         "OpenMP" % (scene.name, done, scene.n, el)}
+        out["cpu_baseline"], par = cpu_parity_leg(a, scene, local, tuning)
+        if par is not None:
+            out["parity"] = par
     if dist:
         dist.barrier()
         dist.destroy_process_group()

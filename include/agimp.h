@@ -55,6 +55,7 @@ enum { AGIMP_MEM_DEVICE = 0, AGIMP_MEM_HOST = 1 };
 #define AGIMP_ERR_ESCAPED 2u  /* a particle left [0,1)^dim; it is frozen (fl_p = -1) */
 #define AGIMP_ERR_MAP_OOB 4u  /* a level-map lookup left the table */
 #define AGIMP_ERR_NOBIN 8u    /* a particle's bin block was not active (internal) */
+#define AGIMP_ERR_WAIT 16u    /* a bounded device wait (tensor-core completion) gave up */
 
 /* Mask flags, utils.py:5-9. */
 #define AGIMP_ACTIVATED 1
@@ -121,6 +122,15 @@ agimp_status agimp_set_particles(agimp_sim* s, const float* x, const float* v, c
  * and Jp.  NULL outputs are skipped. */
 agimp_status agimp_get_particles(agimp_sim* s, float* x, float* v, float* F, float* C, float* m, int32_t* g,
                                  int32_t* fl, float* Jp, int32_t memory, void* stream);
+
+/* The bins of the last substep (adaptive_gimp.py:208-216, the pid[l] lists:
+ * particle p sits in the list of level fl_p at block base // 4 of that
+ * level), one key per particle in the caller's order: the level in bits 60-63
+ * and, per axis, floor(base / 4) + 1 in a 20-bit field (first axis highest);
+ * UINT64_MAX for particles without a level (fl_p = -1).  Particles with equal
+ * keys share a pid block.  AGIMP_NOT_READY until a substep has binned the
+ * current state (after agimp_set_particles, or before the first substep). */
+agimp_status agimp_get_bins(agimp_sim* s, uint64_t* keys, int32_t memory, void* stream);
 
 /* Asynchronous field readback into HOST memory (pinned, for the copy to
  * overlap): enqueues the copy of the current state on `stream` and returns at
@@ -253,6 +263,14 @@ agimp_status agimp_set_recorder(agimp_sim* s, float* X, float* T, int64_t capaci
 agimp_status agimp_recorded(agimp_sim* s, int64_t* count, int32_t reset);
 /* bit 0: a tensor-core completion wait timed out.  Synchronizes the device. */
 agimp_status agimp_mlp_errors(agimp_mlp* m, uint32_t* bits, int32_t clear);
+/* No counterpart in the reference (Taichi has no device-side waits): a
+ * self-test of the bounded completion wait every tensor-core kernel uses.
+ * One CTA waits on an mbarrier; with arrive != 0 a thread arrives first and the
+ * wait succeeds (AGIMP_OK, *bits = 0); with arrive == 0 nothing arrives, the
+ * wait gives up after max_polls polls, the kernel records the timeout and
+ * returns normally: AGIMP_DEVICE_TIMEOUT and *bits = AGIMP_ERR_WAIT, with the
+ * CUDA context still usable.  Synchronizes the device. */
+agimp_status agimp_wait_selftest(int32_t device, int32_t arrive, uint32_t max_polls, uint32_t* bits);
 
 /* ---- Headless drawing (2D).  The reference's GUI (gui.py) draws into a GGUI
  * window; there is no window here, the image goes to a buffer.  img is

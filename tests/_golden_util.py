@@ -48,3 +48,25 @@ def rel_close(a, b, rtol):
     b = np.asarray(b, np.float64)
     scale = max(np.abs(b).max(), 1e-30)
     return np.abs(a - b).max() <= rtol * scale, np.abs(a - b).max() / scale
+
+
+# Nodes lighter than this fraction of a level's heaviest node carry velocities
+# v = p / m whose rounding error grows like 1 / m (a node touched only by the
+# far edge of one particle's stencil can weigh 1e-10 of a typical node); their
+# velocity is checked through the momentum m v instead.
+LIGHT_NODE = 1e-5
+
+
+def grid_v_close(v, v_ref, m_ref, rtol):
+    """Nodal velocities: momentum m_ref v within rtol of the largest momentum,
+    and velocity within rtol of the largest velocity at nodes heavier than
+    LIGHT_NODE of the heaviest.  Returns (ok, worst ratio)."""
+    v = np.asarray(v, np.float64)
+    v_ref = np.asarray(v_ref, np.float64)
+    m = np.asarray(m_ref, np.float64)[..., None]
+    ok_p, r_p = rel_close(m * v, m * v_ref, rtol)
+    heavy = np.broadcast_to(m > LIGHT_NODE * max(m.max(), 1e-30), v.shape)
+    if not heavy.any():
+        return ok_p, r_p
+    ok_v, r_v = rel_close(v[heavy], v_ref[heavy], rtol)
+    return ok_p and ok_v, max(r_p, r_v)
