@@ -33,7 +33,8 @@ EXPORTS = (
     "agimp_set_tuning", "agimp_get_tuning", "agimp_autotune",
     "agimp_batch_create", "agimp_batch_destroy", "agimp_batch_last_error", "agimp_batch_substep",
     "agimp_batch_set_graphs", "agimp_batch_set_tuning", "agimp_batch_get_tuning", "agimp_batch_autotune",
-    "agimp_batch_kernels_per_substep", "agimp_batch_profile_substep",
+    "agimp_batch_kernels_per_substep", "agimp_batch_profile_substep", "agimp_batch_set_surrogate",
+    "agimp_batch_surrogate_stats",
     "agimp_render_mask", "agimp_render_particles", "agimp_get_particles_async", "agimp_batch_positions_async",
     "agimp_get_level_map", "agimp_lattice_count", "agimp_lattice_fill", "agimp_random_fill",
     "agimp_set_level_map_rule", "agimp_set_coarse_level_map", "agimp_render_scene3d", "agimp_cell_lines",
@@ -146,6 +147,9 @@ def load(path: str | None = None):
     L.agimp_mlp_train_step.argtypes = [vp, vp, vp, ctypes.c_int64, ctypes.c_float, vp, vp]
     L.agimp_mlp_reset_optimizer.argtypes = [vp]
     L.agimp_set_surrogate.argtypes = [vp, vp, ctypes.POINTER(ctypes.c_float), ctypes.c_float]
+    L.agimp_batch_set_surrogate.argtypes = [vp, vp, ctypes.POINTER(ctypes.c_float), ctypes.c_float]
+    L.agimp_batch_surrogate_stats.argtypes = [vp, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int64),
+                                              ctypes.POINTER(ctypes.c_uint32)]
     L.agimp_set_recorder.argtypes = [vp, vp, vp, ctypes.c_int64, ctypes.c_int32]
     L.agimp_recorded.argtypes = [vp, ctypes.POINTER(ctypes.c_int64), ctypes.c_int32]
     tp = ctypes.POINTER(Tuning)

@@ -96,3 +96,24 @@ class SceneBatch:
 
     def kernels_per_substep(self):
         return int(self._L.agimp_batch_kernels_per_substep(self._h))
+
+    # -- surrogate return map over the batch (extension) ------------------------
+    def set_surrogate(self, mlp, xmax=None, tol=0.02):
+        """Snow scenes of the batch take their return map from `mlp`
+        (agimp.surrogate.MLP) with the exact map as fallback; one MLP launch per
+        substep serves every scene.  None switches it off."""
+        if mlp is None:
+            _capi.check(self._L.agimp_batch_set_surrogate(self._h, None, None, 0.0), self._h, "batch surrogate",
+                        batch=True)
+            return
+        xm = (ctypes.c_float * 7)(*[float(v) for v in xmax])
+        self._mlp = mlp  # the parameters must outlive their use
+        _capi.check(self._L.agimp_batch_set_surrogate(self._h, mlp._h, xm, float(tol)), self._h, "batch surrogate",
+                    batch=True)
+
+    def surrogate_stats(self):
+        """{'handed_off', 'rejected', 'errors'} of the last substep over the batch."""
+        h, r, e = ctypes.c_int64(), ctypes.c_int64(), ctypes.c_uint32()
+        _capi.check(self._L.agimp_batch_surrogate_stats(self._h, ctypes.byref(h), ctypes.byref(r), ctypes.byref(e)),
+                    self._h, "batch surrogate stats", batch=True)
+        return {"handed_off": h.value, "rejected": r.value, "errors": e.value}

@@ -283,14 +283,21 @@ def _place_boxes(rng, sides, tries=200):
     return placed
 
 
-def make_batch_config(seed=0, n_scenes=256, scale=1.0, device=False):
+SNOW_BATCH = dict(E=1.4e5 / RHO[2], nu=0.2, gravity=(0.0, -9.8), boundary_mode="sticky", plasticity="snow",
+                  theta_c=2.5e-2, theta_s=7.5e-3, hardening=10.0)
+
+
+def make_batch_config(seed=0, n_scenes=256, scale=1.0, device=False, material="elastic"):
     """Config 4: independent 2D scenes for one batch.  Each scene draws its
     level count from {2, 3, 4}, its finest resolution from {256, 512}, 1-3
     boxes and a particle count from a lognormal clipped to [2k, 60k] (times
     `scale`); the boxes share that count at 4 particles per finest cell.
     Material, time step and level maps are config 1's (elastic, E=1e4 with
     rho=100, sticky walls, dt=1e-4, static map: the finest level within 2
-    coarsest cells of a box or below y = 0.25)."""
+    coarsest cells of a box or below y = 0.25).  material="snow" keeps the
+    scenes and gives them config 2's snow material and time step (5e-5), with
+    each box thrown at a velocity drawn uniformly from [-2, 2]^2 (a generator
+    of its own, so the scenes' shapes are the elastic batch's)."""
     rng = np.random.default_rng(seed)
     out = []
     for i in range(n_scenes):
@@ -318,9 +325,16 @@ def make_batch_config(seed=0, n_scenes=256, scale=1.0, device=False):
         xs = [fill_lattice(rng, 2, fin, *box_region(lo, hi)) for lo, hi in boxes]
         x = np.concatenate(xs) if xs else np.zeros((0, 2), np.float32)
         n = len(x)
-        out.append(Scene("config4_scene%03d" % i, 2, L, c, x, np.zeros((n, 2), np.float32),
-                         np.full(n, L - 1, np.int32), _unit_mass(n), 1e-4, 1000,
-                         dict(E=1e4 / RHO[1], nu=0.2, gravity=(0.0, -9.8), boundary_mode="sticky"),
+        if material == "snow":
+            vrng = np.random.default_rng(1000003 * (seed + 1) + i)
+            v = np.concatenate([np.tile(vrng.uniform(-2, 2, 2).astype(np.float32), (len(p), 1)) for p in xs]) \
+                if xs else np.zeros((0, 2), np.float32)
+            kw, dt = dict(SNOW_BATCH), 5e-5
+        else:
+            v, kw, dt = np.zeros((n, 2), np.float32), dict(E=1e4 / RHO[1], nu=0.2, gravity=(0.0, -9.8),
+                                                           boundary_mode="sticky"), 1e-4
+        out.append(Scene("config4_scene%03d" % i, 2, L, c, x, v,
+                         np.full(n, L - 1, np.int32), _unit_mass(n), dt, 1000, kw,
                          grid_initializer=band_level_map([(tuple(lo), tuple(hi)) for lo, hi in boxes], 2, L, c),
                          description="%d levels %d^2..%d^2, %d boxes, %d particles" % (L, c, fin, len(boxes), n)))
     return out

@@ -10,6 +10,7 @@
 //     counts (at least one each);
 //   bin allocator: a quarter of the scene's grid-stride CTAs (at least one).
 // The kernels find their scene by binary search over the range starts.
+#include <cstdlib>
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -35,6 +36,10 @@ Ctx& sim_ctx(agimp_sim* s) {
 
 agimp_status batch_init(agimp_batch* b) {
   const int n = (int)b->sims.size();
+  {
+    const char* e = std::getenv("AGIMP_PDL");
+    b->pdl = !(e && e[0] == '0');
+  }
   b->device = b->sims[0]->device;
   b->dim = b->sims[0]->c.dim;
   b->sms = b->sims[0]->c.sms;
@@ -67,8 +72,51 @@ void batch_drop_graphs(agimp_batch* b) {
     }
 }
 
+// The batch's shared surrogate: slot buffers over all scenes' particles
+// (allocated on first use), the MLP's parameters and the acceptance rule.
+// packed == nullptr switches it off.
+agimp_status batch_set_surrogate(agimp_batch* b, const void* packed, const float* P, const float* xmax, float tol) {
+  BCK(cudaSetDevice(b->device));
+  BCK(cudaDeviceSynchronize());
+  batch_drop_graphs(b);
+  for (int k = 0; k < 2; ++k) std::fill(b->hvalid[k].begin(), b->hvalid[k].end(), 0);
+  if (!packed) {
+    b->sur = 0;
+    return AGIMP_OK;
+  }
+  long long tot = 0;
+  for (agimp_sim* s : b->sims) tot += s->c.N;
+  if (tot > b->scap) {
+    if (b->sX) cudaFree(b->sX);
+    if (b->sY) cudaFree(b->sY);
+    if (b->smeta) cudaFree(b->smeta);
+    b->sX = b->sY = b->smeta = nullptr;
+    b->scap = 0;
+    BCK(cudaMalloc(&b->sX, sizeof(float) * (tot * 7 + 8)));
+    BCK(cudaMalloc(&b->sY, sizeof(float) * (tot * 4 + 8)));
+    BCK(cudaMalloc(&b->smeta, sizeof(float) * (tot * SUR_META + 8)));
+    b->scap = tot;
+  }
+  if (!b->sctr) {
+    BCK(cudaMalloc(&b->sctr, 2 * sizeof(int32_t)));
+    BCK(cudaMemset(b->sctr, 0, 2 * sizeof(int32_t)));
+  }
+  b->mlp_packed = packed;
+  b->mlp_P = P;
+  for (int k = 0; k < 8; ++k) b->sur_xmax[k] = k < 7 ? xmax[k] : 0.f;
+  b->sur_tol = tol;
+  b->sur = 1;
+  return AGIMP_OK;
+}
+
 void batch_free(agimp_batch* b) {
   batch_drop_graphs(b);
+  if (b->sX) cudaFree(b->sX);
+  if (b->sY) cudaFree(b->sY);
+  if (b->smeta) cudaFree(b->smeta);
+  if (b->sctr) cudaFree(b->sctr);
+  b->sX = b->sY = b->smeta = nullptr;
+  b->sctr = nullptr;
   for (int k = 0; k < 2; ++k)
     if (b->dctx[k]) cudaFree(b->dctx[k]);
   if (b->dofs) cudaFree(b->dofs);
@@ -122,9 +170,27 @@ static agimp_status sync_contexts(agimp_batch* b, int ph, float dt, cudaStream_t
     Ctx& c = sim_ctx(b->sims[i]);
     c.dt = dt;
     c.chunk = b->tune.chunk;
+    // what this batch uploads: the scene's context with its index here and,
+    // in a batch of several, the batch's surrogate setting in place of the
+    // scene's own
+    Ctx t = c;
+    t.scene = i;
+    if (!b->single) {
+      t.sur = b->sur && c.plast == 1;
+      if (b->sur) {
+        t.mlp_packed = b->mlp_packed;
+        t.mlp_P = b->mlp_P;
+        t.sur_X = b->sX;
+        t.sur_Y = b->sY;
+        t.sur_meta = b->smeta;
+        t.sur_ctr = b->sctr;
+        t.sur_tol = b->sur_tol;
+        for (int k = 0; k < 8; ++k) t.sur_xmax[k] = b->sur_xmax[k];
+      }
+    }
     Ctx& h = b->hctx[ph][i];
-    if (!b->hvalid[ph][i] || std::memcmp(&h, &c, sizeof(Ctx)) != 0) {
-      std::memcpy(&h, &c, sizeof(Ctx));
+    if (!b->hvalid[ph][i] || std::memcmp(&h, &t, sizeof(Ctx)) != 0) {
+      std::memcpy(&h, &t, sizeof(Ctx));
       b->hvalid[ph][i] = 1;
       lo = std::min(lo, i);
       hi = std::max(hi, i);
@@ -157,6 +223,33 @@ static BatchLaunch make_launch(agimp_batch* b, int ph) {
   bl.side = b->side;
   bl.fork = b->ev_fork;
   bl.join = b->ev_join;
+  bl.pdl = b->pdl;
+  bl.sms = b->sms;
+  bl.sur = 0;
+  if (b->single) {
+    const Ctx& c = b->hctx[ph][0];
+    if (c.sur && c.plast == 1 && c.N) {
+      bl.sur = 1;
+      bl.mlp_packed = c.mlp_packed;
+      bl.mlp_P = c.mlp_P;
+      bl.sur_X = c.sur_X;
+      bl.sur_Y = c.sur_Y;
+      bl.sur_meta = c.sur_meta;
+      bl.sur_n = c.sur_ctr;
+      bl.sur_cap = c.N;
+      bl.sur_err = c.ctr + CTR_ERR;
+    }
+  } else if (b->sur && bl.any_plastic && b->scap) {
+    bl.sur = 1;
+    bl.mlp_packed = b->mlp_packed;
+    bl.mlp_P = b->mlp_P;
+    bl.sur_X = b->sX;
+    bl.sur_Y = b->sY;
+    bl.sur_meta = b->smeta;
+    bl.sur_n = b->sctr;
+    bl.sur_cap = b->scap;
+    bl.sur_err = b->sctr + 1;
+  }
   return bl;
 }
 
@@ -167,7 +260,7 @@ static agimp_batch::Key launch_key(const BatchLaunch& bl, cudaStream_t use) {
   k.any_dynamic = bl.any_dynamic;
   k.any_plastic = bl.any_plastic;
   k.chunk = bl.chunk;
-  k.sur = bl.single && bl.single->sur && bl.single->plast == 1 && bl.single->N;
+  k.sur = bl.sur;
   for (int i = 0; i < NMAP; ++i) k.nct[i] = bl.nct[i];
   k.stream = use;
   return k;
@@ -175,12 +268,6 @@ static agimp_batch::Key launch_key(const BatchLaunch& bl, cudaStream_t use) {
 
 agimp_status batch_step(agimp_batch* b, float dt, int n, cudaStream_t use, cudaEvent_t* ev) {
   BCK(cudaSetDevice(b->device));
-  if (!b->single)
-    for (agimp_sim* s : b->sims)
-      if (s->c.sur) {
-        b->err = "a batch of several scenes cannot use the surrogate return map";
-        return AGIMP_INVALID_ARG;
-      }
   if (!b->maps_valid) {
     const agimp_status st = build_maps(b, use);
     if (st != AGIMP_OK) return st;

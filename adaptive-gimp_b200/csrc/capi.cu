@@ -350,6 +350,7 @@ agimp_status agimp_create(const agimp_params* p, int32_t device, agimp_sim** out
   cudaMemset(c.nmask, 0, Vf.nblocks * per * sizeof(uint32_t));
   AL(c.ctr, CTR_COUNT);
   cudaMemset(c.ctr, 0, CTR_COUNT * sizeof(int32_t));
+  c.sur_ctr = c.ctr + CTR_SUR;  // stepping alone, the surrogate slots count here
   AL(c.touch_flag, Vf.nblocks);
   AL(c.touch_list, Vf.nblocks);
   cudaMemset(c.touch_flag, 0, Vf.nblocks * sizeof(uint32_t));
@@ -816,6 +817,7 @@ agimp_status agimp_set_surrogate(agimp_sim* s, const agimp_mlp* m, const float* 
   mlp_buffers(m, &s->c.mlp_packed, &s->c.mlp_P);
   for (int k = 0; k < 8; ++k) s->c.sur_xmax[k] = k < 7 ? xmax[k] : 0.f;
   s->c.sur_tol = tol;
+  s->c.sur_ctr = s->c.ctr + CTR_SUR;
   s->c.sur = 1;
   return AGIMP_OK;
 }
@@ -1030,6 +1032,44 @@ agimp_status agimp_batch_positions_async(agimp_batch* b, float* x, void* stream)
   if (!b) return AGIMP_INVALID_ARG;
   BatchStream bs(b, stream);
   return batch_positions_async(b, x, bs.use);
+}
+
+agimp_status agimp_batch_set_surrogate(agimp_batch* b, const agimp_mlp* m, const float* xmax, float tol) {
+  if (!b) return AGIMP_INVALID_ARG;
+  if (!m) return batch_set_surrogate(b, nullptr, nullptr, nullptr, 0.f);
+  if (!xmax || !(tol > 0.f)) return bfail(b, AGIMP_INVALID_ARG, "surrogate needs xmax[7] and tol > 0");
+  bool any = false;
+  for (agimp_sim* s : b->sims) any = any || s->c.plast == 1;
+  if (!any) return bfail(b, AGIMP_INVALID_ARG, "the surrogate replaces the snow return map: no scene has snow plasticity");
+  const void* packed = nullptr;
+  const float* P = nullptr;
+  mlp_buffers(m, &packed, &P);
+  return batch_set_surrogate(b, packed, P, xmax, tol);
+}
+
+agimp_status agimp_batch_surrogate_stats(agimp_batch* b, int64_t* handed, int64_t* rejected, uint32_t* errors) {
+  if (!b) return AGIMP_INVALID_ARG;
+  if (cudaSetDevice(b->device) != cudaSuccess || cudaDeviceSynchronize() != cudaSuccess) return AGIMP_CUDA_ERROR;
+  int32_t h[2] = {0, 0};
+  if (b->single) {
+    agimp_sim* s = b->sims[0];
+    if (cudaMemcpy(h, s->c.ctr + CTR_SUR, sizeof(int32_t), cudaMemcpyDeviceToHost) != cudaSuccess)
+      return AGIMP_CUDA_ERROR;
+  } else if (b->sctr &&
+             cudaMemcpy(h, b->sctr, 2 * sizeof(int32_t), cudaMemcpyDeviceToHost) != cudaSuccess) {
+    return AGIMP_CUDA_ERROR;
+  }
+  long long rej = 0;
+  for (agimp_sim* s : b->sims) {
+    int32_t v = 0;
+    if (cudaMemcpy(&v, s->c.ctr + CTR_SURFB, sizeof(int32_t), cudaMemcpyDeviceToHost) != cudaSuccess)
+      return AGIMP_CUDA_ERROR;
+    rej += v;
+  }
+  if (handed) *handed = h[0];
+  if (rejected) *rejected = rej;
+  if (errors) *errors = h[1] ? AGIMP_ERR_WAIT : 0u;
+  return AGIMP_OK;
 }
 
 int32_t agimp_batch_kernels_per_substep(const agimp_batch* b) {

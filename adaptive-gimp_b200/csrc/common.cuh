@@ -119,6 +119,12 @@ struct Ctx {
   float* rec_T;              // [rec_cap][4]
   const void* mlp_packed;    // bf16 operand tiles of the MLP
   const float* mlp_P;        // f32 parameters of the MLP
+  // Slot counter of the surrogate buffers: this scene's ctr[CTR_SUR] when the
+  // simulator steps alone, or one counter shared by every scene of a batch
+  // whose scenes share one set of buffers (then `scene` tells k_sur_finish
+  // whose particle a slot holds).
+  int32_t* sur_ctr;
+  int scene;                 // index of the scene in the batch being stepped
 };
 
 // Surrogate features of a trial elastic state with singular values sig and
@@ -132,7 +138,7 @@ struct Ctx {
 // bf16 resolution only limits the plastic part of the map.
 constexpr float SUR_SIG = 0.05f, SUR_LJ = 0.5f, SUR_H = 5.f;
 constexpr float SUR_DSIG = 0.02f, SUR_DLJ = 0.02f;
-constexpr int SUR_META = 24;  // slot, U[9], V[9], sig[3], jp (padded)
+constexpr int SUR_META = 24;  // slot, U[9], V[9], sig[3], jp, scene
 
 template <int D>
 __host__ __device__ __forceinline__ void snow_features(const float* sig, float jp, float xi, float tc, float ts,
@@ -700,18 +706,33 @@ struct Batch {
 struct BatchLaunch {
   Batch b;
   int dim;
+  int sms;           // multiprocessors of the device
   int maxL;          // most levels of any scene (per-level launches run to it)
   int nct[NMAP];     // CTAs of each launch kind
   int chunk;         // P2G work-item size of every scene
   int any_dynamic;   // some scene activates cells from g_p (runs k_mark_hier)
   int any_plastic;   // some scene has snow plasticity (runs k_project)
-  const Ctx* single; // host context of a single simulator (surrogate step), else null
+  const Ctx* single; // host context of a single simulator, else null
+  // surrogate return map of the substep (sur != 0): the MLP runs over the
+  // *sur_n slots of sur_X / sur_Y, then k_sur_finish applies them
+  int sur;
+  const void* mlp_packed;
+  const float* mlp_P;
+  const float* sur_X;
+  float* sur_Y;
+  const float* sur_meta;
+  const int32_t* sur_n;
+  long long sur_cap;
+  int32_t* sur_err;
   // second stream of the substep (null: everything on the caller's stream):
   // k_ghost_tj runs on it beside the binning kernels and P2G, which read no
   // node mask and only the exact-ACTIVATED cell tests that k_ghost_tj leaves
   // unchanged; the restriction waits for it
   cudaStream_t side;
   cudaEvent_t fork, join;
+  // programmatic dependent launches between consecutive substep kernels on
+  // one stream (launch_k); off for phase timing
+  bool pdl;
 };
 
 // The calling CTA's scene: its context (copied to *sc), its rank among the
@@ -734,6 +755,12 @@ __device__ __forceinline__ const Ctx& scene_slice(const Batch& B, Ctx* sc, int& 
   unsigned* dst = (unsigned*)sc;
   for (int i = threadIdx.x; i < (int)(sizeof(Ctx) / 4); i += blockDim.x) dst[i] = __ldg(&src[i]);
   __syncthreads();
+  // Launched as a programmatic dependent of the previous kernel on the stream
+  // (launch_k with pdl), the CTA may have started before that kernel finished:
+  // everything above reads only host-written launch data; wait here until the
+  // previous kernel has completed and its writes are visible.  Without the
+  // launch attribute this returns at once.
+  asm volatile("griddepcontrol.wait;" ::: "memory");
   return *sc;
 }
 
@@ -751,6 +778,27 @@ __device__ __forceinline__ const Ctx& scene_slice(const Batch& B, Ctx* sc, int& 
 // the CTA (for warp-collective bodies): p = p0 + threadIdx.x may be >= c.N
 #define SCENE_PARTICLES(p0) \
   for (int p0 = bid_ * (int)blockDim.x; p0 < c.N; p0 += nblk_ * (int)blockDim.x)
+
+// Launch kernel k on stream s; with pdl as a programmatic dependent launch:
+// the launch may begin while the previous kernel on s is still finishing, so
+// launch latency and each CTA's prologue (scene lookup and context copy in
+// scene_slice) overlap that kernel's tail.  Every kernel launched this way
+// starts with SCENE_CTA, which waits for the previous kernel before touching
+// its results.
+template <typename... P, typename... A>
+inline cudaError_t launch_k(bool pdl, void (*k)(P...), int grid, int block, size_t smem, cudaStream_t s, A... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)grid);
+  cfg.blockDim = dim3((unsigned)block);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = pdl ? 1 : 0;
+  return cudaLaunchKernelEx(&cfg, k, args...);
+}
 
 // ---------------------------------------------------------------------------
 // host-side launchers (defined in topology.cu / transfer.cu)

@@ -60,6 +60,9 @@ struct agimp_batch {
   int device = 0, dim = 2, sms = 148;
   agimp_tuning tune{agimp::CHUNK, 8, 0.f};
   bool graphs = true;
+  // programmatic dependent launches inside a substep (AGIMP_PDL=0 in the
+  // environment switches them off, for comparison)
+  bool pdl = true;
   agimp::Ctx* dctx[2] = {nullptr, nullptr};
   std::vector<agimp::Ctx> hctx[2];
   std::vector<char> hvalid[2];
@@ -82,6 +85,19 @@ struct agimp_batch {
   long long read_step = 0;
   float* xstage = nullptr;
   void* dsrc = nullptr;  // per-scene sources of the gather
+  // surrogate return map shared by the scenes of a batch of several
+  // (agimp_batch_set_surrogate): one set of slot buffers over all scenes'
+  // particles and one slot counter, so one MLP launch serves the batch
+  int sur = 0;
+  const void* mlp_packed = nullptr;
+  const float* mlp_P = nullptr;
+  float sur_xmax[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  float sur_tol = 0.f;
+  float* sX = nullptr;        // [cap][7]
+  float* sY = nullptr;        // [cap][4]
+  float* smeta = nullptr;     // [cap][SUR_META]
+  int32_t* sctr = nullptr;    // [0] slots this substep, [1] error bits of the MLP
+  long long scap = 0;
 };
 
 namespace agimp {
@@ -100,6 +116,7 @@ agimp_status batch_positions_async(agimp_batch* b, float* x, cudaStream_t use);
 void wait_readback(agimp_sim* s, int buf, cudaStream_t use);
 agimp_status batch_autotune(agimp_batch* b, float dt, int trials, agimp_tuning* best, cudaStream_t use);
 agimp_status batch_set_tuning(agimp_batch* b, const agimp_tuning* t);
+agimp_status batch_set_surrogate(agimp_batch* b, const void* packed, const float* P, const float* xmax, float tol);
 // headless drawing (render.cu)
 agimp_status render_mask(agimp_sim* s, int res, int show_ghost, int show_node, float* img, int memory, cudaStream_t st);
 agimp_status render_scene3d(agimp_sim* s, int res, const agimp_view3d* v, float* img, int memory, cudaStream_t st);

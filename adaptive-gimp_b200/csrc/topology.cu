@@ -50,6 +50,7 @@ __global__ void k_clear(Batch B) {
     c.ctr[CTR_UNBIN] = 0;
     c.ctr[CTR_SUR] = 0;
     c.ctr[CTR_SURFB] = 0;
+    if (c.sur) *c.sur_ctr = 0;  // a batch's shared slot counter (every scene clears it)
     c.ctr[CTR_PROJ] = 0;
     c.ctr[CTR_FULL] = 0;
   }
@@ -750,25 +751,28 @@ static void run_topology(const BatchLaunch& bl, cudaStream_t s, cudaEvent_t* ev)
   const Batch& B = bl.b;
   const int G = bl.nct[MAP_G], Go = bl.nct[MAP_O];
   if (ev) cudaEventRecord(ev[0], s);
-  k_clear<D><<<G, 256, 0, s>>>(B);
-  k_touch_activate<D><<<G, 256, 0, s>>>(B);
-  k_dilate<D><<<G, 256, 0, s>>>(B);
+  const bool pdl = bl.pdl && !ev;
+  // the first kernel follows whatever preceded the substep: a plain launch
+  launch_k(false, k_clear<D>, G, 256, 0, s, B);
+  launch_k(pdl, k_touch_activate<D>, G, 256, 0, s, B);
+  launch_k(pdl, k_dilate<D>, G, 256, 0, s, B);
   if (ev) cudaEventRecord(ev[1], s);
-  if (bl.any_dynamic) k_mark_hier<D><<<G, 256, 0, s>>>(B);
-  k_resolve<D><<<G, 256, 0, s>>>(B);
+  if (bl.any_dynamic) launch_k(pdl, k_mark_hier<D>, G, 256, 0, s, B);
+  launch_k(pdl, k_resolve<D>, G, 256, 0, s, B);
   if (bl.side) {
     cudaEventRecord(bl.fork, s);
     cudaStreamWaitEvent(bl.side, bl.fork, 0);
     k_ghost_tj<D><<<G, 256, 0, bl.side>>>(B);
     cudaEventRecord(bl.join, bl.side);
   } else {
-    k_ghost_tj<D><<<G, 256, 0, s>>>(B);
+    launch_k(pdl, k_ghost_tj<D>, G, 256, 0, s, B);
   }
   if (ev) cudaEventRecord(ev[2], s);
-  k_bin<D><<<G, 256, 0, s>>>(B);
-  k_offsets<D><<<Go, 1024, 0, s>>>(B);
-  k_cell_offsets<D><<<G, 256, 0, s>>>(B);
-  k_scatter<D><<<G, 256, 0, s>>>(B);
+  // after an event record or wait the next launch is a plain one
+  launch_k(pdl && !bl.side, k_bin<D>, G, 256, 0, s, B);
+  launch_k(pdl, k_offsets<D>, Go, 1024, 0, s, B);
+  launch_k(pdl, k_cell_offsets<D>, G, 256, 0, s, B);
+  launch_k(pdl, k_scatter<D>, G, 256, 0, s, B);
   if (ev) cudaEventRecord(ev[3], s);
 }
 

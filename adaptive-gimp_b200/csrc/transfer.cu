@@ -684,9 +684,10 @@ __device__ __forceinline__ bool sur_handoff(const Ctx& c, const float* U, const 
 #pragma unroll
   for (int k = 0; k < 7; ++k) ok = ok && fabsf(x[k]) <= c.sur_xmax[k];
   if (!ok) return false;
-  const int slot = reserve_slot(&c.ctr[CTR_SUR]);
+  const int slot = reserve_slot(c.sur_ctr);
   float* meta = c.sur_meta + (long long)slot * SUR_META;
   meta[0] = __int_as_float(j);
+  meta[23] = __int_as_float(c.scene);
 #pragma unroll
   for (int k = 0; k < D * D; ++k) {
     meta[1 + k] = U[k];
@@ -721,11 +722,13 @@ __device__ __forceinline__ void snow_return_map(const Ctx& c, float* F, float& j
 // log Jp' - log Jp = sum log sig - sum log sig' by more than sur_tol (then the
 // exact return map is used), and write F and Jp.
 template <int D>
-__global__ void k_sur_finish(Ctx c) {
-  const int n = c.ctr[CTR_SUR];
+__global__ void k_sur_finish(Batch B, const float* __restrict__ meta_all, const float* __restrict__ Y,
+                             const int32_t* __restrict__ n_dev) {
+  const int n = *n_dev;
   for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < n; s += gridDim.x * blockDim.x) {
-    const float* meta = c.sur_meta + (long long)s * SUR_META;
+    const float* meta = meta_all + (long long)s * SUR_META;
     const int j = __float_as_int(meta[0]);
+    const Ctx& c = B.ctx[__float_as_int(meta[23])];  // the slot's scene
     float U[D * D], V[D * D], sg[D];
 #pragma unroll
     for (int k = 0; k < D * D; ++k) {
@@ -735,12 +738,13 @@ __global__ void k_sur_finish(Ctx c) {
 #pragma unroll
     for (int d = 0; d < D; ++d) sg[d] = meta[19 + d];
     float jp = meta[22];
-    const float* y = c.sur_Y + (long long)s * 4;
+    const float* y = Y + (long long)s * 4;
+    const float ts = c.theta_s, tcr = c.theta_c;
     float sp[D], r = 0.f, lsum = 0.f;
 #pragma unroll
     for (int d = 0; d < D; ++d) {
       sp[d] = sg[d] + SUR_DSIG * y[d];
-      r = fmaxf(r, fmaxf(sp[d] - (1.f + c.theta_s), (1.f - c.theta_c) - sp[d]));
+      r = fmaxf(r, fmaxf(sp[d] - (1.f + ts), (1.f - tcr) - sp[d]));
       lsum += logf(sg[d]) - logf(fmaxf(sp[d], 1e-6f));
     }
     const float dljp = SUR_DLJ * y[3];
@@ -762,9 +766,11 @@ __global__ void k_sur_finish(Ctx c) {
         }
     }
     const long long N = c.N;
+    float* QF = c.Q.F;
+    float* QJ = c.Q.Jp;
 #pragma unroll
-    for (int k = 0; k < D * D; ++k) __stwb(&c.Q.F[k * N + j], F[k]);
-    __stwb(&c.Q.Jp[j], jp);
+    for (int k = 0; k < D * D; ++k) __stwb(&QF[k * N + j], F[k]);
+    __stwb(&QJ[j], jp);
   }
 }
 
@@ -973,37 +979,39 @@ void prepare_transfer_kernels() {
 }
 
 template <int D>
-static void launch_p2g(const BatchLaunch& bl, cudaStream_t s) {
+static void launch_p2g(const BatchLaunch& bl, cudaStream_t s, bool pdl) {
   const int G = bl.nct[MAP_G];
   switch (bl.chunk) {
-    case 64: k_p2g<D, 64><<<G, 64, P2GLayout<D, 64>::bytes(), s>>>(bl.b); break;
-    case 128: k_p2g<D, 128><<<G, 128, P2GLayout<D, 128>::bytes(), s>>>(bl.b); break;
-    case 512: k_p2g<D, 512><<<G, 512, P2GLayout<D, 512>::bytes(), s>>>(bl.b); break;
-    default: k_p2g<D, 256><<<G, 256, P2GLayout<D, 256>::bytes(), s>>>(bl.b); break;
+    case 64: launch_k(pdl, k_p2g<D, 64>, G, 64, P2GLayout<D, 64>::bytes(), s, bl.b); break;
+    case 128: launch_k(pdl, k_p2g<D, 128>, G, 128, P2GLayout<D, 128>::bytes(), s, bl.b); break;
+    case 512: launch_k(pdl, k_p2g<D, 512>, G, 512, P2GLayout<D, 512>::bytes(), s, bl.b); break;
+    default: launch_k(pdl, k_p2g<D, 256>, G, 256, P2GLayout<D, 256>::bytes(), s, bl.b); break;
   }
 }
 
 template <int D>
 void launch_transfer(const BatchLaunch& bl, cudaStream_t s, cudaEvent_t* ev) {
   const int G = bl.nct[MAP_G];
-  launch_p2g<D>(bl, s);
+  const bool pdl = bl.pdl && !ev;
+  launch_p2g<D>(bl, s, pdl);
   if (bl.side) cudaStreamWaitEvent(s, bl.join, 0);  // k_ghost_tj's node mask
   if (ev) cudaEventRecord(ev[4], s);
-  for (int l = bl.maxL - 1; l >= 1; --l) k_restrict<D><<<G, 256, 0, s>>>(bl.b, l);
+  // the first launch after the join is a plain one
+  bool first = true;
+  for (int l = bl.maxL - 1; l >= 1; --l, first = false)
+    launch_k(pdl && !(first && bl.side), k_restrict<D>, G, 256, 0, s, bl.b, l);
   if (ev) cudaEventRecord(ev[5], s);
   // with more than one level grid_op runs inside the restriction into level 0
   // and the prolongations
-  if (bl.maxL == 1) k_gridop<D><<<G, 256, 0, s>>>(bl.b);
+  if (bl.maxL == 1) launch_k(pdl && !bl.side, k_gridop<D>, G, 256, 0, s, bl.b);
   if (ev) cudaEventRecord(ev[6], s);
-  for (int l = 1; l < bl.maxL; ++l) k_prolong<D><<<G, 256, 0, s>>>(bl.b, l);
+  for (int l = 1; l < bl.maxL; ++l) launch_k(pdl, k_prolong<D>, G, 256, 0, s, bl.b, l);
   if (ev) cudaEventRecord(ev[7], s);
-  k_g2p<D><<<G, 256, 0, s>>>(bl.b);
-  if (bl.any_plastic) k_project<D><<<G, 256, 0, s>>>(bl.b);
-  const Ctx* c = bl.single;
-  if (c && c->sur && c->plast == 1 && c->N) {
-    launch_mlp_forward_dev(c->mlp_packed, c->mlp_P, c->sur_X, c->sur_Y, c->ctr + CTR_SUR, c->N, c->ctr + CTR_ERR,
-                           c->sms, s);
-    k_sur_finish<D><<<c->sms * 8, 256, 0, s>>>(*c);
+  launch_k(pdl, k_g2p<D>, G, 256, 0, s, bl.b);
+  if (bl.any_plastic) launch_k(pdl, k_project<D>, G, 256, 0, s, bl.b);
+  if (bl.sur) {
+    launch_mlp_forward_dev(bl.mlp_packed, bl.mlp_P, bl.sur_X, bl.sur_Y, bl.sur_n, bl.sur_cap, bl.sur_err, bl.sms, s);
+    k_sur_finish<D><<<G, 256, 0, s>>>(bl.b, bl.sur_meta, bl.sur_Y, bl.sur_n);
   }
   if (ev) cudaEventRecord(ev[8], s);
 }

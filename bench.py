@@ -65,6 +65,10 @@ def parse():
                     help="snow return map through this trained surrogate (agimp.train_surrogate output); the line "
                          "then also reports the plain path's throughput and the position error against it")
     ap.add_argument("--sur-tol", type=float, default=1e-3, help="surrogate residual tolerance")
+    ap.add_argument("--snow", action="store_true",
+                    help="config 4 with config 2's snow material (each box thrown at a random velocity)")
+    ap.add_argument("--accuracy-substeps", type=int, default=1000,
+                    help="config 4 with --surrogate: substeps of the accuracy comparison against the plain batch")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default launch sizes")
     ap.add_argument("--tuning", default=None, metavar="CHUNK,CTAS_PER_SM",
                     help="fixed launch sizes instead of the autotuner (e.g. 64,16)")
@@ -508,13 +512,18 @@ def run_batch(a):
 
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
-    sc = scenes.make_batch_config(seed=rank, scale=a.scale)
+    sc = scenes.make_batch_config(seed=rank, scale=a.scale, material="snow" if a.snow else "elastic")
     dt = sc[0].dt
     n_tot = sum(s.n for s in sc)
     stream = torch.cuda.Stream()
     st = ctypes.c_void_p(stream.cuda_stream)
     sims = [s.build(device=local) for s in sc]
     batch = SceneBatch(sims)
+    mlp = None
+    if a.surrogate:
+        from agimp.surrogate import load
+        mlp, xmax = load(a.surrogate, device=local)
+        batch.set_surrogate(mlp, xmax, a.sur_tol)
     if a.tuning:
         ch, cps = (int(v) for v in a.tuning.split(","))
         batch.set_tuning(ch, cps)
@@ -556,6 +565,15 @@ def run_batch(a):
             s.substep(dt, stream=st)
 
     ms_alone = timed(one_at_a_time)
+    ms_plain_batch = None
+    if mlp is not None:
+        plain = [s.build(device=local) for s in sc]
+        pbatch = SceneBatch(plain)
+        pbatch.set_tuning(tuning["chunk"], tuning["ctas_per_sm"])
+        ms_plain_batch = timed(lambda: pbatch.substep(dt, 1, stream=st))
+        pbatch.close()
+        for s in plain:
+            s.close()
     # both runs took warmup + steps substeps; the batch ran 5 more for its profile
     for s in alone:
         with torch.cuda.stream(stream):
@@ -585,7 +603,8 @@ def run_batch(a):
         "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
         "ms_per_step": ms_max / a.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32", "data": "synthetic",
-        "config": {"workload": "config4_batched_2d", "scenes": len(sc), "particles": n_tot,
+        "config": {"workload": "config4_batched_2d" + ("_snow" if a.snow else ""), "scenes": len(sc),
+                   "particles": n_tot, "material": "snow (config 2)" if a.snow else "elastic (config 1)",
                    "levels": {str(k): levels.count(k) for k in sorted(set(levels))},
                    "particles_per_scene": [int(min(s.n for s in sc)), int(max(s.n for s in sc))],
                    "dt": dt, "parallelism": "replicas" if world > 1 else "single",
@@ -604,6 +623,10 @@ def run_batch(a):
         "clocks": clk.summary(),
         "device_errors": int(np.bitwise_or.reduce(errors)),
     }
+    if mlp is not None:
+        (ms_pb,), _ = job_totals(dist, "cuda", [ms_plain_batch], 0)
+        out["surrogate"] = batch_surrogate_report(a, sc, local, tuning, mlp, xmax, ms_max, ms_pb, ms_alone_max,
+                                                  rank == 0 and world == 1 and not a.no_cpu_baseline)
     if not a.no_e2e:
         out["e2e"] = e2e_batch(a, sc, local, tuning)
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
@@ -622,24 +645,90 @@ def run_batch(a):
         print(json.dumps(out))
 
 
+def batch_surrogate_report(a, sc, local, tuning, mlp, xmax, ms_sur, ms_plain_batch, ms_alone, cpu_leg):
+    """The batched+surrogate form against the plain forms on the same scenes.
+    Speed: device time of the timed substeps of the batch with the surrogate,
+    of the plain batch (exact return map) and of the plain scenes stepped one
+    at a time.  Accuracy: from the initial state, --accuracy-substeps
+    substeps of the surrogate batch and of the plain batch; per scene the
+    position error of the surrogate run against the plain run, relative to
+    the plain run's RMS displacement.  In the CPU leg (rank 0, one GPU) the
+    f64 oracle runs the three smallest snow scenes over the same substeps and
+    both GPU runs are compared with it (the plain run's error is the floor)."""
+    import numpy as np
+
+    from agimp.batch import SceneBatch
+    K = a.accuracy_substeps
+    dt = sc[0].dt
+    runs = {}
+    for name, use in (("surrogate", True), ("plain", False)):
+        sims = [s.build(device=local) for s in sc]
+        b = SceneBatch(sims)
+        b.set_tuning(tuning["chunk"], tuning["ctas_per_sm"])
+        if use:
+            b.set_surrogate(mlp, xmax, a.sur_tol)
+        handed = rejected = 0
+        for i in range(K):
+            b.substep(dt, 1)
+            if use and (i % 50 == 0 or i == K - 1):
+                stt = b.surrogate_stats()
+                handed += stt["handed_off"]
+                rejected += stt["rejected"]
+        runs[name] = ([s.x_p.to_numpy().astype(np.float64) for s in sims], handed, rejected,
+                      int(np.bitwise_or.reduce([s.errors() for s in sims])))
+        b.close()
+        for s in sims:
+            s.close()
+    xs, xp = runs["surrogate"][0], runs["plain"][0]
+    rel = []
+    for s, u, p in zip(sc, xs, xp):
+        if not s.n:
+            continue
+        disp = np.sqrt(((p - s.x) ** 2).sum(1).mean())
+        rel.append(float(np.sqrt(((u - p) ** 2).sum(1).mean()) / disp) if disp > 0 else 0.0)
+    rep = {
+        "weights": os.path.relpath(a.surrogate, REPO) if os.path.isabs(a.surrogate) else a.surrogate,
+        "tol": a.sur_tol,
+        "ms_per_step": ms_sur / a.steps, "plain_batch_ms_per_step": ms_plain_batch / a.steps,
+        "plain_one_at_a_time_ms_per_step": ms_alone / a.steps,
+        "speedup_vs_plain_batch": ms_plain_batch / ms_sur, "speedup_vs_plain_one_at_a_time": ms_alone / ms_sur,
+        "accuracy": {"substeps": K,
+                     "position_rel_vs_plain": {"max_over_scenes": max(rel), "median": float(np.median(rel)),
+                                               "mean": float(np.mean(rel))},
+                     "sampled_handed_off": runs["surrogate"][1], "sampled_rejected": runs["surrogate"][2],
+                     "device_errors": [runs["surrogate"][3], runs["plain"][3]]},
+    }
+    if cpu_leg:
+        import parity as PY
+        from agimp.simulator import tabulate_level_map
+        threads = os.cpu_count() or 1
+        idx = [i for i in np.argsort([s.n if s.n else 1 << 30 for s in sc])[:3] if sc[i].n]
+        vs = []
+        for i in idx:
+            s = sc[i]
+            o = PY.make_oracle(s, True, tabulate_level_map(s.grid_initializer, s.dim, s.level, s.coarsest))
+            PY.run(o, s, 0, K, threads)
+            x64 = o.particles()["x"]
+            disp = np.sqrt(((x64 - s.x) ** 2).sum(1).mean())
+
+            def err(x):
+                return float(np.sqrt(((x - x64) ** 2).sum(1).mean()) / disp)
+            vs.append({"scene": s.name, "particles": s.n, "surrogate_vs_f64": err(xs[i]), "plain_vs_f64": err(xp[i])})
+        rep["accuracy"]["vs_f64_oracle"] = vs
+    return rep
+
+
 def cpu_oracle_batch(sc, seconds, threads, steps=3):
     """The oracle stepping scenes one at a time (as the reference would), over
     as many scenes as fit the time budget (setup and one warm-up substep per
     scene untimed); returns (particle-substeps/s, substeps per scene, timed
     seconds, scenes)."""
-    import numpy as np
-
-    import oracle as O
+    import parity as PY
     from agimp.simulator import tabulate_level_map
     el, work, k = 0.0, 0, 0
     for s in sc:
-        d, n = s.dim, s.n
-        sk = s.sim_kwargs
-        o = O.Oracle(d, s.level, s.coarsest, n, gravity=tuple(sk["gravity"]) + (0.0,), E=sk["E"], nu=sk["nu"],
-                     boundary_mode=1)
-        o.set_particles(s.x, s.v, np.tile(np.eye(d), (n, 1, 1)), np.zeros((n, d, d)), s.m, s.g)
-        t, H = tabulate_level_map(s.grid_initializer, d, s.level, s.coarsest)
-        o.set_level_map(t, H)
+        n = s.n
+        o = PY.make_oracle(s, False, tabulate_level_map(s.grid_initializer, s.dim, s.level, s.coarsest))
         o.substep(s.dt, 1, threads)
         t1 = time.perf_counter()
         o.substep(s.dt, steps, threads)

@@ -347,8 +347,10 @@ agimp_status agimp_autotune(agimp_sim* s, float dt, int32_t trials, agimp_tuning
  * for all of them, and the sequence is captured as a CUDA graph.  Each
  * simulator keeps its own state and readback; stepping a batch advances all
  * of them by the same substeps, exactly as agimp_substep on each would (up to
- * the order of float additions).  The simulators must outlive the batch; the
- * surrogate return map is not available in batches of more than one. */
+ * the order of float additions).  The simulators must outlive the batch.  In a
+ * batch of several scenes the surrogate return map is the batch's own
+ * (agimp_batch_set_surrogate): the scenes' individual surrogate settings apply
+ * only when they step alone. */
 typedef struct agimp_batch agimp_batch;
 agimp_status agimp_batch_create(agimp_sim* const* sims, int32_t n, agimp_batch** out);
 agimp_status agimp_batch_destroy(agimp_batch* b);
@@ -370,6 +372,17 @@ int32_t agimp_batch_kernels_per_substep(const agimp_batch* b);
 agimp_status agimp_batch_positions_async(agimp_batch* b, float* x, void* stream);
 /* As agimp_profile_substep, for one substep of the whole batch. */
 agimp_status agimp_batch_profile_substep(agimp_batch* b, float dt, float* ms, int32_t n, void* stream);
+/* No counterpart in the reference (which has no plasticity): the surrogate
+ * return map for every snow scene of a batch of several, as
+ * agimp_set_surrogate describes for one simulator.  All scenes hand their
+ * projections to one set of slot buffers (allocated here, sized by the
+ * scenes' total particle count), so one MLP launch and one finishing kernel
+ * per substep serve the whole batch.  m == NULL switches it off. */
+agimp_status agimp_batch_set_surrogate(agimp_batch* b, const agimp_mlp* m, const float* xmax, float tol);
+/* Surrogate counts of the last substep over the batch: projections handed to
+ * the MLP, predictions rejected (exact map used), and AGIMP_ERR_WAIT in
+ * *errors if an MLP completion wait gave up.  Synchronizes the device. */
+agimp_status agimp_batch_surrogate_stats(agimp_batch* b, int64_t* handed, int64_t* rejected, uint32_t* errors);
 
 /* ---- Scene initialisers on the device.  The reference fills x_p, v_p, F_p,
  * m_p, g_p with Taichi kernels (init.py:3-32 initialize_particle,

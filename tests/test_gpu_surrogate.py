@@ -213,3 +213,47 @@ def test_trained_surrogate_against_plain():
     plain.close()
     sur.close()
     mlp.close()
+
+
+def test_batched_surrogate_matches_scenes_alone():
+    """A batch of several snow scenes with one shared surrogate (one MLP
+    launch per substep over every scene's projections) gives each scene what
+    it gets stepping alone with the same network, up to the run-to-run noise
+    of P2G's float atomics; the batch hands projections to the network."""
+    import os
+
+    from agimp.batch import SceneBatch
+    from agimp.surrogate import load
+    wpath = os.path.join(os.path.dirname(__import__("agimp").__file__), "data", "surrogate_snow.npz")
+    mlp, xmax = load(wpath)
+    scs = []
+    for u in (3.0, 4.0, 2.5):
+        sc = _scene()
+        sc.v = sc.v * np.float32(u / 3.0)
+        scs.append(sc)
+    alone = [sc.build() for sc in scs]
+    together = [sc.build() for sc in scs]
+    for s in alone:
+        s.set_surrogate(mlp, xmax, 1e-3)
+    batch = SceneBatch(together)
+    batch.set_surrogate(mlp, xmax, 1e-3)
+    handed = 0
+    steps = 60
+    for i in range(steps):
+        for k, sc in enumerate(scs):
+            if sc.refine_every and i % sc.refine_every == 0:
+                alone[k].refine_levels(sc.refine_band)
+                together[k].refine_levels(sc.refine_band)
+            alone[k].substep(sc.dt)
+        batch.substep(scs[0].dt)
+        handed += batch.surrogate_stats()["handed_off"]
+    st = batch.surrogate_stats()
+    assert st["errors"] == 0
+    assert handed > 0
+    for a, b in zip(alone, together):
+        assert a.errors() & ~2 == 0 and b.errors() & ~2 == 0
+        xa, xb = a.x_p.to_numpy(), b.x_p.to_numpy()
+        assert np.abs(xa - xb).max() <= 1e-5, np.abs(xa - xb).max()
+    batch.close()
+    for s in alone + together:
+        s.close()
