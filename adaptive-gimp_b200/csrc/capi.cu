@@ -348,6 +348,15 @@ agimp_status agimp_create(const agimp_params* p, int32_t device, agimp_sim** out
     AL(c.occ2, cells);
   }
   cudaMemset(c.nmask, 0, Vf.nblocks * per * sizeof(uint32_t));
+  for (int l = 0; l < c.L; ++l) {
+    LevelDev& V = c.lev[l];
+    if (l == c.L - 1) {
+      V.nm = c.nmask;
+    } else {
+      AL(V.nm, V.nblocks * per);
+      cudaMemset(V.nm, 0, V.nblocks * per * sizeof(uint32_t));
+    }
+  }
   AL(c.ctr, CTR_COUNT);
   cudaMemset(c.ctr, 0, CTR_COUNT * sizeof(int32_t));
   c.sur_ctr = c.ctr + CTR_SUR;  // stepping alone, the surrogate slots count here

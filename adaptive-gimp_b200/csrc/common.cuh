@@ -59,6 +59,11 @@ struct LevelDev {
   float4* node;
   int32_t* bmap;
   int32_t* blist;
+  // node mask of this level's nodes, in the level's own blocked layout
+  // (node_mask[_map(l, I)], adaptive_gimp.py:126-128): the finest level's is
+  // the node mask itself; coarser levels get a copy after ghost / T-junction
+  // marking, so the level transfers read whole blocks of it
+  uint32_t* nm;
 };
 
 struct Particles {

@@ -63,6 +63,7 @@ __global__ void k_clear(Batch B) {
     const long long idx = (blk << (2 * D)) | loc;
     V.cell[idx] = 0u;
     V.node[idx] = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (l < c.L - 1) V.nm[idx] = 0u;
     if (loc == 0) V.bmap[blk] = -1;
     int I[D];
     elem_coords<D>(V, blk, loc, I);
@@ -520,6 +521,28 @@ __global__ void k_ghost_tj(Batch B) {
 }
 
 // ---------------------------------------------------------------------------
+// Per-level node masks for the levels below the finest: node I of level l
+// gets node_mask[_map(l, I)] (adaptive_gimp.py:126-128), 0 outside [0, size].
+// Runs after ghost / T-junction marking, the last writer of the node mask.
+template <int D>
+__global__ void k_level_masks(Batch B) {
+  SCENE_CTA(B, MAP_G);
+  const long long tot = total_elems(c, 0, c.L - 1, D);
+  SCENE_LOOP(e, tot) {
+    int l, loc;
+    long long blk;
+    decode_elem<D>(c, 0, c.L - 1, e, l, blk, loc);
+    const LevelDev& V = c.lev[l];
+    int I[D];
+    elem_coords<D>(V, blk, loc, I);
+    bool inr = true;
+#pragma unroll
+    for (int d = 0; d < D; ++d) inr = inr && I[d] >= 0 && I[d] <= V.size;
+    V.nm[(blk << (2 * D)) | loc] = inr ? nm_get<D>(c, l, I) : 0u;
+  }
+}
+
+// ---------------------------------------------------------------------------
 // level_mapping (adaptive_gimp.py:189-216): fl_p = finest level with an
 // ACTIVATED cell among the 2^d cells around the particle; bin = (fl_p, block
 // of base).  Particles without a level go to one extra bin after all block
@@ -763,9 +786,11 @@ static void run_topology(const BatchLaunch& bl, cudaStream_t s, cudaEvent_t* ev)
     cudaEventRecord(bl.fork, s);
     cudaStreamWaitEvent(bl.side, bl.fork, 0);
     k_ghost_tj<D><<<G, 256, 0, bl.side>>>(B);
+    if (bl.maxL > 1) launch_k(true, k_level_masks<D>, G, 256, 0, bl.side, B);
     cudaEventRecord(bl.join, bl.side);
   } else {
     launch_k(pdl, k_ghost_tj<D>, G, 256, 0, s, B);
+    if (bl.maxL > 1) launch_k(pdl, k_level_masks<D>, G, 256, 0, s, B);
   }
   if (ev) cudaEventRecord(ev[2], s);
   // after an event record or wait the next launch is a plain one
@@ -787,7 +812,7 @@ void launch_substep(const BatchLaunch& bl, cudaStream_t s, cudaEvent_t* ev) {
 }
 
 int kernels_per_substep(const BatchLaunch& bl) {
-  const int topo = 10 - (bl.any_dynamic ? 0 : 1);
+  const int topo = 10 - (bl.any_dynamic ? 0 : 1) + (bl.maxL > 1 ? 1 : 0);
   return topo + 2 + (bl.maxL == 1 ? 1 : 0) + (bl.any_plastic ? 1 : 0) + 2 * (bl.maxL - 1);
 }
 

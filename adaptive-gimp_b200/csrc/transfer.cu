@@ -22,6 +22,7 @@
 // sums its sources) instead of the reference's scatters, so they need no
 // atomics; the set of terms and their weights are the reference's.
 #include "common.cuh"
+#include "umma.cuh"
 
 namespace agimp {
 
@@ -375,13 +376,13 @@ __global__ void __launch_bounds__(CH, 1024 / CH) k_p2g(Batch B) {
 // grid_op (adaptive_gimp.py:277-287) of node I of level l, stored at idx: an
 // activated node's momentum becomes its velocity (gravity, walls, colliders);
 // with inv_norm the other nodes with mass are divided by it.  I lies in
-// [0, size]^d.
+// [0, size]^d; the level's node mask supplies is_activated.
 template <int D>
 __device__ __forceinline__ void gridop_node(const Ctx& c, int l, const int* I, long long idx) {
   const LevelDev& V = c.lev[l];
   const float4 nd = V.node[idx];
   if (!(nd.w > 0.f)) return;
-  if (!is_activated(nm_get<D>(c, l, I))) {
+  if (!is_activated(V.nm[idx])) {
     if (c.inv_norm) V.node[idx] = make_float4(nd.x / nd.w, nd.y / nd.w, D == 3 ? nd.z / nd.w : nd.z, nd.w);
     return;
   }
@@ -419,69 +420,179 @@ __device__ __forceinline__ void gridop_node(const Ctx& c, int l, const int* I, l
 }
 
 // ---------------------------------------------------------------------------
-// grid_restriction(l) as a gather over coarse nodes K of level l-1: the
-// restricted sum onto node K (stored at blk, loc)
+// Level transfers staged through shared memory by the TMA engine.  A CTA takes
+// one destination block at a time; one thread issues bulk copies
+// (cp.async.bulk, global -> shared, completion counted in bytes on an
+// mbarrier) of the source level's node blocks and node-mask blocks the
+// destination block reads, every thread waits on the mbarrier (bounded), and
+// the gather then reads shared memory only.  Blocks are contiguous in HBM
+// (PER nodes of 16 B, PER masks of 4 B), so every copy is one aligned run.
 template <int D>
-__device__ __forceinline__ void restrict_node(const Ctx& c, int l, const int* K, const LevelDev& Vc,
-                                              const LevelDev& Vf, long long blk, int loc, int lsz) {
-  float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
-  bool any = false;
-#pragma unroll
-  for (int a = 0; a < ((D == 2) ? 9 : 27); ++a) {
-    int I[D], nrm = 0;
-    int t = a;
-    bool ok = true;
-#pragma unroll
-    for (int d = D - 1; d >= 0; --d) {
-      const int dI = t % 3 - 1;
-      t /= 3;
-      I[d] = 2 * K[d] - dI;
-      nrm += dI != 0;
-      ok = ok && I[d] >= 0 && I[d] <= lsz;
-    }
-    if (!ok) continue;
-    const uint32_t nm = nm_get<D>(c, l, I);
-    if (!((is_activated(nm) && nrm == 0) || is_tj(nm) || is_ghost(nm))) continue;
-    const float w = (nrm == 0) ? 1.f : (nrm == 1) ? 0.5f : (nrm == 2) ? 0.25f : 0.125f;
-    const float4 f = Vf.node[elem_of<D>(Vf, I)];
-    acc.x += f.x * w;
-    acc.y += f.y * w;
-    acc.z += f.z * w;
-    acc.w += f.w * w;
-    any = true;
-  }
-  if (!any) return;
-  float4* dst = &Vc.node[(blk << (2 * D)) | loc];
-  float4 o = *dst;
-  o.x += acc.x;
-  o.y += acc.y;
-  o.z += acc.z;
-  o.w += acc.w;
-  *dst = o;
+struct Stage {
+  static constexpr int PER = 1 << (2 * D);
+  static constexpr uint32_t NODE_BYTES = PER * 16, MASK_BYTES = PER * 4;
+};
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* m, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(umma::smem_u32(m)), "r"(bytes)
+               : "memory");
 }
 
-// The last restriction (into level 0) also applies grid_op to level 0, whose
-// momentum no later pass reads; in a scene of one level it only does that.
+__device__ __forceinline__ void bulk_to_shared(void* dst, const void* src, uint32_t bytes, uint64_t* m) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   umma::smem_u32(dst)),
+               "l"(src), "r"(bytes), "r"(umma::smem_u32(m))
+               : "memory");
+}
+
+// Wait for the staged copies of this phase.  When the bounded wait gives up,
+// the CTA records ERR_MLP (a bounded device wait gave up), waits once more
+// (bounded) for its copies in flight and returns false.
+__device__ __forceinline__ bool stage_wait(const Ctx& c, uint64_t* m, uint32_t phase) {
+  if (umma::mbar_wait(m, phase)) return true;
+  if (threadIdx.x == 0) set_err(c, ERR_MLP);
+  umma::mbar_wait(m, phase);
+  return false;
+}
+
+__device__ __forceinline__ void stage_init(uint64_t* m) {
+  if (threadIdx.x == 0) {
+    umma::mbar_init(m, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+}
+
+// stored block coordinates of linear block index b (first axis slowest)
 template <int D>
-__global__ void k_restrict(Batch B, int l) {
+__device__ __forceinline__ void block_coords(unsigned b, unsigned nb, int* Bc) {
+#pragma unroll
+  for (int d = D - 1; d >= 0; --d) {
+    Bc[d] = (int)(b % nb);
+    b /= nb;
+  }
+}
+
+// grid_restriction(l) (adaptive_gimp.py:289-301) as a gather over the coarse
+// nodes K of level l-1: the restricted sum onto K of the fine nodes 2K - dI
+// that are (activated and even), T-junctions or ghosts, weight 0.5^|dI|_1.
+// The fine nodes of a coarse block lie in the 3^d fine blocks 2B-2 .. 2B (B:
+// the coarse block's stored coordinates).  The last restriction (into level
+// 0) also applies grid_op to level 0, whose momentum no later pass reads; in a
+// scene of one level it only does that.
+template <int D>
+__global__ void __launch_bounds__(Stage<D>::PER) k_restrict(Batch B, int l) {
   SCENE_CTA(B, MAP_G);
+  using S = Stage<D>;
+  constexpr int NB = (D == 2) ? 9 : 27;
+  __shared__ __align__(128) float4 fn[NB][S::PER];
+  __shared__ __align__(128) uint32_t fm[NB][S::PER];
+  __shared__ int fok[NB];
+  __shared__ __align__(8) uint64_t mbar;
   const bool restrict_l = l < c.L;
   if (!restrict_l && l != 1) return;
   const LevelDev& Vc = c.lev[l - 1];
   const LevelDev& Vf = c.lev[restrict_l ? l : l - 1];
-  const long long tot = (long long)c.ctr[CTR_LEVEL + l - 1] << (2 * D);
+  const int nblk = c.ctr[CTR_LEVEL + l - 1];
   const int lsz = Vf.size, l0sz = Vc.size;
-  SCENE_LOOP(e, tot) {
-    const long long blk = Vc.blist[e >> (2 * D)];
-    const int loc = (int)(e & ((1 << (2 * D)) - 1));
+  const int loc = threadIdx.x;
+  stage_init(&mbar);
+  uint32_t phase = 0;
+  for (int bi = bid_; bi < nblk; bi += nblk_) {
+    const unsigned blk = (unsigned)Vc.blist[bi];
+    int Bc[D];
+    block_coords<D>(blk, (unsigned)Vc.nb, Bc);
+    if (restrict_l) {
+      if (threadIdx.x == 0) {
+        uint32_t bytes = 0;
+        for (int t = 0; t < NB; ++t) {
+          bool ok = true;
+          unsigned fb = 0;
+          int tt = t, fc[D];
+#pragma unroll
+          for (int d = D - 1; d >= 0; --d) {
+            fc[d] = 2 * Bc[d] - 2 + tt % 3;
+            tt /= 3;
+            ok = ok && fc[d] >= 0 && fc[d] < Vf.nb;
+          }
+#pragma unroll
+          for (int d = 0; d < D; ++d) fb = fb * (unsigned)Vf.nb + (unsigned)fc[d];
+          fok[t] = ok ? (int)fb : -1;
+          if (ok) bytes += S::NODE_BYTES + S::MASK_BYTES;
+        }
+        // earlier generic reads of the tile finished at the barrier that
+        // ended the previous block; order them before the async writes
+        umma::fence_proxy_async();
+        mbar_expect_tx(&mbar, bytes);
+        for (int t = 0; t < NB; ++t)
+          if (fok[t] >= 0) {
+            bulk_to_shared(fn[t], Vf.node + ((long long)fok[t] << (2 * D)), S::NODE_BYTES, &mbar);
+            bulk_to_shared(fm[t], Vf.nm + ((long long)fok[t] << (2 * D)), S::MASK_BYTES, &mbar);
+          }
+      }
+      __syncthreads();  // fok
+      const bool ok = stage_wait(c, &mbar, phase);
+      phase ^= 1;
+      if (!ok) return;
+    }
     int K[D];
-    elem_coords<D>(Vc, blk, loc, K);
+#pragma unroll
+    for (int d = D - 1, t = loc; d >= 0; --d, t >>= 2) K[d] = ((Bc[d] - 1) << 2) + (t & 3);
     bool inr = true;
 #pragma unroll
     for (int d = 0; d < D; ++d) inr = inr && K[d] >= 0 && K[d] <= l0sz;
-    if (!inr) continue;
-    if (restrict_l && is_valid(nm_get<D>(c, l - 1, K))) restrict_node<D>(c, l, K, Vc, Vf, blk, loc, lsz);
-    if (l == 1) gridop_node<D>(c, 0, K, (blk << (2 * D)) | loc);
+    const long long cidx = ((long long)blk << (2 * D)) | loc;
+    if (inr && restrict_l && is_valid(Vc.nm[cidx])) {
+      float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
+      bool any = false;
+#pragma unroll
+      for (int a = 0; a < ((D == 2) ? 9 : 27); ++a) {
+        int t = a, nrm = 0, tile = 0, li = 0;
+        bool okI = true;
+#pragma unroll
+        for (int d = D - 1; d >= 0; --d) {
+          const int dI = t % 3 - 1;
+          t /= 3;
+          const int I = 2 * K[d] - dI;
+          nrm += dI != 0;
+          okI = okI && I >= 0 && I <= lsz;
+        }
+        if (!okI) continue;
+        // tile and local index of fine node 2K - dI
+        t = a;
+        int mul = 1, lmul = 1;
+#pragma unroll
+        for (int d = D - 1; d >= 0; --d) {
+          const int dI = t % 3 - 1;
+          t /= 3;
+          const int q = 2 * K[d] - dI + HALO;
+          tile += ((q >> 2) - (2 * Bc[d] - 2)) * mul;
+          li += (q & 3) * lmul;
+          mul *= 3;
+          lmul *= 4;
+        }
+        if (fok[tile] < 0) continue;
+        const uint32_t nm = fm[tile][li];
+        if (!((is_activated(nm) && nrm == 0) || is_tj(nm) || is_ghost(nm))) continue;
+        const float w = (nrm == 0) ? 1.f : (nrm == 1) ? 0.5f : (nrm == 2) ? 0.25f : 0.125f;
+        const float4 f = fn[tile][li];
+        acc.x += f.x * w;
+        acc.y += f.y * w;
+        acc.z += f.z * w;
+        acc.w += f.w * w;
+        any = true;
+      }
+      if (any) {
+        float4 o = Vc.node[cidx];
+        o.x += acc.x;
+        o.y += acc.y;
+        o.z += acc.z;
+        o.w += acc.w;
+        Vc.node[cidx] = o;
+      }
+    }
+    if (inr && l == 1) gridop_node<D>(c, 0, K, cidx);
+    __syncthreads();  // the tile is free for the next block's copies
   }
 }
 
@@ -508,79 +619,137 @@ __global__ void k_gridop(Batch B) {
 }
 
 // ---------------------------------------------------------------------------
-// grid_prolongation(l) as a gather over fine nodes J of level l: T-junction
-// and ghost nodes take the weighted sum of their valid coarse neighbours,
-// other all-even nodes take the coincident coarse velocity if they are
-// activated and it is valid, else 0; the rest keep their value.
+// grid_prolongation(l) (adaptive_gimp.py:303-321) as a gather over the fine
+// nodes J of level l: T-junction and ghost nodes take the weighted sum of
+// their valid coarse neighbours, other all-even nodes take the coincident
+// coarse velocity if they are activated and it is valid, else 0; the rest keep
+// their value.  The coarse nodes of a fine block B lie in the 2^d coarse
+// blocks (2B + 1) / 4 .. (2B + 1) / 4 + 1 per axis, staged like the
+// restriction's.  Level l's grid_op runs first on each node: its momentum is
+// no longer read (the restrictions are done) and its coarser neighbour is
+// final.
 template <int D>
-__global__ void k_prolong(Batch B, int l) {
+__global__ void __launch_bounds__(Stage<D>::PER) k_prolong(Batch B, int l) {
   SCENE_CTA(B, MAP_G);
+  using S = Stage<D>;
+  constexpr int NB = 1 << D;
+  __shared__ __align__(128) float4 cn[NB][S::PER];
+  __shared__ __align__(128) uint32_t cm[NB][S::PER];
+  __shared__ int cok[NB];
+  __shared__ __align__(8) uint64_t mbar;
   if (l >= c.L) return;
   const LevelDev& Vc = c.lev[l - 1];
   const LevelDev& Vf = c.lev[l];
-  const long long tot = (long long)c.ctr[CTR_LEVEL + l] << (2 * D);
+  const int nblk = c.ctr[CTR_LEVEL + l];
   const int lsz = Vf.size;
-  SCENE_LOOP(e, tot) {
-    const long long blk = Vf.blist[e >> (2 * D)];
-    const int loc = (int)(e & ((1 << (2 * D)) - 1));
+  const int loc = threadIdx.x;
+  stage_init(&mbar);
+  uint32_t phase = 0;
+  for (int bi = bid_; bi < nblk; bi += nblk_) {
+    const unsigned blk = (unsigned)Vf.blist[bi];
+    int Bf[D], C0[D];
+    block_coords<D>(blk, (unsigned)Vf.nb, Bf);
+#pragma unroll
+    for (int d = 0; d < D; ++d) C0[d] = (2 * Bf[d] + 1) >> 2;
+    if (threadIdx.x == 0) {
+      uint32_t bytes = 0;
+      for (int t = 0; t < NB; ++t) {
+        bool ok = true;
+        unsigned cb = 0;
+#pragma unroll
+        for (int d = 0; d < D; ++d) {
+          const int q = C0[d] + ((t >> (D - 1 - d)) & 1);
+          ok = ok && q < Vc.nb;
+          cb = cb * (unsigned)Vc.nb + (unsigned)q;
+        }
+        cok[t] = ok ? (int)cb : -1;
+        if (ok) bytes += S::NODE_BYTES + S::MASK_BYTES;
+      }
+      umma::fence_proxy_async();
+      mbar_expect_tx(&mbar, bytes);
+      for (int t = 0; t < NB; ++t)
+        if (cok[t] >= 0) {
+          bulk_to_shared(cn[t], Vc.node + ((long long)cok[t] << (2 * D)), S::NODE_BYTES, &mbar);
+          bulk_to_shared(cm[t], Vc.nm + ((long long)cok[t] << (2 * D)), S::MASK_BYTES, &mbar);
+        }
+    }
+    __syncthreads();  // cok
+    const bool okw = stage_wait(c, &mbar, phase);
+    phase ^= 1;
+    if (!okw) return;
     int J[D];
-    elem_coords<D>(Vf, blk, loc, J);
+#pragma unroll
+    for (int d = D - 1, t = loc; d >= 0; --d, t >>= 2) J[d] = ((Bf[d] - 1) << 2) + (t & 3);
     bool inr = true, even = true;
 #pragma unroll
     for (int d = 0; d < D; ++d) {
       inr = inr && J[d] >= 0 && J[d] <= lsz;
       even = even && (J[d] & 1) == 0;
     }
-    if (!inr) continue;
-    // this level's grid_op first: level l's momentum is no longer read (the
-    // restrictions are done) and its coarser neighbour is final
-    gridop_node<D>(c, l, J, (blk << (2 * D)) | loc);
-    const uint32_t nm = nm_get<D>(c, l, J);
-    const bool tg = is_tj(nm) || is_ghost(nm);
-    if (!tg && !even) continue;
-    float acc[3] = {0.f, 0.f, 0.f};
-    if (tg) {
-      int nodd = 0;
+    const long long fidx = ((long long)blk << (2 * D)) | loc;
+    if (inr) {
+      gridop_node<D>(c, l, J, fidx);
+      const uint32_t nm = Vf.nm[fidx];
+      const bool tg = is_tj(nm) || is_ghost(nm);
+      if (tg || even) {
+        // coarse node K: staged tile and local index
+        auto coarse = [&](const int* K, float4& v) -> bool {
+          int tile = 0, li = 0;
 #pragma unroll
-      for (int d = 0; d < D; ++d) nodd += J[d] & 1;
-      const float w = (nodd == 0) ? 1.f : (nodd == 1) ? 0.5f : (nodd == 2) ? 0.25f : 0.125f;
+          for (int d = 0; d < D; ++d) {
+            const int q = K[d] + HALO;
+            tile = tile * 2 + ((q >> 2) - C0[d]);
+            li = li * 4 + (q & 3);
+          }
+          if (cok[tile] < 0 || !is_valid(cm[tile][li])) return false;
+          v = cn[tile][li];
+          return true;
+        };
+        float acc[3] = {0.f, 0.f, 0.f};
+        if (tg) {
+          int nodd = 0;
 #pragma unroll
-      for (int a = 0; a < (1 << D); ++a) {
-        int K[D];
-        bool use = true;
+          for (int d = 0; d < D; ++d) nodd += J[d] & 1;
+          const float w = (nodd == 0) ? 1.f : (nodd == 1) ? 0.5f : (nodd == 2) ? 0.25f : 0.125f;
 #pragma unroll
-        for (int d = 0; d < D; ++d) {
-          const int bit = (a >> d) & 1;
-          if (J[d] & 1)
-            K[d] = (J[d] - 1) / 2 + bit;
-          else {
-            K[d] = J[d] / 2;
-            use = use && bit == 0;
+          for (int a = 0; a < (1 << D); ++a) {
+            int K[D];
+            bool use = true;
+#pragma unroll
+            for (int d = 0; d < D; ++d) {
+              const int bit = (a >> d) & 1;
+              if (J[d] & 1)
+                K[d] = (J[d] - 1) / 2 + bit;
+              else {
+                K[d] = J[d] / 2;
+                use = use && bit == 0;
+              }
+            }
+            float4 cv;
+            if (!use || !coarse(K, cv)) continue;
+            acc[0] += cv.x * w;
+            acc[1] += cv.y * w;
+            acc[2] += cv.z * w;
+          }
+        } else if (is_activated(nm)) {
+          int K[D];
+#pragma unroll
+          for (int d = 0; d < D; ++d) K[d] = J[d] / 2;
+          float4 cv;
+          if (coarse(K, cv)) {
+            acc[0] = cv.x;
+            acc[1] = cv.y;
+            acc[2] = cv.z;
           }
         }
-        if (!use || !is_valid(nm_get<D>(c, l - 1, K))) continue;
-        const float4 cv = Vc.node[elem_of<D>(Vc, K)];
-        acc[0] += cv.x * w;
-        acc[1] += cv.y * w;
-        acc[2] += cv.z * w;
-      }
-    } else if (is_activated(nm)) {
-      int K[D];
-#pragma unroll
-      for (int d = 0; d < D; ++d) K[d] = J[d] / 2;
-      if (is_valid(nm_get<D>(c, l - 1, K))) {
-        const float4 cv = Vc.node[elem_of<D>(Vc, K)];
-        acc[0] = cv.x;
-        acc[1] = cv.y;
-        acc[2] = cv.z;
+        float4 o = Vf.node[fidx];
+        o.x = acc[0];
+        o.y = acc[1];
+        o.z = acc[2];
+        Vf.node[fidx] = o;
       }
     }
-    float4* dst = &Vf.node[(blk << (2 * D)) | loc];
-    float4 o = *dst;
-    o.x = acc[0];
-    o.y = acc[1];
-    o.z = acc[2];
-    *dst = o;
+    __syncthreads();  // the tile is free for the next block's copies
   }
 }
 
@@ -999,13 +1168,13 @@ void launch_transfer(const BatchLaunch& bl, cudaStream_t s, cudaEvent_t* ev) {
   // the first launch after the join is a plain one
   bool first = true;
   for (int l = bl.maxL - 1; l >= 1; --l, first = false)
-    launch_k(pdl && !(first && bl.side), k_restrict<D>, G, 256, 0, s, bl.b, l);
+    launch_k(pdl && !(first && bl.side), k_restrict<D>, G, Stage<D>::PER, 0, s, bl.b, l);
   if (ev) cudaEventRecord(ev[5], s);
   // with more than one level grid_op runs inside the restriction into level 0
   // and the prolongations
   if (bl.maxL == 1) launch_k(pdl && !bl.side, k_gridop<D>, G, 256, 0, s, bl.b);
   if (ev) cudaEventRecord(ev[6], s);
-  for (int l = 1; l < bl.maxL; ++l) launch_k(pdl, k_prolong<D>, G, 256, 0, s, bl.b, l);
+  for (int l = 1; l < bl.maxL; ++l) launch_k(pdl, k_prolong<D>, G, Stage<D>::PER, 0, s, bl.b, l);
   if (ev) cudaEventRecord(ev[7], s);
   launch_k(pdl, k_g2p<D>, G, 256, 0, s, bl.b);
   if (bl.any_plastic) launch_k(pdl, k_project<D>, G, 256, 0, s, bl.b);

@@ -82,11 +82,11 @@ def test_batch_matches_scenes_stepped_alone():
             assert np.abs(a["x"] - b["x"]).max() <= 1e-5, (k, np.abs(a["x"] - b["x"]).max())
             assert np.abs(a["v"] - b["v"]).max() <= 1e-3 * max(1.0, np.abs(a["v"]).max())
         assert together[k].stats()["substeps"] == steps
-    # 10 topology and binning kernels (k_mark_hier included: one scene is
+    # 11 topology and binning kernels (k_mark_hier and the level masks included: one scene is
     # dynamic), P2G, G2P, the return map (one scene has snow plasticity), and
     # a restriction and a prolongation per level above 0 (grid_op runs inside
     # them)
-    assert batch.kernels_per_substep() == 10 + 3 + 2 * (max(s.level for s in sc) - 1)
+    assert batch.kernels_per_substep() == 11 + 3 + 2 * (max(s.level for s in sc) - 1)
     batch.close()
     for s in alone + together:
         s.close()
@@ -167,7 +167,9 @@ def test_autotune_restores_state_and_batch_autotune():
         s.close()
 
 
-def test_batch_rejects_surrogate_and_mixed_dims():
+def test_batch_rejects_mixed_dims_and_uses_its_own_surrogate_setting():
+    """A scene's own surrogate setting applies when it steps alone; in a batch
+    of several the batch's setting (agimp_batch_set_surrogate) applies."""
     from agimp import AgimpError, scenes
     from agimp.batch import SceneBatch
     from agimp.surrogate import MLP
@@ -181,8 +183,10 @@ def test_batch_rejects_surrogate_and_mixed_dims():
     batch = SceneBatch([a, b])
     mlp = MLP()
     a.set_surrogate(mlp, xmax=np.ones(7, np.float32), tol=0.1)
+    batch.substep(5e-5)  # the scene's own setting is not the batch's
+    assert batch.surrogate_stats()["handed_off"] == 0
     with pytest.raises(AgimpError):
-        batch.substep(5e-5)
+        batch.set_surrogate(mlp, xmax=np.ones(7, np.float32), tol=0.0)
     a.set_surrogate(None)
     batch.substep(5e-5)
     batch.close()
