@@ -103,7 +103,8 @@ def load(path: str | None = None):
     global _lib
     if _lib is not None:
         return _lib
-    path = path or LIB_PATH
+    # AGIMP_LIBRARY: another build of the library (comparing builds)
+    path = path or os.environ.get("AGIMP_LIBRARY") or LIB_PATH
     if not os.path.exists(path):
         from . import build as _build
         _build.build()

@@ -653,6 +653,22 @@ __host__ __device__ __forceinline__ bool singular_values_within(const float* F, 
   return true;
 }
 
+// singular_values_within for a matrix given by its Gram matrix S = F^T F
+// (upper entries, row by row: 2D s00 s01 s11, 3D s00 s01 s02 s11 s12 s22) and
+// its determinant: the same Gershgorin test.
+template <int D>
+__host__ __device__ __forceinline__ bool gram_within(const float* S, float detF, float lo, float hi) {
+  if (!(detF > 0.f)) return false;
+  const float lo2 = lo * lo, hi2 = hi * hi;
+  if (D == 2) {
+    const float r = fabsf(S[1]);
+    return S[0] - r >= lo2 && S[0] + r <= hi2 && S[2] - r >= lo2 && S[2] + r <= hi2;
+  }
+  const float r0 = fabsf(S[1]) + fabsf(S[2]), r1 = fabsf(S[1]) + fabsf(S[4]), r2 = fabsf(S[2]) + fabsf(S[4]);
+  return S[0] - r0 >= lo2 && S[0] + r0 <= hi2 && S[3] - r1 >= lo2 && S[3] + r1 <= hi2 && S[5] - r2 >= lo2 &&
+         S[5] + r2 <= hi2;
+}
+
 // GIMP weights factorised per axis.  get_weight_stencil (adaptive_gimp.py:
 // 218-228) sums get_linear_weight (utils.py:18-42) over the 2^d cells dI and
 // 2^d corners cell_ that meet at node n = dI + cell_; the summand is a product

@@ -316,9 +316,13 @@ __global__ void k_dilate(Batch B) {
   // (2R_l + 1)^d neighbourhood at every level
   const int lane = threadIdx.x & 31;
   const int wid = bid_ * (blockDim.x >> 5) + (threadIdx.x >> 5), nw = nblk_ * (blockDim.x >> 5);
+  // (touched block, level) pairs go to separate warps, so a block's levels
+  // are dilated concurrently; level L works the static-map lookups
   const LevelDev& Vf = c.lev[c.L - 1];
   const int ntouch = c.ctr[CTR_TOUCH];
-  for (int t = wid; t < ntouch; t += nw) {
+  const int nlev = c.L + (c.is_static ? 1 : 0);
+  for (int u = wid; u < ntouch * nlev; u += nw) {
+    const int t = u / nlev, l = u - t * nlev;
     const int key = c.touch_list[t];
     const unsigned reach = c.touch_flag[key];
     int fb[D];
@@ -328,7 +332,11 @@ __global__ void k_dilate(Batch B) {
       fb[d] = (int)(k % (unsigned)Vf.nb) - 1;
       k /= (unsigned)Vf.nb;
     }
-    for (int l = 0; l < c.L; ++l) {
+    if (l == c.L) {
+      static_window<D>(c, key, fb, lane);
+      continue;
+    }
+    {
       const int R = dilate_radius(c, l, reach);
       const int w = 2 * R + 1;
       const int items = (D == 2) ? w * w : w * w * w;
@@ -356,7 +364,6 @@ __global__ void k_dilate(Batch B) {
         }
       }
     }
-    if (c.is_static) static_window<D>(c, key, fb, lane);
   }
 }
 

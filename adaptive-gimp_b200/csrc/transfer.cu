@@ -1004,9 +1004,27 @@ __device__ __forceinline__ void g2p_one(const Ctx& c, int j) {
   // Gather by rows along the last axis: the weights are products of per-axis
   // terms, so a row's nodes are first summed with the last axis's weight (S)
   // and gradient (T), and the other axes' factors are applied once per row.
-  float W[D][3], Gw[D][3];
-#pragma unroll
-  for (int d = 0; d < D; ++d) axis_weights(tc[d], c.radius, W[d], Gw[d]);
+  // Only the last axis's factors are kept; the others are formed when their
+  // row starts (closed form for radius 1/2), which keeps G2P inside 64
+  // registers with a slab of nodes in flight.
+  const bool half = c.radius == 0.5f;
+  float W2[3], G2[3];
+  if (half)
+    axis_weights_half(tc[D - 1], W2, G2);
+  else
+    axis_weights(tc[D - 1], c.radius, W2, G2);
+  auto axis_factor = [&](float t, int k, float& w, float& g) {
+    if (half) {
+      const float a = 0.5f - t, b = 0.5f + t;
+      w = k == 0 ? a * a : (k == 1 ? fmaf(-2.f * t, t, 1.5f) : b * b);
+      g = k == 0 ? -a : (k == 1 ? -2.f * t : b);
+    } else {
+      float Wk[3], Gk[3];
+      axis_weights(t, c.radius, Wk, Gk);
+      w = k == 0 ? Wk[0] : (k == 1 ? Wk[1] : Wk[2]);
+      g = k == 0 ? Gk[0] : (k == 1 ? Gk[1] : Gk[2]);
+    }
+  };
   const float r2 = 2.f * c.radius;
   const float kw = (D == 2) ? 1.f / (4.f * r2 * r2) : 1.f / (8.f * r2 * r2 * r2);
   const float kg = (D == 2) ? 1.f / (2.f * r2 * r2) : 1.f / (4.f * r2 * r2 * r2);
@@ -1015,12 +1033,10 @@ __device__ __forceinline__ void g2p_one(const Ctx& c, int j) {
   for (int i = 0; i < D; ++i) nv[i] = 0.f;
 #pragma unroll
   for (int i = 0; i < D * D; ++i) G[i] = 0.f;
-  // 3D: one x-slab of 3 rows (9 nodes) at a time keeps fewer gathers in
-  // flight, so G2P fits in 64 registers (4 CTAs per SM)
 #pragma unroll(D == 3 ? 1 : 3)
   for (int n0 = 0; n0 < 3; ++n0) {
-    const float w0 = n0 == 0 ? W[0][0] : (n0 == 1 ? W[0][1] : W[0][2]);
-    const float g0 = n0 == 0 ? Gw[0][0] : (n0 == 1 ? Gw[0][1] : Gw[0][2]);
+    float w0, g0;
+    axis_factor(tc[0], n0, w0, g0);
 #pragma unroll
     for (int n1 = 0; n1 < ((D == 2) ? 1 : 3); ++n1) {
       float S[D], T[D];
@@ -1037,8 +1053,8 @@ __device__ __forceinline__ void g2p_one(const Ctx& c, int j) {
         const float gv[3] = {nd.x, nd.y, nd.z};
 #pragma unroll
         for (int i = 0; i < D; ++i) {
-          S[i] += gv[i] * W[D - 1][k];
-          T[i] += gv[i] * Gw[D - 1][k];
+          S[i] += gv[i] * W2[k];
+          T[i] += gv[i] * G2[k];
         }
       }
       // row factors: weight, and the gradient components of the other axes
@@ -1048,10 +1064,12 @@ __device__ __forceinline__ void g2p_one(const Ctx& c, int j) {
         cg[0] = g0 * kg;
         cg[1] = w0 * kg;
       } else {
-        const float wxy = w0 * W[1][n1];
+        float w1, g1;
+        axis_factor(tc[1], n1, w1, g1);
+        const float wxy = w0 * w1;
         cw = wxy * kw;
-        cg[0] = g0 * W[1][n1] * kg;
-        cg[1] = w0 * Gw[1][n1] * kg;
+        cg[0] = g0 * w1 * kg;
+        cg[1] = w0 * g1 * kg;
         cg[D - 1] = wxy * kg;
       }
 #pragma unroll
@@ -1070,37 +1088,51 @@ __device__ __forceinline__ void g2p_one(const Ctx& c, int j) {
   }
 #pragma unroll
   for (int i = 0; i < D * D; ++i) __stwb(&c.Q.C[i * N + j], G[i]);
-  // the rest of the particle is loaded only now (fewer live registers
-  // during the gather)
+  // the rest of the particle is read only now (fewer live registers during
+  // the gather); m, g, id and Jp travel unchanged
+  __stwb(&c.Q.m[j], __ldg(&c.P.m[p]));
+  __stwb(&c.Q.g[j], __ldg(&c.P.g[p]));
+  __stwb(&c.Q.id[j], __ldg(&c.P.id[p]));
+  __stwb(&c.Q.Jp[j], c.plast == 1 ? __ldg(&c.P.Jp[p]) : 1.f);
+  __stwb(&c.Q.fl[j], l);
   float F[D * D];
 #pragma unroll
   for (int k = 0; k < D * D; ++k) F[k] = __ldg(&c.P.F[k * N + p]);
-  const float mp = __ldg(&c.P.m[p]);
-  const int gp = __ldg(&c.P.g[p]);
-  const int idp = __ldg(&c.P.id[p]);
-  float jp = c.plast == 1 ? __ldg(&c.P.Jp[p]) : 1.f;
   const float s = (c.dt * pw) / (rd * dx);
-  float Fn[D * D];
+  // F' = (I + s G) F row by row, each row stored at once; the Gram matrix
+  // F'^T F' is summed from the rows for the return-map test below
+  float Sg[(D == 2) ? 3 : 6];
 #pragma unroll
-  for (int i = 0; i < D; ++i)
+  for (int k = 0; k < ((D == 2) ? 3 : 6); ++k) Sg[k] = 0.f;
+#pragma unroll
+  for (int i = 0; i < D; ++i) {
+    float row[D];
 #pragma unroll
     for (int q = 0; q < D; ++q) {
       float a = 0.f;
 #pragma unroll
       for (int k = 0; k < D; ++k) a += ((i == k ? 1.f : 0.f) + s * G[i * D + k]) * F[k * D + q];
-      Fn[i * D + q] = a;
+      row[q] = a;
+      __stwb(&c.Q.F[(i * D + q) * N + j], a);
     }
-  // trial states that may leave the elastic interval get the return map in
-  // k_project (it needs an SVD, whose registers would halve G2P's occupancy)
-  if (c.plast == 1 && !singular_values_within<D>(Fn, 1.f - c.theta_c, 1.f + c.theta_s))
-    c.proj[reserve_slot(&c.ctr[CTR_PROJ])] = j;
+    int u = 0;
 #pragma unroll
-  for (int i = 0; i < D * D; ++i) __stwb(&c.Q.F[i * N + j], Fn[i]);
-  __stwb(&c.Q.m[j], mp);
-  __stwb(&c.Q.Jp[j], jp);
-  __stwb(&c.Q.g[j], gp);
-  __stwb(&c.Q.id[j], idp);
-  __stwb(&c.Q.fl[j], l);
+    for (int a = 0; a < D; ++a)
+#pragma unroll
+      for (int b = a; b < D; ++b) Sg[u++] += row[a] * row[b];
+  }
+  // trial states that may leave the elastic interval get the return map in
+  // k_project (it needs an SVD, whose registers would halve G2P's occupancy);
+  // det F' = det(I + s G) det F
+  if (c.plast == 1) {
+    float A[D * D];
+#pragma unroll
+    for (int i = 0; i < D; ++i)
+#pragma unroll
+      for (int k = 0; k < D; ++k) A[i * D + k] = (i == k ? 1.f : 0.f) + s * G[i * D + k];
+    if (!gram_within<D>(Sg, det<D>(A) * det<D>(F), 1.f - c.theta_c, 1.f + c.theta_s))
+      c.proj[reserve_slot(&c.ctr[CTR_PROJ])] = j;
+  }
 }
 
 template <int D>
