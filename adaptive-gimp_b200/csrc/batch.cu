@@ -147,16 +147,19 @@ static agimp_status build_maps(agimp_batch* b, cudaStream_t use) {
   const long long G = (long long)b->sms * b->tune.ctas_per_sm;
   int* Gm = b->hofs.data() + MAP_G * (n + 1);
   int* O = b->hofs.data() + MAP_O * (n + 1);
-  Gm[0] = O[0] = 0;
+  int* T = b->hofs.data() + MAP_T * (n + 1);
+  Gm[0] = O[0] = T[0] = 0;
   for (int i = 0; i < n; ++i) {
     const long long N = b->sims[i]->c.N;
     const int cg = n == 1 ? (int)std::max<long long>(1, G)
                           : (int)std::max<long long>(1, sumN ? (long long)std::llround((double)G * N / sumN) : 1);
     Gm[i + 1] = Gm[i] + cg;
     O[i + 1] = O[i] + std::max(1, cg / 4);
+    T[i + 1] = T[i] + 4 * cg;
   }
   b->nct[MAP_G] = Gm[n];
   b->nct[MAP_O] = O[n];
+  b->nct[MAP_T] = T[n];
   BCK(cudaMemcpyAsync(b->dofs, b->hofs.data(), sizeof(int) * b->hofs.size(), cudaMemcpyHostToDevice, use));
   b->maps_valid = true;
   return AGIMP_OK;

@@ -715,7 +715,8 @@ __host__ __device__ __forceinline__ void axis_weights_half(float t, float* W, fl
 // over the range starts and copies the scene's context into shared memory.
 enum { MAP_G = 0,  // grid-stride kernels over particles, active blocks or work items
        MAP_O = 1,  // bin allocation (1024-thread CTAs)
-       NMAP = 2 };
+       MAP_T = 2,  // staged level transfers (one 4^d block per CTA at a time: 4x MAP_G's CTAs)
+       NMAP = 3 };
 
 struct Batch {
   const Ctx* ctx;  // [n] scene contexts in device memory

@@ -482,7 +482,7 @@ __device__ __forceinline__ void block_coords(unsigned b, unsigned nb, int* Bc) {
 // scene of one level it only does that.
 template <int D>
 __global__ void __launch_bounds__(Stage<D>::PER) k_restrict(Batch B, int l) {
-  SCENE_CTA(B, MAP_G);
+  SCENE_CTA(B, MAP_T);
   using S = Stage<D>;
   constexpr int NB = (D == 2) ? 9 : 27;
   __shared__ __align__(128) float4 fn[NB][S::PER];
@@ -630,7 +630,7 @@ __global__ void k_gridop(Batch B) {
 // final.
 template <int D>
 __global__ void __launch_bounds__(Stage<D>::PER) k_prolong(Batch B, int l) {
-  SCENE_CTA(B, MAP_G);
+  SCENE_CTA(B, MAP_T);
   using S = Stage<D>;
   constexpr int NB = 1 << D;
   __shared__ __align__(128) float4 cn[NB][S::PER];
@@ -1200,13 +1200,13 @@ void launch_transfer(const BatchLaunch& bl, cudaStream_t s, cudaEvent_t* ev) {
   // the first launch after the join is a plain one
   bool first = true;
   for (int l = bl.maxL - 1; l >= 1; --l, first = false)
-    launch_k(pdl && !(first && bl.side), k_restrict<D>, G, Stage<D>::PER, 0, s, bl.b, l);
+    launch_k(pdl && !(first && bl.side), k_restrict<D>, bl.nct[MAP_T], Stage<D>::PER, 0, s, bl.b, l);
   if (ev) cudaEventRecord(ev[5], s);
   // with more than one level grid_op runs inside the restriction into level 0
   // and the prolongations
   if (bl.maxL == 1) launch_k(pdl && !bl.side, k_gridop<D>, G, 256, 0, s, bl.b);
   if (ev) cudaEventRecord(ev[6], s);
-  for (int l = 1; l < bl.maxL; ++l) launch_k(pdl, k_prolong<D>, G, Stage<D>::PER, 0, s, bl.b, l);
+  for (int l = 1; l < bl.maxL; ++l) launch_k(pdl, k_prolong<D>, bl.nct[MAP_T], Stage<D>::PER, 0, s, bl.b, l);
   if (ev) cudaEventRecord(ev[7], s);
   launch_k(pdl, k_g2p<D>, G, 256, 0, s, bl.b);
   if (bl.any_plastic) launch_k(pdl, k_project<D>, G, 256, 0, s, bl.b);
