@@ -143,3 +143,38 @@ def save(path, mlp, xmax, meta=None):
 def load(path, device=0):
     z = np.load(path)
     return MLP(device=device, params=z["params"]), z["xmax"]
+
+
+def bench(rows=2_000_000, reps=10, device=0):
+    """Throughput of the tensor-core forward pass and of one training step on
+    `rows` random samples (CUDA events); returns a dict."""
+    import torch
+    m = MLP(device=device)
+    X = torch.randn((rows, IN), device="cuda:%d" % device)
+    T = torch.randn((rows, OUT), device="cuda:%d" % device)
+    for _ in range(3):
+        m.forward(X)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps):
+        m.forward(X)
+    e1.record()
+    torch.cuda.synchronize()
+    fwd = e0.elapsed_time(e1) / reps
+    train(m, X, T, steps=3, batch=min(rows, 1 << 20))
+    torch.cuda.synchronize()
+    e0.record()
+    train(m, X, T, steps=reps, batch=min(rows, 1 << 20))
+    e1.record()
+    torch.cuda.synchronize()
+    step = e0.elapsed_time(e1) / reps
+    flop = 2 * (IN * H + H * H + H * OUT)
+    return {"rows": rows, "forward_ms": fwd, "forward_tflops": rows * flop / (fwd * 1e-3) / 1e12,
+            "train_step_ms": step, "train_batch": min(rows, 1 << 20), "errors": m.errors()}
+
+
+if __name__ == "__main__":
+    import json
+    import sys
+    print(json.dumps(bench(int(sys.argv[1]) if len(sys.argv) > 1 else 2_000_000)))
