@@ -77,15 +77,16 @@ __device__ __forceinline__ float2 dup2(float a) { return make_float2(a, a); }
 //     per-axis GIMP weights and gradients, m, a = m (v - C (tc+1)) and
 //     B = m C, and its base cell inside the block, and stores them in shared
 //     memory at its thread index;
-//  2. each warp cuts its own 32 particles into SLOTS contiguous ranges of
-//     equal length (3 of 11/11/10 in 3D, 10 of 3-4 in 2D); a lane owns one row
-//     of three stencil nodes (the last axis runs along the row; 3^(d-1) rows
-//     per cell) of one range and walks its particles.  While the base cell
-//     stays the same it sums w m and w (a + B n) + S grad w of its three
-//     nodes in registers (one read of a particle record serves three nodes,
-//     and the row's weight products are shared); when the cell changes, and
-//     at the end, the sums go into the (4+2)^d node tile in shared memory.
-//     Equal ranges keep every slot busy for the same number of steps;
+//  2. each warp cuts its own 32 particles into ranges: in 3D SLOTS = 3
+//     contiguous ranges of equal length (11/11/10), which keeps every slot
+//     busy for the same number of steps; in 2D runs of one base cell (about 4
+//     particles), 10 at a time.  A lane owns one row of three stencil nodes
+//     (the last axis runs along the row; 3^(d-1) rows per cell) of one range
+//     and walks its particles.  While the base cell stays the same it sums
+//     w m and w (a + B n) + S grad w of its three nodes in registers (one read
+//     of a particle record serves three nodes, and the row's weight products
+//     are shared); when the cell changes, and at the end, the sums go into
+//     the (4+2)^d node tile in shared memory;
 //  3. a CTA takes a contiguous range of work items, so consecutive items of
 //     one block (a dense block holds many) keep summing into the same tile;
 //     when the next item is another block, the tile is flushed after one
@@ -109,7 +110,10 @@ struct P2GLayout {
   static constexpr int OFF_WP = (D == 3) ? 20 : 12;  // (W, G) pairs of the axes before the last
   static constexpr int OFF_WL = (D == 3) ? 32 : 20;  // last axis: W[0..2], then G[0..2] at +4
   static constexpr int OFF_CELL = (D == 3) ? 35 : 3;
-  static constexpr size_t bytes() { return sizeof(float) * ((size_t)CH * STRIDE + 2 * 4 * TN); }
+  static constexpr int TMAX = 16;  // 2D: longest run of one base cell walked by one slot
+  static constexpr size_t bytes() {
+    return sizeof(float) * ((size_t)CH * STRIDE + 2 * 4 * TN) + sizeof(int) * (CH / 32) * 33;
+  }
 };
 
 // A lane's three node sums of one base cell into the node tile ([4][TN]:
@@ -138,6 +142,7 @@ __global__ void __launch_bounds__(CH, 1024 / CH) k_p2g(Batch B) {
   extern __shared__ float4 dsm4[];
   float* pd = (float*)dsm4;             // [CH][STRIDE]
   float* tiles = pd + CH * Y::STRIDE;   // [2][4][TN]: p_x, p_y, p_z, m
+  int* starts = (int*)(tiles + 2 * 4 * Y::TN);  // 2D: [warps][33] run starts
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int nch = c.ctr[CTR_CHUNKS];
   const float pw = (D == 2) ? 0.25f : 0.125f;                                        // 0.5**dim
@@ -170,6 +175,7 @@ __global__ void __launch_bounds__(CH, 1024 / CH) k_p2g(Batch B) {
     float* tile = tiles + tb * 4 * Y::TN;
     // -- 1. per-particle records -----------------------------------------------
     const int i = threadIdx.x;
+    int cell = -1;
     if (i < wd.w) {
       const int p = __ldg(&c.perm[wd.z + i]);
       const long long N = c.N;
@@ -189,7 +195,7 @@ __global__ void __launch_bounds__(CH, 1024 / CH) k_p2g(Batch B) {
       const float mp = __ldg(&c.P.m[p]);
       const float jp = c.plast == 1 ? __ldg(&c.P.Jp[p]) : 1.f;
       float tc[D];
-      int cell = 0;
+      cell = 0;
 #pragma unroll
       for (int d = 0; d < D; ++d) {
         const float xs = xp[d] * inv;
@@ -258,11 +264,10 @@ __global__ void __launch_bounds__(CH, 1024 / CH) k_p2g(Batch B) {
       }
     }
     __syncwarp();
-    // -- 2. this warp's particles: SLOTS equal ranges, lane <-> node row ---------
+    // -- 2. this warp's particles in SLOTS ranges, lane <-> node row -------------
     const int wbase = warp * 32;
     const int nvalid = max(0, min(32, wd.w - wbase));
-    if (q < Y::SLOTS) {
-      const int j0 = (q * nvalid) / Y::SLOTS, j1 = ((q + 1) * nvalid) / Y::SLOTS;
+    auto walk = [&](const int j0, const int j1) {
       const float2 nn0 = dup2((float)n0), nn1 = dup2((float)n1);
       float2 axy[3];
       float az[3], am[3];
@@ -344,9 +349,33 @@ __global__ void __launch_bounds__(CH, 1024 / CH) k_p2g(Batch B) {
         }
       }
       if (cur >= 0) p2g_row_flush<D>(tile, Y::TN, cur, n0, n1, axy, az, am);
+    };
+    if (D == 3) {
+      // 3D: SLOTS equal ranges of consecutive particles in one pass (11, 11,
+      // 10); a range's sums go to the tile whenever its base cell changes
+      if (q < Y::SLOTS) walk((q * nvalid) / Y::SLOTS, ((q + 1) * nvalid) / Y::SLOTS);
+    } else {
+      // 2D: runs of one base cell (found with ballots, at most TMAX long; a
+      // cell holds about 4 particles), SLOTS runs at a time, one tile update
+      // per run
+      const bool valid = lane < nvalid;
+      const int prev = __shfl_up_sync(0xffffffffu, cell, 1);
+      const unsigned runs = __ballot_sync(0xffffffffu, valid && (lane == 0 || cell != prev));
+      const int rs = valid ? 31 - __clz(runs & ((2u << lane) - 1u)) : 0;  // start of this lane's run
+      const bool tstart = valid && (lane - rs) % Y::TMAX == 0;
+      const unsigned tmask = __ballot_sync(0xffffffffu, tstart);
+      const int ntask = __popc(tmask);
+      int* ws = starts + warp * 33;  // task k starts at ws[k]; ws[ntask] = nvalid
+      if (tstart) ws[__popc(tmask & ((1u << lane) - 1u))] = lane;
+      if (lane == 0) ws[ntask] = nvalid;
+      __syncwarp();
+      for (int t0 = 0; t0 < ntask; t0 += Y::SLOTS) {
+        const int t = t0 + q;
+        if (q < Y::SLOTS && t < ntask) walk(ws[t], ws[t + 1]);
+      }
     }
-    // the next work item's step 1 overwrites this warp's records, which lanes
-    // of this warp may still be reading above
+    // the next work item's step 1 overwrites this warp's records and task
+    // starts, which lanes of this warp may still be reading above
     __syncwarp();
     if (!last) continue;  // the same block follows: keep summing into this tile
     __syncthreads();
@@ -594,6 +623,152 @@ __global__ void __launch_bounds__(Stage<D>::PER) k_restrict(Batch B, int l) {
     if (inr && l == 1) gridop_node<D>(c, 0, K, cidx);
     __syncthreads();  // the tile is free for the next block's copies
   }
+}
+
+// ---------------------------------------------------------------------------
+// The same two transfers as direct gathers through L1 (one thread per
+// destination node, the level node masks read in place): used for 2D
+// scenes, whose 16-node blocks are too small for a staging round trip per
+// block to pay.
+template <int D>
+__global__ void k_restrict_gather(Batch B, int l) {
+  SCENE_CTA(B, MAP_G);
+  const bool restrict_l = l < c.L;
+  if (!restrict_l && l != 1) return;
+  const LevelDev& Vc = c.lev[l - 1];
+  const LevelDev& Vf = c.lev[restrict_l ? l : l - 1];
+  const long long tot = (long long)c.ctr[CTR_LEVEL + l - 1] << (2 * D);
+  const int lsz = Vf.size, l0sz = Vc.size;
+  SCENE_LOOP(e, tot) {
+    const long long blk = Vc.blist[e >> (2 * D)];
+    const int loc = (int)(e & ((1 << (2 * D)) - 1));
+    int K[D];
+    elem_coords<D>(Vc, blk, loc, K);
+    bool inr = true;
+#pragma unroll
+    for (int d = 0; d < D; ++d) inr = inr && K[d] >= 0 && K[d] <= l0sz;
+    if (!inr) continue;
+    const long long cidx = (blk << (2 * D)) | loc;
+    if (restrict_l && is_valid(Vc.nm[cidx])) {
+      float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
+      bool any = false;
+#pragma unroll
+      for (int a = 0; a < ((D == 2) ? 9 : 27); ++a) {
+        int I[D], nrm = 0, t = a;
+        bool ok = true;
+#pragma unroll
+        for (int d = D - 1; d >= 0; --d) {
+          const int dI = t % 3 - 1;
+          t /= 3;
+          I[d] = 2 * K[d] - dI;
+          nrm += dI != 0;
+          ok = ok && I[d] >= 0 && I[d] <= lsz;
+        }
+        if (!ok) continue;
+        const long long fidx = elem_of<D>(Vf, I);
+        const uint32_t nm = Vf.nm[fidx];
+        if (!((is_activated(nm) && nrm == 0) || is_tj(nm) || is_ghost(nm))) continue;
+        const float w = (nrm == 0) ? 1.f : (nrm == 1) ? 0.5f : (nrm == 2) ? 0.25f : 0.125f;
+        const float4 f = Vf.node[fidx];
+        acc.x += f.x * w;
+        acc.y += f.y * w;
+        acc.z += f.z * w;
+        acc.w += f.w * w;
+        any = true;
+      }
+      if (any) {
+        float4 o = Vc.node[cidx];
+        o.x += acc.x;
+        o.y += acc.y;
+        o.z += acc.z;
+        o.w += acc.w;
+        Vc.node[cidx] = o;
+      }
+    }
+    if (l == 1) gridop_node<D>(c, 0, K, cidx);
+  }
+}
+
+template <int D>
+__global__ void k_prolong_gather(Batch B, int l) {
+  SCENE_CTA(B, MAP_G);
+  if (l >= c.L) return;
+  const LevelDev& Vc = c.lev[l - 1];
+  const LevelDev& Vf = c.lev[l];
+  const long long tot = (long long)c.ctr[CTR_LEVEL + l] << (2 * D);
+  const int lsz = Vf.size;
+  SCENE_LOOP(e, tot) {
+    const long long blk = Vf.blist[e >> (2 * D)];
+    const int loc = (int)(e & ((1 << (2 * D)) - 1));
+    int J[D];
+    elem_coords<D>(Vf, blk, loc, J);
+    bool inr = true, even = true;
+#pragma unroll
+    for (int d = 0; d < D; ++d) {
+      inr = inr && J[d] >= 0 && J[d] <= lsz;
+      even = even && (J[d] & 1) == 0;
+    }
+    if (!inr) continue;
+    const long long fidx = (blk << (2 * D)) | loc;
+    gridop_node<D>(c, l, J, fidx);
+    const uint32_t nm = Vf.nm[fidx];
+    const bool tg = is_tj(nm) || is_ghost(nm);
+    if (!tg && !even) continue;
+    float acc[3] = {0.f, 0.f, 0.f};
+    if (tg) {
+      int nodd = 0;
+#pragma unroll
+      for (int d = 0; d < D; ++d) nodd += J[d] & 1;
+      const float w = (nodd == 0) ? 1.f : (nodd == 1) ? 0.5f : (nodd == 2) ? 0.25f : 0.125f;
+#pragma unroll
+      for (int a = 0; a < (1 << D); ++a) {
+        int K[D];
+        bool use = true;
+#pragma unroll
+        for (int d = 0; d < D; ++d) {
+          const int bit = (a >> d) & 1;
+          if (J[d] & 1)
+            K[d] = (J[d] - 1) / 2 + bit;
+          else {
+            K[d] = J[d] / 2;
+            use = use && bit == 0;
+          }
+        }
+        if (!use) continue;
+        const long long cidx = elem_of<D>(Vc, K);
+        if (!is_valid(Vc.nm[cidx])) continue;
+        const float4 cv = Vc.node[cidx];
+        acc[0] += cv.x * w;
+        acc[1] += cv.y * w;
+        acc[2] += cv.z * w;
+      }
+    } else if (is_activated(nm)) {
+      int K[D];
+#pragma unroll
+      for (int d = 0; d < D; ++d) K[d] = J[d] / 2;
+      const long long cidx = elem_of<D>(Vc, K);
+      if (is_valid(Vc.nm[cidx])) {
+        const float4 cv = Vc.node[cidx];
+        acc[0] = cv.x;
+        acc[1] = cv.y;
+        acc[2] = cv.z;
+      }
+    }
+    float4 o = Vf.node[fidx];
+    o.x = acc[0];
+    o.y = acc[1];
+    o.z = acc[2];
+    Vf.node[fidx] = o;
+  }
+}
+
+#ifndef AGIMP_TRANSFER_GATHER_3D
+#define AGIMP_TRANSFER_GATHER_3D 0
+#endif
+// 3D scenes stage their transfers through shared memory, 2D scenes gather
+template <int D>
+constexpr bool staged_transfers() {
+  return D == 3 && !AGIMP_TRANSFER_GATHER_3D;
 }
 
 // ---------------------------------------------------------------------------
@@ -1037,7 +1212,9 @@ __device__ __forceinline__ void g2p_one(const Ctx& c, int j) {
   for (int n0 = 0; n0 < 3; ++n0) {
     float w0, g0;
     axis_factor(tc[0], n0, w0, g0);
-#pragma unroll
+    // one row (3 nodes) in flight at a time: measured faster than a slab of
+    // 9 gathers, which does not fit the 64-register budget
+#pragma unroll 1
     for (int n1 = 0; n1 < ((D == 2) ? 1 : 3); ++n1) {
       float S[D], T[D];
 #pragma unroll
@@ -1199,14 +1376,23 @@ void launch_transfer(const BatchLaunch& bl, cudaStream_t s, cudaEvent_t* ev) {
   if (ev) cudaEventRecord(ev[4], s);
   // the first launch after the join is a plain one
   bool first = true;
-  for (int l = bl.maxL - 1; l >= 1; --l, first = false)
-    launch_k(pdl && !(first && bl.side), k_restrict<D>, bl.nct[MAP_T], Stage<D>::PER, 0, s, bl.b, l);
+  for (int l = bl.maxL - 1; l >= 1; --l, first = false) {
+    if (staged_transfers<D>())
+      launch_k(pdl && !(first && bl.side), k_restrict<D>, bl.nct[MAP_T], Stage<D>::PER, 0, s, bl.b, l);
+    else
+      launch_k(pdl && !(first && bl.side), k_restrict_gather<D>, G, 256, 0, s, bl.b, l);
+  }
   if (ev) cudaEventRecord(ev[5], s);
   // with more than one level grid_op runs inside the restriction into level 0
   // and the prolongations
   if (bl.maxL == 1) launch_k(pdl && !bl.side, k_gridop<D>, G, 256, 0, s, bl.b);
   if (ev) cudaEventRecord(ev[6], s);
-  for (int l = 1; l < bl.maxL; ++l) launch_k(pdl, k_prolong<D>, bl.nct[MAP_T], Stage<D>::PER, 0, s, bl.b, l);
+  for (int l = 1; l < bl.maxL; ++l) {
+    if (staged_transfers<D>())
+      launch_k(pdl, k_prolong<D>, bl.nct[MAP_T], Stage<D>::PER, 0, s, bl.b, l);
+    else
+      launch_k(pdl, k_prolong_gather<D>, G, 256, 0, s, bl.b, l);
+  }
   if (ev) cudaEventRecord(ev[7], s);
   launch_k(pdl, k_g2p<D>, G, 256, 0, s, bl.b);
   if (bl.any_plastic) launch_k(pdl, k_project<D>, G, 256, 0, s, bl.b);
