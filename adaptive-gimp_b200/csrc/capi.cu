@@ -352,7 +352,7 @@ agimp_status agimp_create(const agimp_params* p, int32_t device, agimp_sim** out
     LevelDev& V = c.lev[l];
     if (l == c.L - 1) {
       V.nm = c.nmask;
-    } else {
+    } else if (D == 3) {  // 2D transfers read the node mask itself
       AL(V.nm, V.nblocks * per);
       cudaMemset(V.nm, 0, V.nblocks * per * sizeof(uint32_t));
     }
@@ -409,7 +409,9 @@ agimp_status agimp_create(const agimp_params* p, int32_t device, agimp_sim** out
       cudaEventCreateWithFlags(&s->ev_out, cudaEventDisableTiming) != cudaSuccess ||
       cudaEventCreateWithFlags(&s->ev_state, cudaEventDisableTiming) != cudaSuccess ||
       cudaEventCreateWithFlags(&s->ev_read[0], cudaEventDisableTiming) != cudaSuccess ||
-      cudaEventCreateWithFlags(&s->ev_read[1], cudaEventDisableTiming) != cudaSuccess) {
+      cudaEventCreateWithFlags(&s->ev_read[1], cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&s->ev_stage[0], cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&s->ev_stage[1], cudaEventDisableTiming) != cudaSuccess) {
     agimp_destroy(s);
     return AGIMP_CUDA_ERROR;
   }
@@ -444,7 +446,7 @@ agimp_status agimp_destroy(agimp_sim* s) {
   for (void* p : s->allocs) cudaFree(p);
   if (s->rimg) cudaFree(s->rimg);
   if (s->astage) cudaFree(s->astage);
-  for (cudaEvent_t e : {s->ev_state, s->ev_read[0], s->ev_read[1]})
+  for (cudaEvent_t e : {s->ev_state, s->ev_read[0], s->ev_read[1], s->ev_stage[0], s->ev_stage[1]})
     if (e) cudaEventDestroy(e);
   if (s->rwin) cudaFree(s->rwin);
   if (s->rkey) cudaFree(s->rkey);
@@ -594,30 +596,45 @@ agimp_status agimp_get_particles_async(agimp_sim* s, float* x, float* v, float* 
     CK(cudaEventRecord(s->ev_state, su.use));
   }
   CK(cudaStreamWaitEvent(su.use, s->ev_state, 0));  // the state is written
-  if (s->last_read >= 0) CK(cudaStreamWaitEvent(su.use, s->ev_read[s->last_read], 0));  // staging is free
+  // Two staging slots: the fields are first gathered into caller order in
+  // this call's slot (a short kernel), which frees the particle state for the
+  // substep that overwrites it; the host copies out of the slot then overlap
+  // the following substeps.  A slot is reused two calls later, after its
+  // copies.
+  const int slot = s->stage_next;
+  s->stage_next ^= 1;
+  if (s->stage_busy[slot]) CK(cudaStreamWaitEvent(su.use, s->ev_stage[slot], 0));
   const size_t need = (size_t)N * (2 * D + 2 * D * D + 4) + 16;
   if (need > s->astage_floats) {
-    CK(cudaStreamSynchronize(su.use));
+    CK(cudaDeviceSynchronize());  // both slots idle before they move
     if (s->astage) cudaFree(s->astage);
     s->astage = nullptr;
     s->astage_floats = 0;
-    CK(cudaMalloc(&s->astage, need * sizeof(float)));
+    CK(cudaMalloc(&s->astage, 2 * need * sizeof(float)));
     s->astage_floats = need;
   }
-  float* st = s->astage;
+  float* const st0 = s->astage + (size_t)slot * s->astage_floats;
+  struct Copy {
+    void* dst;
+    const float* src;
+    size_t bytes;
+  };
+  Copy copies[8];
+  int ncopy = 0;
+  float* st = st0;
   auto field = [&](const float* src, float* dst, int comps) -> cudaError_t {
     if (!dst || !N) return cudaSuccess;
     k_soa_to_aos<<<gs_blocks(N * comps), 256, 0, su.use>>>(src, P.id, st, N, comps);
-    cudaError_t e = cudaMemcpyAsync(dst, st, N * comps * sizeof(float), cudaMemcpyDeviceToHost, su.use);
+    copies[ncopy++] = {dst, st, N * comps * sizeof(float)};
     st += N * comps;
-    return e;
+    return cudaGetLastError();
   };
   auto ifield = [&](const int32_t* src, int32_t* dst) -> cudaError_t {
     if (!dst || !N) return cudaSuccess;
     k_i32_out<<<gs_blocks(N), 256, 0, su.use>>>(src, P.id, (int32_t*)st, N);
-    cudaError_t e = cudaMemcpyAsync(dst, st, N * sizeof(int32_t), cudaMemcpyDeviceToHost, su.use);
+    copies[ncopy++] = {dst, st, N * sizeof(int32_t)};
     st += N;
-    return e;
+    return cudaGetLastError();
   };
   CK(field(P.x, x, D));
   CK(field(P.v, v, D));
@@ -627,10 +644,14 @@ agimp_status agimp_get_particles_async(agimp_sim* s, float* x, float* v, float* 
   CK(field(P.Jp, Jp, 1));
   CK(ifield(P.g, g));
   CK(ifield(P.fl, fl));
-  CK(cudaGetLastError());
+  // the state has been read: a substep may overwrite it from here on
   CK(cudaEventRecord(s->ev_read[k], su.use));
   s->read_pending[k] = true;
   s->last_read = k;
+  for (int i = 0; i < ncopy; ++i)
+    CK(cudaMemcpyAsync(copies[i].dst, copies[i].src, copies[i].bytes, cudaMemcpyDeviceToHost, su.use));
+  CK(cudaEventRecord(s->ev_stage[slot], su.use));
+  s->stage_busy[slot] = true;
   return AGIMP_OK;
 }
 

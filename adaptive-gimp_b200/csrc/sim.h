@@ -32,8 +32,11 @@ struct agimp_sim {
   cudaEvent_t ev_read[2] = {nullptr, nullptr};
   bool read_pending[2] = {false, false};
   int last_read = -1;           // buffer of the last asynchronous readback (its staging is busy until ev_read)
-  float* astage = nullptr;      // staging of asynchronous readbacks
+  float* astage = nullptr;      // staging of asynchronous readbacks: two slots of astage_floats
   size_t astage_floats = 0;
+  int stage_next = 0;           // slot of the next asynchronous readback
+  bool stage_busy[2] = {false, false};
+  cudaEvent_t ev_stage[2] = {nullptr, nullptr};  // the host copy out of slot k has been issued up to here
   float* rimg = nullptr;        // headless drawing: image scratch for host outputs
   size_t rimg_floats = 0;
   int* rwin = nullptr;          // headless drawing: particle covering each pixel

@@ -63,7 +63,7 @@ __global__ void k_clear(Batch B) {
     const long long idx = (blk << (2 * D)) | loc;
     V.cell[idx] = 0u;
     V.node[idx] = make_float4(0.f, 0.f, 0.f, 0.f);
-    if (l < c.L - 1) V.nm[idx] = 0u;
+    if (D == 3 && l < c.L - 1) V.nm[idx] = 0u;
     if (loc == 0) V.bmap[blk] = -1;
     int I[D];
     elem_coords<D>(V, blk, loc, I);
@@ -316,13 +316,9 @@ __global__ void k_dilate(Batch B) {
   // (2R_l + 1)^d neighbourhood at every level
   const int lane = threadIdx.x & 31;
   const int wid = bid_ * (blockDim.x >> 5) + (threadIdx.x >> 5), nw = nblk_ * (blockDim.x >> 5);
-  // (touched block, level) pairs go to separate warps, so a block's levels
-  // are dilated concurrently; level L works the static-map lookups
   const LevelDev& Vf = c.lev[c.L - 1];
   const int ntouch = c.ctr[CTR_TOUCH];
-  const int nlev = c.L + (c.is_static ? 1 : 0);
-  for (int u = wid; u < ntouch * nlev; u += nw) {
-    const int t = u / nlev, l = u - t * nlev;
+  for (int t = wid; t < ntouch; t += nw) {
     const int key = c.touch_list[t];
     const unsigned reach = c.touch_flag[key];
     int fb[D];
@@ -332,11 +328,7 @@ __global__ void k_dilate(Batch B) {
       fb[d] = (int)(k % (unsigned)Vf.nb) - 1;
       k /= (unsigned)Vf.nb;
     }
-    if (l == c.L) {
-      static_window<D>(c, key, fb, lane);
-      continue;
-    }
-    {
+    for (int l = 0; l < c.L; ++l) {
       const int R = dilate_radius(c, l, reach);
       const int w = 2 * R + 1;
       const int items = (D == 2) ? w * w : w * w * w;
@@ -364,6 +356,7 @@ __global__ void k_dilate(Batch B) {
         }
       }
     }
+    if (c.is_static) static_window<D>(c, key, fb, lane);
   }
 }
 
@@ -528,8 +521,9 @@ __global__ void k_ghost_tj(Batch B) {
 }
 
 // ---------------------------------------------------------------------------
-// Per-level node masks for the levels below the finest: node I of level l
-// gets node_mask[_map(l, I)] (adaptive_gimp.py:126-128), 0 outside [0, size].
+// Per-level node masks for the levels below the finest (3D scenes, whose
+// level transfers copy them by whole blocks): node I of level l gets
+// node_mask[_map(l, I)] (adaptive_gimp.py:126-128), 0 outside [0, size].
 // Runs after ghost / T-junction marking, the last writer of the node mask.
 template <int D>
 __global__ void k_level_masks(Batch B) {
@@ -793,11 +787,11 @@ static void run_topology(const BatchLaunch& bl, cudaStream_t s, cudaEvent_t* ev)
     cudaEventRecord(bl.fork, s);
     cudaStreamWaitEvent(bl.side, bl.fork, 0);
     k_ghost_tj<D><<<G, 256, 0, bl.side>>>(B);
-    if (bl.maxL > 1) launch_k(true, k_level_masks<D>, G, 256, 0, bl.side, B);
+    if (D == 3 && bl.maxL > 1) launch_k(true, k_level_masks<D>, G, 256, 0, bl.side, B);
     cudaEventRecord(bl.join, bl.side);
   } else {
     launch_k(pdl, k_ghost_tj<D>, G, 256, 0, s, B);
-    if (bl.maxL > 1) launch_k(pdl, k_level_masks<D>, G, 256, 0, s, B);
+    if (D == 3 && bl.maxL > 1) launch_k(pdl, k_level_masks<D>, G, 256, 0, s, B);
   }
   if (ev) cudaEventRecord(ev[2], s);
   // after an event record or wait the next launch is a plain one
@@ -819,7 +813,7 @@ void launch_substep(const BatchLaunch& bl, cudaStream_t s, cudaEvent_t* ev) {
 }
 
 int kernels_per_substep(const BatchLaunch& bl) {
-  const int topo = 10 - (bl.any_dynamic ? 0 : 1) + (bl.maxL > 1 ? 1 : 0);
+  const int topo = 10 - (bl.any_dynamic ? 0 : 1) + (bl.dim == 3 && bl.maxL > 1 ? 1 : 0);
   return topo + 2 + (bl.maxL == 1 ? 1 : 0) + (bl.any_plastic ? 1 : 0) + 2 * (bl.maxL - 1);
 }
 

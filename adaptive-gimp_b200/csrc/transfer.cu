@@ -405,13 +405,22 @@ __global__ void __launch_bounds__(CH, 1024 / CH) k_p2g(Batch B) {
 // grid_op (adaptive_gimp.py:277-287) of node I of level l, stored at idx: an
 // activated node's momentum becomes its velocity (gravity, walls, colliders);
 // with inv_norm the other nodes with mass are divided by it.  I lies in
-// [0, size]^d; the level's node mask supplies is_activated.
+// [0, size]^d.
+// Node mask of node I of level l stored at idx: 3D scenes read the level's
+// own copy (k_level_masks), which the staged transfers copy by whole blocks;
+// 2D scenes, whose transfers gather node by node, read the node mask itself.
+template <int D>
+__device__ __forceinline__ uint32_t level_mask(const Ctx& c, int l, const int* I, long long idx) {
+  if (D == 3) return c.lev[l].nm[idx];
+  return nm_get<D>(c, l, I);
+}
+
 template <int D>
 __device__ __forceinline__ void gridop_node(const Ctx& c, int l, const int* I, long long idx) {
   const LevelDev& V = c.lev[l];
   const float4 nd = V.node[idx];
   if (!(nd.w > 0.f)) return;
-  if (!is_activated(V.nm[idx])) {
+  if (!is_activated(level_mask<D>(c, l, I, idx))) {
     if (c.inv_norm) V.node[idx] = make_float4(nd.x / nd.w, nd.y / nd.w, D == 3 ? nd.z / nd.w : nd.z, nd.w);
     return;
   }
@@ -627,9 +636,8 @@ __global__ void __launch_bounds__(Stage<D>::PER) k_restrict(Batch B, int l) {
 
 // ---------------------------------------------------------------------------
 // The same two transfers as direct gathers through L1 (one thread per
-// destination node, the level node masks read in place): used for 2D
-// scenes, whose 16-node blocks are too small for a staging round trip per
-// block to pay.
+// destination node): used for 2D scenes, whose 16-node blocks are too small
+// for a staging round trip per block to pay.
 template <int D>
 __global__ void k_restrict_gather(Batch B, int l) {
   SCENE_CTA(B, MAP_G);
@@ -649,7 +657,7 @@ __global__ void k_restrict_gather(Batch B, int l) {
     for (int d = 0; d < D; ++d) inr = inr && K[d] >= 0 && K[d] <= l0sz;
     if (!inr) continue;
     const long long cidx = (blk << (2 * D)) | loc;
-    if (restrict_l && is_valid(Vc.nm[cidx])) {
+    if (restrict_l && is_valid(level_mask<D>(c, l - 1, K, cidx))) {
       float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
       bool any = false;
 #pragma unroll
@@ -666,7 +674,7 @@ __global__ void k_restrict_gather(Batch B, int l) {
         }
         if (!ok) continue;
         const long long fidx = elem_of<D>(Vf, I);
-        const uint32_t nm = Vf.nm[fidx];
+        const uint32_t nm = level_mask<D>(c, l, I, fidx);
         if (!((is_activated(nm) && nrm == 0) || is_tj(nm) || is_ghost(nm))) continue;
         const float w = (nrm == 0) ? 1.f : (nrm == 1) ? 0.5f : (nrm == 2) ? 0.25f : 0.125f;
         const float4 f = Vf.node[fidx];
@@ -711,7 +719,7 @@ __global__ void k_prolong_gather(Batch B, int l) {
     if (!inr) continue;
     const long long fidx = (blk << (2 * D)) | loc;
     gridop_node<D>(c, l, J, fidx);
-    const uint32_t nm = Vf.nm[fidx];
+    const uint32_t nm = level_mask<D>(c, l, J, fidx);
     const bool tg = is_tj(nm) || is_ghost(nm);
     if (!tg && !even) continue;
     float acc[3] = {0.f, 0.f, 0.f};
@@ -736,7 +744,7 @@ __global__ void k_prolong_gather(Batch B, int l) {
         }
         if (!use) continue;
         const long long cidx = elem_of<D>(Vc, K);
-        if (!is_valid(Vc.nm[cidx])) continue;
+        if (!is_valid(level_mask<D>(c, l - 1, K, cidx))) continue;
         const float4 cv = Vc.node[cidx];
         acc[0] += cv.x * w;
         acc[1] += cv.y * w;
@@ -747,7 +755,7 @@ __global__ void k_prolong_gather(Batch B, int l) {
 #pragma unroll
       for (int d = 0; d < D; ++d) K[d] = J[d] / 2;
       const long long cidx = elem_of<D>(Vc, K);
-      if (is_valid(Vc.nm[cidx])) {
+      if (is_valid(level_mask<D>(c, l - 1, K, cidx))) {
         const float4 cv = Vc.node[cidx];
         acc[0] = cv.x;
         acc[1] = cv.y;

@@ -82,11 +82,11 @@ def test_batch_matches_scenes_stepped_alone():
             assert np.abs(a["x"] - b["x"]).max() <= 1e-5, (k, np.abs(a["x"] - b["x"]).max())
             assert np.abs(a["v"] - b["v"]).max() <= 1e-3 * max(1.0, np.abs(a["v"]).max())
         assert together[k].stats()["substeps"] == steps
-    # 11 topology and binning kernels (k_mark_hier and the level masks included: one scene is
+    # 10 topology and binning kernels (k_mark_hier included: one scene is
     # dynamic), P2G, G2P, the return map (one scene has snow plasticity), and
     # a restriction and a prolongation per level above 0 (grid_op runs inside
     # them)
-    assert batch.kernels_per_substep() == 11 + 3 + 2 * (max(s.level for s in sc) - 1)
+    assert batch.kernels_per_substep() == 10 + 3 + 2 * (max(s.level for s in sc) - 1)
     batch.close()
     for s in alone + together:
         s.close()
