@@ -135,40 +135,8 @@ __device__ __forceinline__ void p2g_row_flush(float* tile, int TN, int cc, int n
   }
 }
 
-// 3D, one lane per node plane (n0 fixed): its nine node sums of one base
-// cell into the node tile.
-__device__ __forceinline__ void p2g_plane_flush(float* tile, int TN, int cc, int n0, const float2 (*axy)[3],
-                                                const float (*az)[3], const float (*am)[3]) {
-  const int t0 = ((((cc >> 4) & 3) + n0) * 6 + ((cc >> 2) & 3)) * 6 + (cc & 3);
-#pragma unroll
-  for (int n1 = 0; n1 < 3; ++n1)
-#pragma unroll
-    for (int k = 0; k < 3; ++k) {
-      const int ti = t0 + n1 * 6 + k;
-      atomicAdd(&tile[ti], axy[n1][k].x);
-      atomicAdd(&tile[TN + ti], axy[n1][k].y);
-      atomicAdd(&tile[2 * TN + ti], az[n1][k]);
-      atomicAdd(&tile[3 * TN + ti], am[n1][k]);
-    }
-}
-
-#ifndef AGIMP_P2G_PLANES
-#define AGIMP_P2G_PLANES 0
-#endif
-// 3D P2G lanes: 0 = one lane per row of 3 nodes (9 lanes a particle), 1 = one
-// lane per plane of 9 nodes (3 lanes a particle, a third of the record reads,
-// 36 sums in registers: 3 CTAs of 256 per SM)
-#ifndef AGIMP_P2G_PLANE_THREADS
-#define AGIMP_P2G_PLANE_THREADS 768
-#endif
-constexpr int P2G_PLANES = AGIMP_P2G_PLANES;
 template <int D, int CH>
-constexpr int p2g_min_ctas() {
-  return (D == 3 && P2G_PLANES) ? AGIMP_P2G_PLANE_THREADS / CH : 1024 / CH;
-}
-
-template <int D, int CH>
-__global__ void __launch_bounds__(CH, (p2g_min_ctas<D, CH>() > 0 ? p2g_min_ctas<D, CH>() : 1)) k_p2g(Batch B) {
+__global__ void __launch_bounds__(CH, 1024 / CH) k_p2g(Batch B) {
   SCENE_CTA(B, MAP_G);
   using Y = P2GLayout<D, CH>;
   extern __shared__ float4 dsm4[];
@@ -382,76 +350,7 @@ __global__ void __launch_bounds__(CH, (p2g_min_ctas<D, CH>() > 0 ? p2g_min_ctas<
       }
       if (cur >= 0) p2g_row_flush<D>(tile, Y::TN, cur, n0, n1, axy, az, am);
     };
-    if (D == 3 && P2G_PLANES) {
-      // 3D planes: 10 equal ranges (3-4 particles), lane <-> plane n0 of one
-      const int qp = lane / 3, p0 = lane % 3;
-      if (qp < 10) {
-        const int j0 = (qp * nvalid) / 10, j1 = ((qp + 1) * nvalid) / 10;
-        float2 axy[3][3];
-        float az[3][3], am[3][3];
-#pragma unroll
-        for (int a = 0; a < 3; ++a)
-#pragma unroll
-          for (int k = 0; k < 3; ++k) {
-            axy[a][k] = make_float2(0.f, 0.f);
-            az[a][k] = am[a][k] = 0.f;
-          }
-        int cur = -1;
-        const float2 np0 = dup2((float)p0);
-        for (int j = j0; j < j1; ++j) {
-          const float* R = pd + (wbase + j) * Y::STRIDE;
-          const int cc = __float_as_int(R[Y::OFF_CELL]);
-          if (cc != cur) {
-            if (cur >= 0) p2g_plane_flush(tile, Y::TN, cur, p0, axy, az, am);
-#pragma unroll
-            for (int a = 0; a < 3; ++a)
-#pragma unroll
-              for (int k = 0; k < 3; ++k) {
-                axy[a][k] = make_float2(0.f, 0.f);
-                az[a][k] = am[a][k] = 0.f;
-              }
-            cur = cc;
-          }
-          const float4 q0 = *(const float4*)R;
-          const float4 b1 = *(const float4*)(R + 4);   // Bx0 By0 Bx1 By1
-          const float4 b2 = *(const float4*)(R + 8);   // Bx2 By2 Bz0 Bz1
-          const float4 s1 = *(const float4*)(R + 12);  // Sxx Sxy Sxy Syy
-          const float4 s2 = *(const float4*)(R + 16);  // Sxz Syz Szz Bz2
-          const float2 wg0 = *(const float2*)(R + Y::OFF_WP + 2 * p0);
-          const float4 wl = *(const float4*)(R + Y::OFF_WL);
-          const float4 gl = *(const float4*)(R + Y::OFF_WL + 4);
-          const float wL[3] = {wl.x, wl.y, wl.z}, gL[3] = {gl.x, gl.y, gl.z};
-          // the plane's part of u = a + B n: a + B[:, 0] n0
-          const float2 uxy0 = ffma2(make_float2(b1.x, b1.y), np0, make_float2(q0.x, q0.y));
-          const float uz0 = fmaf(b2.z, (float)p0, q0.z);
-#pragma unroll
-          for (int n1 = 0; n1 < 3; ++n1) {
-            const float2 wg1 = *(const float2*)(R + Y::OFF_WP + 6 + 2 * n1);
-            const float cw = wg0.x * wg1.x, cg0 = wg0.y * wg1.x, cg1 = wg0.x * wg1.y;
-            const float2 cw2 = dup2(cw);
-            const float2 uxy = ffma2(make_float2(b1.z, b1.w), dup2((float)n1), uxy0);
-            const float2 Axy = ffma2(cw2, uxy, ffma2(make_float2(s1.x, s1.y), dup2(cg0),
-                                                     fmul2(make_float2(s1.z, s1.w), dup2(cg1))));
-            const float2 bkxy = fmul2(cw2, make_float2(b2.x, b2.y));
-            const float2 slxy = fmul2(cw2, make_float2(s2.x, s2.y));
-            const float2 A1xy = fadd2(Axy, bkxy), A2xy = ffma2(dup2(2.f), bkxy, Axy);
-            axy[n1][0] = ffma2(dup2(gL[0]), slxy, ffma2(dup2(wL[0]), Axy, axy[n1][0]));
-            axy[n1][1] = ffma2(dup2(gL[1]), slxy, ffma2(dup2(wL[1]), A1xy, axy[n1][1]));
-            axy[n1][2] = ffma2(dup2(gL[2]), slxy, ffma2(dup2(wL[2]), A2xy, axy[n1][2]));
-            const float uz = fmaf(b2.w, (float)n1, uz0);
-            const float Az = fmaf(cw, uz, fmaf(s2.x, cg0, s2.y * cg1));
-            const float bkz = cw * s2.w, slz = cw * s2.z;
-            az[n1][0] = fmaf(gL[0], slz, fmaf(wL[0], Az, az[n1][0]));
-            az[n1][1] = fmaf(gL[1], slz, fmaf(wL[1], Az + bkz, az[n1][1]));
-            az[n1][2] = fmaf(gL[2], slz, fmaf(wL[2], fmaf(2.f, bkz, Az), az[n1][2]));
-            const float cm = cw * q0.w;
-#pragma unroll
-            for (int k = 0; k < 3; ++k) am[n1][k] = fmaf(wL[k], cm, am[n1][k]);
-          }
-        }
-        if (cur >= 0) p2g_plane_flush(tile, Y::TN, cur, p0, axy, az, am);
-      }
-    } else if (D == 3) {
+    if (D == 3) {
       // 3D: SLOTS equal ranges of consecutive particles in one pass (11, 11,
       // 10); a range's sums go to the tile whenever its base cell changes
       if (q < Y::SLOTS) walk((q * nvalid) / Y::SLOTS, ((q + 1) * nvalid) / Y::SLOTS);

@@ -40,6 +40,9 @@ sys.path.insert(0, os.path.join(REPO, "adaptive-gimp_b200"))
 sys.path.insert(0, os.path.join(REPO, "oracle"))
 
 METRIC = "particle-substeps/s"
+# the end-to-end run takes at least this many substeps (a wall-clock figure
+# over a few milliseconds is dominated by host-side jitter)
+E2E_MIN_STEPS = 100
 FALLBACK_HBM_GBS = 6650.0
 # algorithmic bytes per particle-substep (f32 SoA), counted once per kernel
 BYTES = {  # (dim, with Jp) -> (P2G, G2P)
@@ -771,11 +774,12 @@ def e2e_batch(a, sc, local, tuning=None):
     sm, scp = ctypes.c_void_p(main_s.cuda_stream), ctypes.c_void_p(copy_s.cuda_stream)
     outs = [torch.empty((n_tot, 2), dtype=torch.float32, pin_memory=True).numpy() for _ in range(2)]
     done = [None, None]
+    steps = max(a.steps, E2E_MIN_STEPS)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     for sim, h in zip(sims, hosts):
         sim.set_particles(x=h["x"], v=h["v"], F=h["F"], C=h["C"], m=h["m"], g=h["g"])
-    for i in range(a.steps):
+    for i in range(steps):
         batch.substep(sc[0].dt, stream=sm)
         # every scene's x_p in one gathered copy on a copy stream, overlapping
         # the next substep; double-buffered
@@ -793,8 +797,8 @@ def e2e_batch(a, sc, local, tuning=None):
     for s in sims:
         s.close()
     h2d = sum(s.n * 4 * (2 * 2 + 2 * 4 + 2) for s in sc)
-    return {"value": n_tot * a.steps / el, "unit": METRIC, "h2d_bytes_per_step": h2d / a.steps,
-            "d2h_bytes_per_step": n_tot * 2 * 4,
+    return {"value": n_tot * steps / el, "unit": METRIC, "h2d_bytes_per_step": h2d / steps,
+            "d2h_bytes_per_step": n_tot * 2 * 4, "substeps": steps,
             "timing": "wall clock; every substep's positions of all scenes read back to pinned host memory in one "
                       "asynchronous gathered copy overlapping the next substep, double-buffered, all landed before "
                       "the clock stops",
@@ -822,6 +826,7 @@ def e2e_run(a, scene, local, sur=None, tuning=None):
     hg[:] = scene.g
     hJ[:] = 1
     outs = [pinned((n, d)), pinned((n, d))]
+    steps = max(a.steps, E2E_MIN_STEPS)
     sim = scene.build(device=local)
     if tuning:
         sim.set_tuning(tuning["chunk"], tuning["ctas_per_sm"])
@@ -834,7 +839,7 @@ def e2e_run(a, scene, local, sur=None, tuning=None):
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     sim.set_particles(x=hx, v=hv, F=hF, C=hC, m=hm, g=hg, Jp=hJ)
-    for i in range(a.steps):
+    for i in range(steps):
         if scene.refine_every and i % scene.refine_every == 0:
             sim.refine_levels(scene.refine_band, stream=sm)
         sim.substep(scene.dt, stream=sm)
@@ -853,8 +858,8 @@ def e2e_run(a, scene, local, sur=None, tuning=None):
     el = time.perf_counter() - t0
     sim.close()
     h2d = n * 4 * (2 * d + 2 * d * d + 3)
-    return {"value": n * a.steps / el, "unit": METRIC, "h2d_bytes_per_step": h2d / a.steps,
-            "d2h_bytes_per_step": n * d * 4,
+    return {"value": n * steps / el, "unit": METRIC, "h2d_bytes_per_step": h2d / steps,
+            "d2h_bytes_per_step": n * d * 4, "substeps": steps,
             "timing": "wall clock; every substep's x_p read back to pinned host memory (asynchronous copy on a "
                       "second stream overlapping the next substep, double-buffered, all landed before the clock stops)",
             "note": "h2d is the one-time upload of the scene state spread over the timed substeps"}
