@@ -71,22 +71,24 @@ __device__ __forceinline__ float2 dup2(float a) { return make_float2(a, a); }
 // ---------------------------------------------------------------------------
 // P2G (adaptive_gimp.py:230-250).  Per work item (up to CH particles of one
 // 4^d block of one level, in base-cell order: bins store their particles
-// sorted by cell):
+// sorted by cell, the last axis fastest):
 //  1. one thread per particle computes the scaled Kirchhoff stress S
 //     (utils.py:11-16, adaptive_gimp.py:240; symmetric, kirchhoff_sym), its
 //     per-axis GIMP weights and gradients, m, a = m (v - C (tc+1)) and
-//     B = m C, and its base cell inside the block, and stores them in shared
+//     B = m C, and its base cell inside the block, forms each node row's
+//     share A of the momentum term (below) and stores the record in shared
 //     memory at its thread index;
 //  2. each warp cuts its own 32 particles into ranges: in 3D SLOTS = 3
 //     contiguous ranges of equal length (11/11/10), which keeps every slot
 //     busy for the same number of steps; in 2D runs of one base cell (about 4
-//     particles), 10 at a time.  A lane owns one row of three stencil nodes
-//     (the last axis runs along the row; 3^(d-1) rows per cell) of one range
-//     and walks its particles.  While the base cell stays the same it sums
-//     w m and w (a + B n) + S grad w of its three nodes in registers (one read
-//     of a particle record serves three nodes, and the row's weight products
-//     are shared); when the cell changes, and at the end, the sums go into
-//     the (4+2)^d node tile in shared memory;
+//     particles), 10 at a time.  A lane owns one row of three
+//     stencil nodes (the last axis runs along the row; 3^(d-1) rows per cell)
+//     of one range and walks its particles, reading its row's float4 and the
+//     record's shared part (3D 18 floats, 2D 16, of 52 / 28).  It sums the
+//     three nodes' w m and w (a + B n) + S grad w in registers; when the base
+//     cell moves one or two cells along the row, the nodes left behind go to
+//     the (4+2)^d node tile in shared memory and the others move down the
+//     row; any other change, and the end, sends all three;
 //  3. a CTA takes a contiguous range of work items, so consecutive items of
 //     one block (a dense block holds many) keep summing into the same tile;
 //     when the next item is another block, the tile is flushed after one
@@ -99,40 +101,44 @@ struct P2GLayout {
   static constexpr int ROWS = (D == 2) ? 3 : 9;   // node rows per stencil
   static constexpr int SLOTS = 32 / ROWS;         // particle ranges served by one warp at once
   static constexpr int TN = (D == 2) ? 36 : 216;  // nodes of the (4+2)^d tile
-  // per-particle record (floats; pairs that the row sums read together sit at
-  // even offsets):
-  //  3D  0 a_x a_y a_z m | 4 Bx0 By0 Bx1 By1 | 8 Bx2 By2 Bz0 Bz1 | 12 Sxx Sxy Sxy Syy |
-  //     16 Sxz Syz Szz Bz2 | 20 (W0 G0)[0] (W0 G0)[1] | 24 (W0 G0)[2] (W1 G1)[0] |
-  //     28 (W1 G1)[1] (W1 G1)[2] | 32 W2[0..2] cell | 36 G2[0..2] -
-  //  2D  0 a_x a_y m cell | 4 Bx0 By0 Bx1 By1 | 8 Sxx Sxy Sxy Syy |
-  //     12 (W0 G0)[0] (W0 G0)[1] | 16 (W0 G0)[2] - - | 20 W1[0..2] - | 24 G1[0..2] -
-  static constexpr int STRIDE = (D == 3) ? 40 : 28;  // 16-byte aligned records
-  static constexpr int OFF_WP = (D == 3) ? 20 : 12;  // (W, G) pairs of the axes before the last
-  static constexpr int OFF_WL = (D == 3) ? 32 : 20;  // last axis: W[0..2], then G[0..2] at +4
-  static constexpr int OFF_CELL = (D == 3) ? 35 : 3;
+  // per-particle record (floats): one float4 per node row (a lane reads only
+  // its own row and the part every row shares):
+  //  3D  4 r: A_x A_y A_z cw of row r = 3 n0 + n1 (r < 9) | 36 Bk_x Bk_y Bk_z m |
+  //     40 SL_x SL_y SL_z cell | 44 W2[0..2] G2[0] | 48 G2[1] G2[2] - -
+  //  2D  4 r: A_x A_y cw cell of row r = n0 (r < 3) | 12 Bk_x Bk_y SL_x SL_y |
+  //     16 W1[0..2] m | 20 G1[0..2] - | 24 - - - -
+  // Strides are odd multiples of four floats: the float4 stores of eight
+  // consecutive threads (one shared-memory wavefront) fall in distinct banks.
+  static constexpr int STRIDE = (D == 3) ? 52 : 28;
   static constexpr int TMAX = 16;  // 2D: longest run of one base cell walked by one slot
   static constexpr size_t bytes() {
     return sizeof(float) * ((size_t)CH * STRIDE + 2 * 4 * TN) + sizeof(int) * (CH / 32) * 33;
   }
 };
 
-// A lane's three node sums of one base cell into the node tile ([4][TN]:
-// p_x, p_y, p_z, m).
+// Node k of a lane's row of base cell cc sits at tile index row_tile + k.
+template <int D>
+__device__ __forceinline__ int p2g_row_tile(int cc, int n0, int n1) {
+  if (D == 2) return (((cc >> 2) & 3) + n0) * 6 + (cc & 3);
+  return ((((cc >> 4) & 3) + n0) * 6 + ((cc >> 2) & 3) + n1) * 6 + (cc & 3);
+}
+
+// One node's sums into the node tile ([4][TN]: p_x, p_y, p_z, m).
+template <int D>
+__device__ __forceinline__ void p2g_node_flush(float* tile, int TN, int ti, float2 axy, float az, float am) {
+  atomicAdd(&tile[ti], axy.x);
+  atomicAdd(&tile[TN + ti], axy.y);
+  if (D == 3) atomicAdd(&tile[2 * TN + ti], az);
+  atomicAdd(&tile[3 * TN + ti], am);
+}
+
+// A lane's three node sums of one base cell into the node tile.
 template <int D>
 __device__ __forceinline__ void p2g_row_flush(float* tile, int TN, int cc, int n0, int n1, const float2* axy,
                                               const float* az, const float* am) {
-  int ti;
-  if (D == 2)
-    ti = (((cc >> 2) & 3) + n0) * 6 + (cc & 3);
-  else
-    ti = ((((cc >> 4) & 3) + n0) * 6 + ((cc >> 2) & 3) + n1) * 6 + (cc & 3);
+  const int ti = p2g_row_tile<D>(cc, n0, n1);
 #pragma unroll
-  for (int k = 0; k < 3; ++k) {
-    atomicAdd(&tile[ti + k], axy[k].x);
-    atomicAdd(&tile[TN + ti + k], axy[k].y);
-    if (D == 3) atomicAdd(&tile[2 * TN + ti + k], az[k]);
-    atomicAdd(&tile[3 * TN + ti + k], am[k]);
-  }
+  for (int k = 0; k < 3; ++k) p2g_node_flush<D>(tile, TN, ti + k, axy[k], az[k], am[k]);
 }
 
 template <int D, int CH>
@@ -241,26 +247,44 @@ __global__ void __launch_bounds__(CH, 1024 / CH) k_p2g(Batch B) {
       float4* P4 = (float4*)(pd + i * Y::STRIDE);
       const float cf = __int_as_float(cell);
       if (D == 3) {
-        P4[0] = make_float4(a[0], a[1], a[D - 1], mp);
-        P4[1] = make_float4(mp * Cm[0], mp * Cm[D], mp * Cm[1], mp * Cm[D + 1]);
-        P4[2] = make_float4(mp * Cm[2 % (D * D)], mp * Cm[(D + 2) % (D * D)], mp * Cm[(2 * D) % (D * D)],
-                            mp * Cm[(2 * D + 1) % (D * D)]);
-        P4[3] = make_float4(sc * tau[0], sc * tau[1], sc * tau[1], sc * tau[2]);
-        P4[4] = make_float4(sc * tau[3 % (D == 3 ? 6 : 3)], sc * tau[4 % (D == 3 ? 6 : 3)],
-                            sc * tau[5 % (D == 3 ? 6 : 3)], mp * Cm[(D * D - 1)]);
-        P4[5] = make_float4(W[0][0], G[0][0], W[0][1], G[0][1]);
-        P4[6] = make_float4(W[0][2], G[0][2], W[1][0], G[1][0]);
-        P4[7] = make_float4(W[1][1], G[1][1], W[1][2], G[1][2]);
-        P4[8] = make_float4(W[D - 1][0], W[D - 1][1], W[D - 1][2], cf);
-        P4[9] = make_float4(G[D - 1][0], G[D - 1][1], G[D - 1][2], 0.f);
+        // row r = 3 n0 + n1: A = cw (a + B[:,0] n0 + B[:,1] n1) + S[:,0] cg0 + S[:,1] cg1
+        // with cw = W0[n0] W1[n1], cg0 = G0[n0] W1[n1], cg1 = W0[n0] G1[n1]
+        const float Bx0 = mp * Cm[0], By0 = mp * Cm[D], Bz0 = mp * Cm[(2 * D) % (D * D)];
+        const float Bx1 = mp * Cm[1], By1 = mp * Cm[D + 1], Bz1 = mp * Cm[(2 * D + 1) % (D * D)];
+        const float Sxx = sc * tau[0], Sxy = sc * tau[1], Syy = sc * tau[2];
+        const float Sxz = sc * tau[3 % (D == 3 ? 6 : 3)], Syz = sc * tau[4 % (D == 3 ? 6 : 3)];
+        const float Szz = sc * tau[5 % (D == 3 ? 6 : 3)];
+#pragma unroll
+        for (int r0 = 0; r0 < 3; ++r0) {
+#pragma unroll
+          for (int r1 = 0; r1 < 3; ++r1) {
+            const float cw = W[0][r0] * W[1][r1], cg0 = G[0][r0] * W[1][r1], cg1 = W[0][r0] * G[1][r1];
+            const float fn0 = (float)r0, fn1 = (float)r1;
+            const float ux = fmaf(Bx1, fn1, fmaf(Bx0, fn0, a[0]));
+            const float uy = fmaf(By1, fn1, fmaf(By0, fn0, a[1]));
+            const float uz = fmaf(Bz1, fn1, fmaf(Bz0, fn0, a[D - 1]));
+            P4[3 * r0 + r1] = make_float4(fmaf(cw, ux, fmaf(Sxx, cg0, Sxy * cg1)),
+                                          fmaf(cw, uy, fmaf(Sxy, cg0, Syy * cg1)),
+                                          fmaf(cw, uz, fmaf(Sxz, cg0, Syz * cg1)), cw);
+          }
+        }
+        P4[9] = make_float4(mp * Cm[2 % (D * D)], mp * Cm[(D + 2) % (D * D)], mp * Cm[D * D - 1], mp);
+        P4[10] = make_float4(Sxz, Syz, Szz, cf);
+        P4[11] = make_float4(W[D - 1][0], W[D - 1][1], W[D - 1][2], G[D - 1][0]);
+        *(float2*)(P4 + 12) = make_float2(G[D - 1][1], G[D - 1][2]);
       } else {
-        P4[0] = make_float4(a[0], a[1], mp, cf);
-        P4[1] = make_float4(mp * Cm[0], mp * Cm[D], mp * Cm[1], mp * Cm[D + 1 < D * D ? D + 1 : 0]);
-        P4[2] = make_float4(sc * tau[0], sc * tau[1], sc * tau[1], sc * tau[2]);
-        P4[3] = make_float4(W[0][0], G[0][0], W[0][1], G[0][1]);
-        P4[4] = make_float4(W[0][2], G[0][2], 0.f, 0.f);
-        P4[5] = make_float4(W[D - 1][0], W[D - 1][1], W[D - 1][2], 0.f);
-        P4[6] = make_float4(G[D - 1][0], G[D - 1][1], G[D - 1][2], 0.f);
+        // row r = n0: A = cw (a + B[:,0] n0) + S[:,0] cg0 with cw = W0[n0], cg0 = G0[n0]
+        const float Bx0 = mp * Cm[0], By0 = mp * Cm[D];
+        const float Sxx = sc * tau[0], Sxy = sc * tau[1], Syy = sc * tau[2];
+#pragma unroll
+        for (int r0 = 0; r0 < 3; ++r0) {
+          const float cw = W[0][r0], cg0 = G[0][r0], fn0 = (float)r0;
+          const float ux = fmaf(Bx0, fn0, a[0]), uy = fmaf(By0, fn0, a[1]);
+          P4[r0] = make_float4(fmaf(cw, ux, Sxx * cg0), fmaf(cw, uy, Sxy * cg0), cw, cf);
+        }
+        P4[3] = make_float4(mp * Cm[1], mp * Cm[D + 1 < D * D ? D + 1 : 0], Sxy, Syy);
+        P4[4] = make_float4(W[D - 1][0], W[D - 1][1], W[D - 1][2], mp);
+        P4[5] = make_float4(G[D - 1][0], G[D - 1][1], G[D - 1][2], 0.f);
       }
     }
     __syncwarp();
@@ -268,7 +292,6 @@ __global__ void __launch_bounds__(CH, 1024 / CH) k_p2g(Batch B) {
     const int wbase = warp * 32;
     const int nvalid = max(0, min(32, wd.w - wbase));
     auto walk = [&](const int j0, const int j1) {
-      const float2 nn0 = dup2((float)n0), nn1 = dup2((float)n1);
       float2 axy[3];
       float az[3], am[3];
 #pragma unroll
@@ -280,84 +303,92 @@ __global__ void __launch_bounds__(CH, 1024 / CH) k_p2g(Batch B) {
 #pragma unroll 2
       for (int j = j0; j < j1; ++j) {
         const float* R = pd + (wbase + j) * Y::STRIDE;
-        const float4 q0 = *(const float4*)R;
-        const int cc = __float_as_int(R[Y::OFF_CELL]);
+        const float4 rw = *(const float4*)(R + 4 * row);  // this row's A (and cw, 2D: and the cell)
+        const float4 sl = D == 3 ? *(const float4*)(R + 40) : make_float4(0.f, 0.f, 0.f, 0.f);  // SL, cell
+        const int cc = __float_as_int(D == 3 ? sl.w : rw.w);
         if (cc != cur) {
-          if (cur >= 0) p2g_row_flush<D>(tile, Y::TN, cur, n0, n1, axy, az, am);
+          // Cells ascend with the row axis fastest: the next cell one or two
+          // steps further along the same line shares the row's last nodes,
+          // so only the nodes it leaves behind go to the tile and the others
+          // move down the row.
+          const int dz = cc - cur;
+          if (cur >= 0 && (cc >> 2) == (cur >> 2) && dz > 0 && dz < 3) {
+            const int ti = p2g_row_tile<D>(cur, n0, n1);
+            p2g_node_flush<D>(tile, Y::TN, ti, axy[0], az[0], am[0]);
+            if (dz == 2) p2g_node_flush<D>(tile, Y::TN, ti + 1, axy[1], az[1], am[1]);
+            const float2 zz = make_float2(0.f, 0.f);
+            axy[0] = dz == 1 ? axy[1] : axy[2];
+            az[0] = dz == 1 ? az[1] : az[2];
+            am[0] = dz == 1 ? am[1] : am[2];
+            axy[1] = dz == 1 ? axy[2] : zz;
+            az[1] = dz == 1 ? az[2] : 0.f;
+            am[1] = dz == 1 ? am[2] : 0.f;
+            axy[2] = zz;
+            az[2] = am[2] = 0.f;
+          } else {
+            if (cur >= 0) p2g_row_flush<D>(tile, Y::TN, cur, n0, n1, axy, az, am);
 #pragma unroll
-          for (int k = 0; k < 3; ++k) {
-            axy[k] = make_float2(0.f, 0.f);
-            az[k] = am[k] = 0.f;
+            for (int k = 0; k < 3; ++k) {
+              axy[k] = make_float2(0.f, 0.f);
+              az[k] = am[k] = 0.f;
+            }
           }
           cur = cc;
         }
-        const float4 wl = *(const float4*)(R + Y::OFF_WL);
-        const float4 gl = *(const float4*)(R + Y::OFF_WL + 4);
-        const float wL[3] = {wl.x, wl.y, wl.z}, gL[3] = {gl.x, gl.y, gl.z};
         // Node k of the row has weight cw wL[k] and gradient
         // (cg_0 wL[k], .., cg_{d-2} wL[k], cw gL[k]); its momentum term is
         //   w (a + B n) + S grad w = wL[k] (A + k Bk) + gL[k] s_L
-        // with A = cw (a + B n_row) + sum_{b<d-1} S[:, b] cg_b, Bk = cw B[:, d-1]
-        // and s_L = cw S[:, d-1]; the mass term is wL[k] cw m.
+        // with A = cw (a + B n_row) + sum_{b<d-1} S[:, b] cg_b (the record's
+        // row part), Bk = cw B[:, d-1] and s_L = cw S[:, d-1]; the mass term
+        // is wL[k] cw m.
+        float wL[3], gL[3], cw, mp;
+        float2 Axy, bkxy, slxy;
         if (D == 3) {
-          const float4 b1 = *(const float4*)(R + 4);   // Bx0 By0 Bx1 By1
-          const float4 b2 = *(const float4*)(R + 8);   // Bx2 By2 Bz0 Bz1
-          const float4 s1 = *(const float4*)(R + 12);  // Sxx Sxy Sxy Syy
-          const float4 s2 = *(const float4*)(R + 16);  // Sxz Syz Szz Bz2
-          const float2 wg0 = *(const float2*)(R + Y::OFF_WP + 2 * n0);
-          const float2 wg1 = *(const float2*)(R + Y::OFF_WP + 6 + 2 * n1);
-          const float cw = wg0.x * wg1.x, cg0 = wg0.y * wg1.x, cg1 = wg0.x * wg1.y;
-          const float2 cw2 = dup2(cw);
-          // x, y channels as pairs
-          const float2 uxy = ffma2(make_float2(b1.z, b1.w), nn1, ffma2(make_float2(b1.x, b1.y), nn0,
-                                                                       make_float2(q0.x, q0.y)));
-          const float2 Axy = ffma2(cw2, uxy, ffma2(make_float2(s1.x, s1.y), dup2(cg0),
-                                                   fmul2(make_float2(s1.z, s1.w), dup2(cg1))));
-          const float2 bkxy = fmul2(cw2, make_float2(b2.x, b2.y));
-          const float2 slxy = fmul2(cw2, make_float2(s2.x, s2.y));
-          const float2 A1xy = fadd2(Axy, bkxy), A2xy = ffma2(dup2(2.f), bkxy, Axy);
-          axy[0] = ffma2(dup2(gL[0]), slxy, ffma2(dup2(wL[0]), Axy, axy[0]));
-          axy[1] = ffma2(dup2(gL[1]), slxy, ffma2(dup2(wL[1]), A1xy, axy[1]));
-          axy[2] = ffma2(dup2(gL[2]), slxy, ffma2(dup2(wL[2]), A2xy, axy[2]));
-          // z channel (S symmetric: S[z][0] = Sxz, S[z][1] = Syz) and mass
-          const float uz = fmaf(b2.w, (float)n1, fmaf(b2.z, (float)n0, q0.z));
-          const float Az = fmaf(cw, uz, fmaf(s2.x, cg0, s2.y * cg1));
-          const float bkz = cw * s2.w, slz = cw * s2.z;
+          const float4 bm = *(const float4*)(R + 36);           // Bk_x Bk_y Bk_z m
+          const float4 wl = *(const float4*)(R + 44);           // W2[0..2] G2[0]
+          const float2 gh = *(const float2*)(R + 48);           // G2[1] G2[2]
+          wL[0] = wl.x, wL[1] = wl.y, wL[2] = wl.z;
+          gL[0] = wl.w, gL[1] = gh.x, gL[2] = gh.y;
+          cw = rw.w;
+          mp = bm.w;
+          Axy = make_float2(rw.x, rw.y);
+          bkxy = fmul2(dup2(cw), make_float2(bm.x, bm.y));
+          slxy = fmul2(dup2(cw), make_float2(sl.x, sl.y));
+          const float Az = rw.z, bkz = cw * bm.z, slz = cw * sl.z;
           az[0] = fmaf(gL[0], slz, fmaf(wL[0], Az, az[0]));
           az[1] = fmaf(gL[1], slz, fmaf(wL[1], Az + bkz, az[1]));
           az[2] = fmaf(gL[2], slz, fmaf(wL[2], fmaf(2.f, bkz, Az), az[2]));
-          const float cm = cw * q0.w;
-#pragma unroll
-          for (int k = 0; k < 3; ++k) am[k] = fmaf(wL[k], cm, am[k]);
         } else {
-          const float4 b1 = *(const float4*)(R + 4);  // Bx0 By0 Bx1 By1
-          const float4 s1 = *(const float4*)(R + 8);  // Sxx Sxy Sxy Syy
-          const float2 wg0 = *(const float2*)(R + Y::OFF_WP + 2 * n0);
-          const float cw = wg0.x, cg0 = wg0.y;
-          const float2 cw2 = dup2(cw);
-          const float2 uxy = ffma2(make_float2(b1.x, b1.y), nn0, make_float2(q0.x, q0.y));
-          const float2 Axy = ffma2(cw2, uxy, fmul2(make_float2(s1.x, s1.y), dup2(cg0)));
-          const float2 bkxy = fmul2(cw2, make_float2(b1.z, b1.w));
-          const float2 slxy = fmul2(cw2, make_float2(s1.z, s1.w));
-          const float2 A1xy = fadd2(Axy, bkxy), A2xy = ffma2(dup2(2.f), bkxy, Axy);
-          axy[0] = ffma2(dup2(gL[0]), slxy, ffma2(dup2(wL[0]), Axy, axy[0]));
-          axy[1] = ffma2(dup2(gL[1]), slxy, ffma2(dup2(wL[1]), A1xy, axy[1]));
-          axy[2] = ffma2(dup2(gL[2]), slxy, ffma2(dup2(wL[2]), A2xy, axy[2]));
-          const float cm = cw * q0.z;
-#pragma unroll
-          for (int k = 0; k < 3; ++k) am[k] = fmaf(wL[k], cm, am[k]);
+          const float4 bs = *(const float4*)(R + 12);  // Bk_x Bk_y SL_x SL_y
+          const float4 wl = *(const float4*)(R + 16);  // W1[0..2] m
+          const float4 gl = *(const float4*)(R + 20);  // G1[0..2]
+          wL[0] = wl.x, wL[1] = wl.y, wL[2] = wl.z;
+          gL[0] = gl.x, gL[1] = gl.y, gL[2] = gl.z;
+          cw = rw.z;
+          mp = wl.w;
+          Axy = make_float2(rw.x, rw.y);
+          bkxy = fmul2(dup2(cw), make_float2(bs.x, bs.y));
+          slxy = fmul2(dup2(cw), make_float2(bs.z, bs.w));
         }
+        const float2 A1xy = fadd2(Axy, bkxy), A2xy = ffma2(dup2(2.f), bkxy, Axy);
+        axy[0] = ffma2(dup2(gL[0]), slxy, ffma2(dup2(wL[0]), Axy, axy[0]));
+        axy[1] = ffma2(dup2(gL[1]), slxy, ffma2(dup2(wL[1]), A1xy, axy[1]));
+        axy[2] = ffma2(dup2(gL[2]), slxy, ffma2(dup2(wL[2]), A2xy, axy[2]));
+        const float cm = cw * mp;
+#pragma unroll
+        for (int k = 0; k < 3; ++k) am[k] = fmaf(wL[k], cm, am[k]);
       }
       if (cur >= 0) p2g_row_flush<D>(tile, Y::TN, cur, n0, n1, axy, az, am);
     };
     if (D == 3) {
       // 3D: SLOTS equal ranges of consecutive particles in one pass (11, 11,
-      // 10); a range's sums go to the tile whenever its base cell changes
+      // 10)
       if (q < Y::SLOTS) walk((q * nvalid) / Y::SLOTS, ((q + 1) * nvalid) / Y::SLOTS);
     } else {
       // 2D: runs of one base cell (found with ballots, at most TMAX long; a
       // cell holds about 4 particles), SLOTS runs at a time, one tile update
-      // per run
+      // per run (equal ranges of 3-4 particles would mostly straddle two
+      // cells: twice the tile updates)
       const bool valid = lane < nvalid;
       const int prev = __shfl_up_sync(0xffffffffu, cell, 1);
       const unsigned runs = __ballot_sync(0xffffffffu, valid && (lane == 0 || cell != prev));
@@ -1320,10 +1351,234 @@ __device__ __forceinline__ void g2p_one(const Ctx& c, int j) {
   }
 }
 
+// 2D G2P: one thread per particle slot, grid-stride (a 2D block holds about
+// one work item, too little to pay for staging its nodes).
 template <int D>
-__global__ void __launch_bounds__(256, 4) k_g2p(Batch B) {
+__global__ void __launch_bounds__(256, 4) k_g2p_gather(Batch B) {
   SCENE_CTA(B, MAP_G);
   SCENE_LOOP(j, c.N) g2p_one<D>(c, (int)j);
+}
+
+// The new state of particle p (slot j of this substep's bin order) whose
+// base cell lies in the block with first node O, from the block's staged
+// node velocities: txy[t] = (v_x, v_y), tz[t] = v_z of tile node t (the
+// (4+2)^d nodes O..O+5, last axis fastest).
+template <int D>
+__device__ __forceinline__ void g2p_staged(const Ctx& c, int l, int p, int j, const float* xp, const int* O,
+                                           const float2* txy, const float* tz) {
+  const float pw = (D == 2) ? 0.25f : 0.125f;
+  const float rd = (D == 2) ? c.radius * c.radius : c.radius * c.radius * c.radius;
+  const long long N = c.N;
+  const float inv = (float)(c.coarsest << l);
+  const float dx = 1.f / inv;
+  float tc[D];
+  int t0 = 0;
+  bool inside = true;
+#pragma unroll
+  for (int d = 0; d < D; ++d) {
+    const float xs = xp[d] * inv;
+    const int base = (int)(xs + 0.5f) - 1;
+    tc[d] = xs - (float)(base + 1);
+    // the binning put the base cell in this block; a cell outside it would
+    // read another tile's nodes, so it is clamped and reported
+    int r = base - O[d];
+    inside = inside && r >= 0 && r <= 3;
+    r = min(max(r, 0), 3);
+    t0 = t0 * 6 + r;
+  }
+  if (!inside) set_err(c, ERR_OOB);
+  const bool half = c.radius == 0.5f;
+  float W2[3], G2[3];
+  if (half)
+    axis_weights_half(tc[D - 1], W2, G2);
+  else
+    axis_weights(tc[D - 1], c.radius, W2, G2);
+  auto axis_factor = [&](float t, int k, float& w, float& g) {
+    if (half) {
+      const float a = 0.5f - t, b = 0.5f + t;
+      w = k == 0 ? a * a : (k == 1 ? fmaf(-2.f * t, t, 1.5f) : b * b);
+      g = k == 0 ? -a : (k == 1 ? -2.f * t : b);
+    } else {
+      float Wk[3], Gk[3];
+      axis_weights(t, c.radius, Wk, Gk);
+      w = k == 0 ? Wk[0] : (k == 1 ? Wk[1] : Wk[2]);
+      g = k == 0 ? Gk[0] : (k == 1 ? Gk[1] : Gk[2]);
+    }
+  };
+  const float r2 = 2.f * c.radius;
+  const float kw = (D == 2) ? 1.f / (4.f * r2 * r2) : 1.f / (8.f * r2 * r2 * r2);
+  const float kg = (D == 2) ? 1.f / (2.f * r2 * r2) : 1.f / (4.f * r2 * r2 * r2);
+  float nv[D], G[D * D];
+#pragma unroll
+  for (int i = 0; i < D; ++i) nv[i] = 0.f;
+#pragma unroll
+  for (int i = 0; i < D * D; ++i) G[i] = 0.f;
+  // Rows along the last axis: a row's nodes are summed with the last axis's
+  // weight (S) and gradient (T) first; the other axes' factors are applied
+  // once per row.
+#pragma unroll
+  for (int n0 = 0; n0 < 3; ++n0) {
+    float w0, g0;
+    axis_factor(tc[0], n0, w0, g0);
+#pragma unroll
+    for (int n1 = 0; n1 < ((D == 2) ? 1 : 3); ++n1) {
+      const int tr = t0 + n0 * ((D == 2) ? 6 : 36) + ((D == 2) ? 0 : n1 * 6);
+      float2 Sxy = make_float2(0.f, 0.f), Txy = make_float2(0.f, 0.f);
+      float Sz = 0.f, Tz = 0.f;
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        const float2 v = txy[tr + k];
+        Sxy = ffma2(v, dup2(W2[k]), Sxy);
+        Txy = ffma2(v, dup2(G2[k]), Txy);
+        if (D == 3) {
+          const float vz = tz[tr + k];
+          Sz = fmaf(vz, W2[k], Sz);
+          Tz = fmaf(vz, G2[k], Tz);
+        }
+      }
+      const float S[3] = {Sxy.x, Sxy.y, Sz}, T[3] = {Txy.x, Txy.y, Tz};
+      // row factors: weight, and the gradient components of the other axes
+      float cw, cg[D];
+      if (D == 2) {
+        cw = w0 * kw;
+        cg[0] = g0 * kg;
+        cg[1] = w0 * kg;
+      } else {
+        float w1, g1;
+        axis_factor(tc[1], n1, w1, g1);
+        const float wxy = w0 * w1;
+        cw = wxy * kw;
+        cg[0] = g0 * w1 * kg;
+        cg[1] = w0 * g1 * kg;
+        cg[D - 1] = wxy * kg;
+      }
+#pragma unroll
+      for (int i = 0; i < D; ++i) {
+        nv[i] = fmaf(cw, S[i], nv[i]);
+#pragma unroll
+        for (int q = 0; q < D - 1; ++q) G[i * D + q] = fmaf(cg[q], S[i], G[i * D + q]);
+        G[i * D + D - 1] = fmaf(cg[D - 1], T[i], G[i * D + D - 1]);
+      }
+    }
+  }
+#pragma unroll
+  for (int d = 0; d < D; ++d) {
+    __stwb(&c.Q.v[d * N + j], nv[d]);
+    __stwb(&c.Q.x[d * N + j], xp[d] + c.dt * nv[d]);
+  }
+#pragma unroll
+  for (int i = 0; i < D * D; ++i) __stwb(&c.Q.C[i * N + j], G[i]);
+  // m, g, id and Jp travel unchanged
+  __stwb(&c.Q.m[j], __ldg(&c.P.m[p]));
+  __stwb(&c.Q.g[j], __ldg(&c.P.g[p]));
+  __stwb(&c.Q.id[j], __ldg(&c.P.id[p]));
+  __stwb(&c.Q.Jp[j], c.plast == 1 ? __ldg(&c.P.Jp[p]) : 1.f);
+  __stwb(&c.Q.fl[j], l);
+  float F[D * D];
+#pragma unroll
+  for (int k = 0; k < D * D; ++k) F[k] = __ldg(&c.P.F[k * N + p]);
+  const float s = (c.dt * pw) / (rd * dx);
+  // F' = (I + s G) F row by row, each row stored at once; the Gram matrix
+  // F'^T F' is summed from the rows for the return-map test below
+  float Sg[(D == 2) ? 3 : 6];
+#pragma unroll
+  for (int k = 0; k < ((D == 2) ? 3 : 6); ++k) Sg[k] = 0.f;
+#pragma unroll
+  for (int i = 0; i < D; ++i) {
+    float row[D];
+#pragma unroll
+    for (int q = 0; q < D; ++q) {
+      float a = 0.f;
+#pragma unroll
+      for (int k = 0; k < D; ++k) a += ((i == k ? 1.f : 0.f) + s * G[i * D + k]) * F[k * D + q];
+      row[q] = a;
+      __stwb(&c.Q.F[(i * D + q) * N + j], a);
+    }
+    int u = 0;
+#pragma unroll
+    for (int a = 0; a < D; ++a)
+#pragma unroll
+      for (int b = a; b < D; ++b) Sg[u++] += row[a] * row[b];
+  }
+  // trial states that may leave the elastic interval get the return map in
+  // k_project (it needs an SVD, whose registers would halve G2P's occupancy);
+  // det F' = det(I + s G) det F
+  if (c.plast == 1) {
+    float A[D * D];
+#pragma unroll
+    for (int i = 0; i < D; ++i)
+#pragma unroll
+      for (int k = 0; k < D; ++k) A[i * D + k] = (i == k ? 1.f : 0.f) + s * G[i * D + k];
+    if (!gram_within<D>(Sg, det<D>(A) * det<D>(F), 1.f - c.theta_c, 1.f + c.theta_s))
+      c.proj[reserve_slot(&c.ctr[CTR_PROJ])] = j;
+  }
+}
+
+// 3D G2P (adaptive_gimp.py:289-321) over the P2G work items: a CTA takes a
+// contiguous range of them (up to CH particles of one 4^3 block each); when
+// the block changes it stages the block's 6^3 node velocities in shared
+// memory (two tiles alternate, so one barrier per block suffices: a thread
+// that passed the previous barrier has finished reading the tile from two
+// blocks ago), and each thread then computes one particle from the tile.
+// Particles without a level (the extra bin) are copied unchanged.
+template <int D, int CH>
+__global__ void __launch_bounds__(CH, 1024 / CH) k_g2p(Batch B) {
+  SCENE_CTA(B, MAP_G);
+  constexpr int TN = (D == 2) ? 36 : 216;
+  __shared__ float2 txy[2][TN];
+  __shared__ float tz[2][(D == 3) ? TN : 1];
+  const int nch = c.ctr[CTR_CHUNKS];
+  const int per = (nch + nblk_ - 1) / nblk_;
+  const int c0 = bid_ * per, c1 = min(nch, c0 + per);
+  const long long N = c.N;
+  int tb = 1, tl = -1, tk = -1;
+  for (int ch = c0; ch < c1; ++ch) {
+    const int4 wd = c.chunks[ch];
+    const int i = threadIdx.x, j = wd.z + i;
+    const bool mine = i < wd.w;
+    if (wd.x < 0) {  // uniform over the CTA
+      if (mine) copy_particle<D>(c, __ldg(&c.perm[j]), j);
+      continue;
+    }
+    const int l = wd.x;
+    const LevelDev& V = c.lev[l];
+    int O[D];
+    chunk_origin<D>(V, wd.y, O);
+    // the particle's position and the fields read after the gather start
+    // moving before the tile load, so both latencies overlap
+    int p = 0;
+    float xp[D];
+    if (mine) {
+      p = __ldg(&c.perm[j]);
+#pragma unroll
+      for (int d = 0; d < D; ++d) xp[d] = __ldg(&c.P.x[d * N + p]);
+#pragma unroll
+      for (int k = 0; k < D * D; ++k) asm volatile("prefetch.global.L1 [%0];" ::"l"(&c.P.F[k * N + p]));
+      asm volatile("prefetch.global.L1 [%0];" ::"l"(&c.P.m[p]));
+      asm volatile("prefetch.global.L1 [%0];" ::"l"(&c.P.g[p]));
+      asm volatile("prefetch.global.L1 [%0];" ::"l"(&c.P.id[p]));
+      if (c.plast == 1) asm volatile("prefetch.global.L1 [%0];" ::"l"(&c.P.Jp[p]));
+    }
+    if (l != tl || wd.y != tk) {  // uniform over the CTA
+      tb ^= 1;
+      tl = l;
+      tk = wd.y;
+      for (int t = threadIdx.x; t < TN; t += CH) {
+        int I[D], r = t;
+#pragma unroll
+        for (int d = D - 1; d >= 0; --d) {
+          I[d] = O[d] + r % 6;
+          r /= 6;
+        }
+        float4 nd = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (in_store<D>(V, I)) nd = __ldg(&V.node[elem_of<D>(V, I)]);
+        txy[tb][t] = make_float2(nd.x, nd.y);
+        if (D == 3) tz[tb][t] = nd.z;
+      }
+      __syncthreads();
+    }
+    if (mine) g2p_staged<D>(c, l, p, j, xp, O, txy[tb], tz[tb]);
+  }
 }
 
 // Snow return map (extension) of the particles G2P listed: the trial state
@@ -1376,6 +1631,21 @@ static void launch_p2g(const BatchLaunch& bl, cudaStream_t s, bool pdl) {
 }
 
 template <int D>
+static void launch_g2p(const BatchLaunch& bl, cudaStream_t s, bool pdl) {
+  const int G = bl.nct[MAP_G];
+  if constexpr (D == 2) {
+    launch_k(pdl, k_g2p_gather<D>, G, 256, 0, s, bl.b);
+  } else {
+    switch (bl.chunk) {
+      case 64: launch_k(pdl, k_g2p<D, 64>, G, 64, 0, s, bl.b); break;
+      case 128: launch_k(pdl, k_g2p<D, 128>, G, 128, 0, s, bl.b); break;
+      case 512: launch_k(pdl, k_g2p<D, 512>, G, 512, 0, s, bl.b); break;
+      default: launch_k(pdl, k_g2p<D, 256>, G, 256, 0, s, bl.b); break;
+    }
+  }
+}
+
+template <int D>
 void launch_transfer(const BatchLaunch& bl, cudaStream_t s, cudaEvent_t* ev) {
   const int G = bl.nct[MAP_G];
   const bool pdl = bl.pdl && !ev;
@@ -1402,7 +1672,7 @@ void launch_transfer(const BatchLaunch& bl, cudaStream_t s, cudaEvent_t* ev) {
       launch_k(pdl, k_prolong_gather<D>, G, 256, 0, s, bl.b, l);
   }
   if (ev) cudaEventRecord(ev[7], s);
-  launch_k(pdl, k_g2p<D>, G, 256, 0, s, bl.b);
+  launch_g2p<D>(bl, s, pdl);
   if (bl.any_plastic) launch_k(pdl, k_project<D>, G, 256, 0, s, bl.b);
   if (bl.sur) {
     launch_mlp_forward_dev(bl.mlp_packed, bl.mlp_P, bl.sur_X, bl.sur_Y, bl.sur_n, bl.sur_cap, bl.sur_err, bl.sms, s);
