@@ -159,7 +159,7 @@ __host__ __device__ __forceinline__ void snow_features(const float* sig, float j
 // ---------------------------------------------------------------------------
 // index helpers
 template <int D>
-__device__ __forceinline__ bool in_store(const LevelDev& V, const int* I) {
+__host__ __device__ __forceinline__ bool in_store(const LevelDev& V, const int* I) {
 #pragma unroll
   for (int d = 0; d < D; ++d)
     if ((unsigned)(I[d] + HALO) >= (unsigned)(4 * V.nb)) return false;
@@ -169,7 +169,7 @@ __device__ __forceinline__ bool in_store(const LevelDev& V, const int* I) {
 // Element and block indices fit in 32 bits (agimp_create rejects lattices of
 // more than 2^31 elements per level), so the index arithmetic is 32-bit.
 template <int D>
-__device__ __forceinline__ long long elem_of(const LevelDev& V, const int* I) {
+__host__ __device__ __forceinline__ long long elem_of(const LevelDev& V, const int* I) {
   unsigned b = 0, loc = 0;
 #pragma unroll
   for (int d = 0; d < D; ++d) {
@@ -179,6 +179,44 @@ __device__ __forceinline__ long long elem_of(const LevelDev& V, const int* I) {
   }
   return (long long)((b << (2 * D)) | loc);
 }
+
+// The 2^D elements I0 + {0,1}^D of one level (corner a adds bit D-1-d of a
+// on axis d, the order of the corner loops): each axis's share of the
+// element index (block part and local part) is formed once for I0[d] and
+// I0[d] + 1, so a corner costs D-1 additions instead of a full elem_of.
+template <int D>
+struct Corners {
+  unsigned t[D][2];
+  bool v[D][2];
+  __host__ __device__ __forceinline__ Corners(const LevelDev& V, const int* I0) {
+    const unsigned nb = (unsigned)V.nb;
+    unsigned m = 1;  // nb^(D-1-d)
+#pragma unroll
+    for (int d = D - 1; d >= 0; --d) {
+#pragma unroll
+      for (int k = 0; k < 2; ++k) {
+        const unsigned a = (unsigned)(I0[d] + k + HALO);
+        v[d][k] = a < 4u * nb;
+        t[d][k] = (((a >> 2) * m) << (2 * D)) | ((a & 3u) << (2 * (D - 1 - d)));
+      }
+      m *= nb;
+    }
+  }
+  // element index of corner a (equal to elem_of of I0 + corner offsets)
+  __host__ __device__ __forceinline__ unsigned idx(int a) const {
+    unsigned r = 0;
+#pragma unroll
+    for (int d = 0; d < D; ++d) r += t[d][(a >> (D - 1 - d)) & 1];
+    return r;
+  }
+  // corner a lies in the store (in_store)
+  __host__ __device__ __forceinline__ bool ok(int a) const {
+    bool r = true;
+#pragma unroll
+    for (int d = 0; d < D; ++d) r = r && v[d][(a >> (D - 1 - d)) & 1];
+    return r;
+  }
+};
 
 template <int D>
 __device__ __forceinline__ long long block_of(const LevelDev& V, const int* I) {
@@ -256,6 +294,44 @@ __device__ __forceinline__ bool decode_elem(const Ctx& c, int l0, int l1, long l
     bi -= n;
   }
   return false;
+}
+
+// First entry of each level's active blocks in the level-by-level block
+// numbering (s[q] = active blocks of the levels below q, s[L] = all of them),
+// read from the counters once per CTA: the per-element loops then decode an
+// element from shared memory instead of re-reading the counters.  Every
+// thread of the CTA calls it (it ends with a barrier).
+struct BlockRanges {
+  int s[MAXL + 1];
+};
+
+__device__ __forceinline__ void load_block_ranges(const Ctx& c, BlockRanges& r) {
+  if (threadIdx.x == 0) {
+    int t = 0;
+    for (int q = 0; q < c.L; ++q) {
+      r.s[q] = t;
+      t += c.ctr[CTR_LEVEL + q];
+    }
+    r.s[c.L] = t;
+  }
+  __syncthreads();
+}
+
+// element e of the active blocks of levels [l0, l1): its level, stored
+// block and local index (decode_elem through the CTA's BlockRanges)
+template <int D>
+__device__ __forceinline__ void decode_elem_r(const Ctx& c, const BlockRanges& r, int l0, int l1, long long e, int& l,
+                                              long long& blk, int& loc) {
+  const int bi = (int)(e >> (2 * D)) + r.s[l0];
+  loc = (int)(e & ((1 << (2 * D)) - 1));
+  int q = l0;
+  while (q + 1 < l1 && bi >= r.s[q + 1]) ++q;
+  l = q;
+  blk = c.lev[q].blist[bi - r.s[q]];
+}
+
+__device__ __forceinline__ long long total_elems_r(const BlockRanges& r, int l0, int l1, int D) {
+  return (long long)(r.s[l1] - r.s[l0]) << (2 * D);
 }
 
 __device__ __forceinline__ long long total_elems(const Ctx& c, int l0, int l1, int D) {

@@ -54,11 +54,13 @@ __global__ void k_clear(Batch B) {
     c.ctr[CTR_PROJ] = 0;
     c.ctr[CTR_FULL] = 0;
   }
-  const long long tot = total_elems(c, 0, c.L, D);
+  __shared__ BlockRanges br;
+  load_block_ranges(c, br);
+  const long long tot = total_elems_r(br, 0, c.L, D);
   SCENE_LOOP(e, tot) {
     int l, loc;
     long long blk;
-    decode_elem<D>(c, 0, c.L, e, l, blk, loc);
+    decode_elem_r<D>(c, br, 0, c.L, e, l, blk, loc);
     const LevelDev& V = c.lev[l];
     const long long idx = (blk << (2 * D)) | loc;
     V.cell[idx] = 0u;
@@ -369,11 +371,13 @@ template <int D>
 __global__ void k_mark_hier(Batch B) {
   SCENE_CTA(B, MAP_G);
   if (c.is_static) return;  // static mode has no culling (adaptive_gimp.py:335-337)
-  const long long tot = total_elems(c, 1, c.L, D);
+  __shared__ BlockRanges br;
+  load_block_ranges(c, br);
+  const long long tot = total_elems_r(br, 1, c.L, D);
   SCENE_LOOP(e, tot) {
     int l, loc;
     long long blk;
-    decode_elem<D>(c, 1, c.L, e, l, blk, loc);
+    decode_elem_r<D>(c, br, 1, c.L, e, l, blk, loc);
     const LevelDev& V = c.lev[l];
     const uint32_t v = V.cell[(blk << (2 * D)) | loc];
     if (!(v & ACT)) continue;
@@ -414,11 +418,13 @@ __global__ void k_resolve(Batch B) {
     if (c.is_static)
       for (int w = 0; w < ((D == 2) ? 1 : 5); ++w) c.touch_occ[(long long)key * ((D == 2) ? 1 : 5) + w] = 0u;
   }
-  const long long tot = total_elems(c, 0, c.L, D);
+  __shared__ BlockRanges br;
+  load_block_ranges(c, br);
+  const long long tot = total_elems_r(br, 0, c.L, D);
   SCENE_LOOP(e, tot) {
     int l, loc;
     long long blk;
-    decode_elem<D>(c, 0, c.L, e, l, blk, loc);
+    decode_elem_r<D>(c, br, 0, c.L, e, l, blk, loc);
     const LevelDev& V = c.lev[l];
     const long long idx = (blk << (2 * D)) | loc;
     const uint32_t v = V.cell[idx];
@@ -458,11 +464,13 @@ __global__ void k_resolve(Batch B) {
 template <int D>
 __global__ void k_ghost_tj(Batch B) {
   SCENE_CTA(B, MAP_G);
-  const long long tot = total_elems(c, 0, c.L, D);
+  __shared__ BlockRanges br;
+  load_block_ranges(c, br);
+  const long long tot = total_elems_r(br, 0, c.L, D);
   SCENE_LOOP(e, tot) {
     int l, loc;
     long long blk;
-    decode_elem<D>(c, 0, c.L, e, l, blk, loc);
+    decode_elem_r<D>(c, br, 0, c.L, e, l, blk, loc);
     const LevelDev& V = c.lev[l];
     if (V.cell[(blk << (2 * D)) | loc] != ACT) continue;
     int I[D];
@@ -528,11 +536,13 @@ __global__ void k_ghost_tj(Batch B) {
 template <int D>
 __global__ void k_level_masks(Batch B) {
   SCENE_CTA(B, MAP_G);
-  const long long tot = total_elems(c, 0, c.L - 1, D);
+  __shared__ BlockRanges br;
+  load_block_ranges(c, br);
+  const long long tot = total_elems_r(br, 0, c.L - 1, D);
   SCENE_LOOP(e, tot) {
     int l, loc;
     long long blk;
-    decode_elem<D>(c, 0, c.L - 1, e, l, blk, loc);
+    decode_elem_r<D>(c, br, 0, c.L - 1, e, l, blk, loc);
     const LevelDev& V = c.lev[l];
     int I[D];
     elem_coords<D>(V, blk, loc, I);
@@ -549,8 +559,10 @@ __global__ void k_level_masks(Batch B) {
 // of base).  Particles without a level go to one extra bin after all block
 // bins, so that every particle gets a slot in the new order.  The rank inside
 // the bin comes from a warp-aggregated atomic.
+// lb: lb[l] = bins of the levels below l (block bins are numbered level by
+// level); lb[L] = all block bins, the index of the extra bin
 template <int D>
-__device__ __forceinline__ void bin_one(const Ctx& c, int p) {
+__device__ __forceinline__ void bin_one(const Ctx& c, int p, const int* lb) {
   const int lane = threadIdx.x & 31;
   int bin = -1;
   if (p < c.N) {
@@ -562,8 +574,6 @@ __device__ __forceinline__ void bin_one(const Ctx& c, int p) {
       if (!(xp[d] >= 0.f && xp[d] < 1.f)) esc = true;
     }
     int fl = -1;
-    int nbins = 0;
-    for (int q = 0; q < c.L; ++q) nbins += c.ctr[CTR_LEVEL + q];
     if (!esc) {
       // the finest level with an ACTIVATED cell: search from the finest down
       for (int l = c.L - 1; l >= 0 && fl < 0; --l) {
@@ -571,13 +581,11 @@ __device__ __forceinline__ void bin_one(const Ctx& c, int p) {
         int base[D];
 #pragma unroll
         for (int d = 0; d < D; ++d) base[d] = (int)(xp[d] * inv + 0.5f) - 1;
+        const LevelDev& V = c.lev[l];
+        const Corners<D> K(V, base);
 #pragma unroll
-        for (int a = 0; a < (1 << D); ++a) {
-          int I[D];
-#pragma unroll
-          for (int d = 0; d < D; ++d) I[d] = base[d] + ((a >> (D - 1 - d)) & 1);
-          if (cell_get<D>(c, l, I) == ACT) fl = l;
-        }
+        for (int a = 0; a < (1 << D); ++a)
+          if (K.ok(a) && V.cell[K.idx(a)] == ACT) fl = l;
       }
       if (fl >= 0) {
         const float inv = (float)(c.coarsest << fl);
@@ -598,13 +606,11 @@ __device__ __forceinline__ void bin_one(const Ctx& c, int p) {
           set_err(c, ERR_NOBIN);
           fl = -1;
         } else {
-          int lb = 0;
-          for (int q = 0; q < fl; ++q) lb += c.ctr[CTR_LEVEL + q];
-          bin = ((lb + bi) << (2 * D)) | cell;
+          bin = ((lb[fl] + bi) << (2 * D)) | cell;
         }
       }
     }
-    if (fl < 0) bin = nbins << (2 * D);  // the extra bin
+    if (fl < 0) bin = lb[c.L] << (2 * D);  // the extra bin
     c.P.fl[p] = fl;
   }
   // bin sizes and the rank inside the (bin, cell): warp-aggregated atomics
@@ -628,7 +634,17 @@ __device__ __forceinline__ void bin_one(const Ctx& c, int p) {
 template <int D>
 __global__ void k_bin(Batch B) {
   SCENE_CTA(B, MAP_G);
-  SCENE_PARTICLES(p0) bin_one<D>(c, p0 + (int)threadIdx.x);
+  __shared__ int lb[MAXL + 1];
+  if (threadIdx.x == 0) {
+    int t = 0;
+    for (int q = 0; q < c.L; ++q) {
+      lb[q] = t;
+      t += c.ctr[CTR_LEVEL + q];
+    }
+    lb[c.L] = t;
+  }
+  __syncthreads();
+  SCENE_PARTICLES(p0) bin_one<D>(c, p0 + (int)threadIdx.x, lb);
 }
 
 // ---------------------------------------------------------------------------

@@ -817,11 +817,13 @@ constexpr bool staged_transfers() {
 template <int D>
 __global__ void k_gridop(Batch B) {
   SCENE_CTA(B, MAP_G);
-  const long long tot = total_elems(c, 0, c.L, D);
+  __shared__ BlockRanges br;
+  load_block_ranges(c, br);
+  const long long tot = total_elems_r(br, 0, c.L, D);
   SCENE_LOOP(e, tot) {
     int l, loc;
     long long blk;
-    decode_elem<D>(c, 0, c.L, e, l, blk, loc);
+    decode_elem_r<D>(c, br, 0, c.L, e, l, blk, loc);
     const LevelDev& V = c.lev[l];
     int I[D];
     elem_coords<D>(V, blk, loc, I);

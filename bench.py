@@ -426,7 +426,7 @@ def run_agimp(a):
         sim.set_tuning(ch, cps)
     elif not a.no_autotune:
         with torch.cuda.stream(stream):
-            sim.autotune(scene.dt, trials=3, stream=st)
+            sim.autotune(scene.dt, trials=10, stream=st)
     tuning = sim.tuning
     mlp = None
     if a.surrogate:
@@ -532,7 +532,7 @@ def run_batch(a):
         batch.set_tuning(ch, cps)
         tuning = batch.tuning
     else:
-        tuning = batch.autotune(dt, trials=3, stream=st) if not a.no_autotune else batch.tuning
+        tuning = batch.autotune(dt, trials=10, stream=st) if not a.no_autotune else batch.tuning
 
     def timed(step, clocks=None):
         import contextlib

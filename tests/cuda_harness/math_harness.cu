@@ -21,6 +21,33 @@ void h_svd(int dim, const float* A, float* U, float* S, float* V, int n) {
     else svd3(A + 9 * i, U + 9 * i, S + 3 * i, V + 9 * i);
   }
 }
+// the 2^dim corner elements of I0 on a level of nb blocks per axis, through
+// Corners and through elem_of / in_store one corner at a time
+void h_corners(int dim, int nb, const int* I0, int n, unsigned* idx, int* ok, long long* ref_idx, int* ref_ok) {
+  LevelDev V = {};
+  V.nb = nb;
+  for (int i = 0; i < n; ++i) {
+    const int* b = I0 + dim * i;
+    for (int a = 0; a < (1 << dim); ++a) {
+      int I[3];
+      for (int d = 0; d < dim; ++d) I[d] = b[d] + ((a >> (dim - 1 - d)) & 1);
+      const int o = (1 << dim) * i + a;
+      if (dim == 2) {
+        const Corners<2> K(V, b);
+        idx[o] = K.idx(a);
+        ok[o] = K.ok(a);
+        ref_ok[o] = in_store<2>(V, I);
+        ref_idx[o] = ref_ok[o] ? elem_of<2>(V, I) : -1;
+      } else {
+        const Corners<3> K(V, b);
+        idx[o] = K.idx(a);
+        ok[o] = K.ok(a);
+        ref_ok[o] = in_store<3>(V, I);
+        ref_idx[o] = ref_ok[o] ? elem_of<3>(V, I) : -1;
+      }
+    }
+  }
+}
 void h_axis_weights(float t, float r, float* W, float* G) { axis_weights(t, r, W, G); }
 void h_axis_weights_half(float t, float* W, float* G) { axis_weights_half(t, W, G); }
 // symmetric Kirchhoff stress expanded to full dim x dim matrices

@@ -162,3 +162,23 @@ def test_snow_skip_is_sound(h, dim):
     assert sel.sum() > 1000
     assert np.all(s[sel] >= lo - 1e-6) and np.all(s[sel] <= hi + 1e-6)
     assert np.all(np.linalg.det(F[sel]) > 0)
+
+
+@pytest.mark.parametrize("dim", [2, 3])
+def test_corner_elements_match_elem_of(h, dim):
+    """The per-axis corner indices of the binning's level search give the
+    same element (and the same in-store verdict) as elem_of / in_store for
+    every corner, block boundaries and the store's edges included."""
+    rng = np.random.default_rng(11)
+    nb = 19  # 64 cells per axis + 3 halo blocks
+    I0 = rng.integers(-7, 4 * nb - 1, (4000, dim)).astype(np.int32)
+    I0[:64] = np.array([[3, 3, 3][:dim]] * 64) + rng.integers(-1, 1, (64, dim))  # around a block corner
+    n, k = len(I0), 1 << dim
+    idx, ok = np.zeros(n * k, np.uint32), np.zeros(n * k, np.int32)
+    ref_idx, ref_ok = np.zeros(n * k, np.int64), np.zeros(n * k, np.int32)
+    h.h_corners(dim, nb, I0.ctypes.data_as(ctypes.c_void_p), n, idx.ctypes.data_as(ctypes.c_void_p),
+                ok.ctypes.data_as(ctypes.c_void_p), ref_idx.ctypes.data_as(ctypes.c_void_p),
+                ref_ok.ctypes.data_as(ctypes.c_void_p))
+    np.testing.assert_array_equal(ok, ref_ok)
+    assert ok.sum() > n * k // 2 and (ok == 0).sum() > 0
+    np.testing.assert_array_equal(idx[ok == 1].astype(np.int64), ref_idx[ok == 1])
