@@ -60,6 +60,12 @@ agimp_status batch_init(agimp_batch* b) {
     BCK(cudaEventCreateWithFlags(&b->ev_out, cudaEventDisableTiming));
     BCK(cudaEventCreateWithFlags(&b->ev_done, cudaEventDisableTiming));
     BCK(cudaEventCreateWithFlags(&b->ev_read, cudaEventDisableTiming));
+    BCK(cudaStreamCreateWithFlags(&b->gather, cudaStreamNonBlocking));
+    for (int k = 0; k < 2; ++k) {
+      BCK(cudaEventCreateWithFlags(&b->ev_xs[k], cudaEventDisableTiming));
+      BCK(cudaEventCreateWithFlags(&b->ev_hsrc[k], cudaEventDisableTiming));
+      BCK(cudaEventCreateWithFlags(&b->ev_gath[k], cudaEventDisableTiming));
+    }
   }
   return AGIMP_OK;
 }
@@ -130,9 +136,20 @@ void batch_free(agimp_batch* b) {
   if (b->ev_read) cudaEventDestroy(b->ev_read);
   if (b->xstage) cudaFree(b->xstage);
   if (b->dsrc) cudaFree(b->dsrc);
+  if (b->hsrc) cudaFreeHost(b->hsrc);
+  if (b->gather) cudaStreamDestroy(b->gather);
+  for (int k = 0; k < 2; ++k)
+    for (cudaEvent_t* e : {&b->ev_xs[k], &b->ev_hsrc[k], &b->ev_gath[k]}) {
+      if (*e) cudaEventDestroy(*e);
+      *e = nullptr;
+    }
   b->ev_done = b->ev_read = nullptr;
   b->xstage = nullptr;
   b->dsrc = nullptr;
+  b->hsrc = nullptr;
+  b->gather = nullptr;
+  b->xstage_floats = 0;
+  b->xs_busy[0] = b->xs_busy[1] = b->hsrc_busy[0] = b->hsrc_busy[1] = false;
   b->dctx[0] = b->dctx[1] = nullptr;
   b->dofs = nullptr;
   b->internal = nullptr;
@@ -363,30 +380,53 @@ agimp_status batch_positions_async(agimp_batch* b, float* x, cudaStream_t use) {
     if (st != AGIMP_OK) return st;
   }
   const int n = (int)b->sims.size();
-  std::vector<GatherSrc> src(n);
   long long tot = 0;
+  for (agimp_sim* s : b->sims) tot += s->c.N;
+  if (!b->xstage) {
+    const long long per = std::max<long long>(tot * b->dim, 1);
+    BCK(cudaMalloc(&b->xstage, 2 * per * sizeof(float)));
+    BCK(cudaMalloc(&b->dsrc, 2 * sizeof(GatherSrc) * n));
+    BCK(cudaMallocHost(&b->hsrc, 2 * sizeof(GatherSrc) * n));
+    b->xstage_floats = per;
+  }
+  // Two slots.  The source table goes to the device from pinned memory (an
+  // upload from pageable memory would wait for the stream); the gather runs
+  // on the batch's gather stream behind the last substep and the slot's
+  // previous host copy, so it frees the scenes' state without waiting for
+  // the previous readback's copy; the host copy runs on the caller's stream.
+  const int slot = b->xs_next;
+  b->xs_next ^= 1;
+  GatherSrc* hs = (GatherSrc*)b->hsrc + (size_t)slot * n;
+  GatherSrc* ds = (GatherSrc*)b->dsrc + (size_t)slot * n;
+  float* xs = b->xstage + (size_t)slot * b->xstage_floats;
+  if (b->hsrc_busy[slot]) BCK(cudaEventSynchronize(b->ev_hsrc[slot]));  // its last upload has run
+  long long off = 0;
   for (int i = 0; i < n; ++i) {
     agimp_sim* s = b->sims[i];
-    src[i] = GatherSrc{s->buf[s->par].x, s->buf[s->par].id, (long long)s->c.N, tot};
-    tot += s->c.N;
+    hs[i] = GatherSrc{s->buf[s->par].x, s->buf[s->par].id, (long long)s->c.N, off};
+    off += s->c.N;
   }
-  if (!b->xstage) {
-    BCK(cudaMalloc(&b->xstage, std::max<long long>(tot * b->dim, 1) * sizeof(float)));
-    BCK(cudaMalloc(&b->dsrc, sizeof(GatherSrc) * n));
-  }
-  BCK(cudaStreamWaitEvent(use, b->ev_done, 0));  // the batch's last substep is written
-  if (b->read_pending) BCK(cudaStreamWaitEvent(use, b->ev_read, 0));  // the staging is free
-  BCK(cudaMemcpyAsync(b->dsrc, src.data(), sizeof(GatherSrc) * n, cudaMemcpyHostToDevice, use));
+  cudaStream_t gs = b->gather;
+  BCK(cudaStreamWaitEvent(gs, b->ev_done, 0));  // the batch's last substep is written
+  if (b->xs_busy[slot]) BCK(cudaStreamWaitEvent(gs, b->ev_xs[slot], 0));  // the slot's last copy is done
+  BCK(cudaMemcpyAsync(ds, hs, sizeof(GatherSrc) * n, cudaMemcpyHostToDevice, gs));
+  BCK(cudaEventRecord(b->ev_hsrc[slot], gs));
+  b->hsrc_busy[slot] = true;
   const int G = b->nct[MAP_G];
   if (b->dim == 2)
-    k_gather_x<2><<<G, 256, 0, use>>>(b->dofs + MAP_G * (n + 1), n, (const GatherSrc*)b->dsrc, b->xstage);
+    k_gather_x<2><<<G, 256, 0, gs>>>(b->dofs + MAP_G * (n + 1), n, ds, xs);
   else
-    k_gather_x<3><<<G, 256, 0, use>>>(b->dofs + MAP_G * (n + 1), n, (const GatherSrc*)b->dsrc, b->xstage);
+    k_gather_x<3><<<G, 256, 0, gs>>>(b->dofs + MAP_G * (n + 1), n, ds, xs);
   BCK(cudaGetLastError());
-  BCK(cudaMemcpyAsync(x, b->xstage, tot * b->dim * sizeof(float), cudaMemcpyDeviceToHost, use));
-  BCK(cudaEventRecord(b->ev_read, use));
+  // the scenes' state has been read: the substep that overwrites it may run
+  BCK(cudaEventRecord(b->ev_read, gs));
   b->read_pending = true;
   b->read_step = b->steps;
+  BCK(cudaEventRecord(b->ev_gath[slot], gs));
+  BCK(cudaStreamWaitEvent(use, b->ev_gath[slot], 0));
+  BCK(cudaMemcpyAsync(x, xs, tot * b->dim * sizeof(float), cudaMemcpyDeviceToHost, use));
+  BCK(cudaEventRecord(b->ev_xs[slot], use));
+  b->xs_busy[slot] = true;
   return AGIMP_OK;
 }
 

@@ -411,7 +411,10 @@ agimp_status agimp_create(const agimp_params* p, int32_t device, agimp_sim** out
       cudaEventCreateWithFlags(&s->ev_read[0], cudaEventDisableTiming) != cudaSuccess ||
       cudaEventCreateWithFlags(&s->ev_read[1], cudaEventDisableTiming) != cudaSuccess ||
       cudaEventCreateWithFlags(&s->ev_stage[0], cudaEventDisableTiming) != cudaSuccess ||
-      cudaEventCreateWithFlags(&s->ev_stage[1], cudaEventDisableTiming) != cudaSuccess) {
+      cudaEventCreateWithFlags(&s->ev_stage[1], cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&s->ev_gath[0], cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&s->ev_gath[1], cudaEventDisableTiming) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&s->gather, cudaStreamNonBlocking) != cudaSuccess) {
     agimp_destroy(s);
     return AGIMP_CUDA_ERROR;
   }
@@ -446,8 +449,10 @@ agimp_status agimp_destroy(agimp_sim* s) {
   for (void* p : s->allocs) cudaFree(p);
   if (s->rimg) cudaFree(s->rimg);
   if (s->astage) cudaFree(s->astage);
-  for (cudaEvent_t e : {s->ev_state, s->ev_read[0], s->ev_read[1], s->ev_stage[0], s->ev_stage[1]})
+  for (cudaEvent_t e : {s->ev_state, s->ev_read[0], s->ev_read[1], s->ev_stage[0], s->ev_stage[1], s->ev_gath[0],
+                        s->ev_gath[1]})
     if (e) cudaEventDestroy(e);
+  if (s->gather) cudaStreamDestroy(s->gather);
   if (s->rwin) cudaFree(s->rwin);
   if (s->rkey) cudaFree(s->rkey);
   if (s->rdir) cudaFree(s->rdir);
@@ -529,6 +534,7 @@ agimp_status agimp_set_particles(agimp_sim* s, const float* x, const float* v, c
   if (m && (r = upload_soa(s, m, P.m, 1, memory, su.use))) return r;
   if (Jp && (r = upload_soa(s, Jp, P.Jp, 1, memory, su.use))) return r;
   if (g && (r = copy_i32(s, g, P.g, 1, memory, su.use))) return r;
+  if (s->async_used) CK(cudaEventRecord(s->ev_state, su.use));  // later asynchronous readbacks follow the upload
   if (memory == AGIMP_MEM_HOST) CK(cudaStreamSynchronize(su.use));  // host buffers may be reused on return
   return AGIMP_OK;
 }
@@ -595,16 +601,20 @@ agimp_status agimp_get_particles_async(agimp_sim* s, float* x, float* v, float* 
     s->async_used = true;
     CK(cudaEventRecord(s->ev_state, su.use));
   }
-  CK(cudaStreamWaitEvent(su.use, s->ev_state, 0));  // the state is written
   // Two staging slots: the fields are first gathered into caller order in
-  // this call's slot (a short kernel), which frees the particle state for the
-  // substep that overwrites it; the host copies out of the slot then overlap
-  // the following substeps.  A slot is reused two calls later, after its
-  // copies.
+  // this call's slot (a short kernel on the gather stream, behind the state
+  // and the slot's previous host copy), which frees the particle state for
+  // the substep that overwrites it; the host copies out of the slot run on
+  // the caller's stream and overlap the following substeps.  A slot is
+  // reused two calls later, after its copies.
+  cudaStream_t gs = s->gather;
+  CK(cudaStreamWaitEvent(gs, s->ev_state, 0));  // the state is written
   const int slot = s->stage_next;
   s->stage_next ^= 1;
-  if (s->stage_busy[slot]) CK(cudaStreamWaitEvent(su.use, s->ev_stage[slot], 0));
-  const size_t need = (size_t)N * (2 * D + 2 * D * D + 4) + 16;
+  if (s->stage_busy[slot]) CK(cudaStreamWaitEvent(gs, s->ev_stage[slot], 0));
+  const int comps = (x ? D : 0) + (v ? D : 0) + (F ? D * D : 0) + (C ? D * D : 0) + (m ? 1 : 0) + (Jp ? 1 : 0) +
+                    (g ? 1 : 0) + (fl ? 1 : 0);
+  const size_t need = (size_t)N * comps + 16;
   if (need > s->astage_floats) {
     CK(cudaDeviceSynchronize());  // both slots idle before they move
     if (s->astage) cudaFree(s->astage);
@@ -624,14 +634,14 @@ agimp_status agimp_get_particles_async(agimp_sim* s, float* x, float* v, float* 
   float* st = st0;
   auto field = [&](const float* src, float* dst, int comps) -> cudaError_t {
     if (!dst || !N) return cudaSuccess;
-    k_soa_to_aos<<<gs_blocks(N * comps), 256, 0, su.use>>>(src, P.id, st, N, comps);
+    k_soa_to_aos<<<gs_blocks(N * comps), 256, 0, gs>>>(src, P.id, st, N, comps);
     copies[ncopy++] = {dst, st, N * comps * sizeof(float)};
     st += N * comps;
     return cudaGetLastError();
   };
   auto ifield = [&](const int32_t* src, int32_t* dst) -> cudaError_t {
     if (!dst || !N) return cudaSuccess;
-    k_i32_out<<<gs_blocks(N), 256, 0, su.use>>>(src, P.id, (int32_t*)st, N);
+    k_i32_out<<<gs_blocks(N), 256, 0, gs>>>(src, P.id, (int32_t*)st, N);
     copies[ncopy++] = {dst, st, N * sizeof(int32_t)};
     st += N;
     return cudaGetLastError();
@@ -645,9 +655,11 @@ agimp_status agimp_get_particles_async(agimp_sim* s, float* x, float* v, float* 
   CK(ifield(P.g, g));
   CK(ifield(P.fl, fl));
   // the state has been read: a substep may overwrite it from here on
-  CK(cudaEventRecord(s->ev_read[k], su.use));
+  CK(cudaEventRecord(s->ev_read[k], gs));
   s->read_pending[k] = true;
   s->last_read = k;
+  CK(cudaEventRecord(s->ev_gath[slot], gs));
+  CK(cudaStreamWaitEvent(su.use, s->ev_gath[slot], 0));
   for (int i = 0; i < ncopy; ++i)
     CK(cudaMemcpyAsync(copies[i].dst, copies[i].src, copies[i].bytes, cudaMemcpyDeviceToHost, su.use));
   CK(cudaEventRecord(s->ev_stage[slot], su.use));
@@ -730,6 +742,7 @@ agimp_status agimp_refine_levels(agimp_sim* s, int32_t band, void* stream) {
   wait_readback(s, s->par, su.use);  // g_p of the state being read is rewritten
   launch_refine(cur(s), band, su.use);
   CK(cudaGetLastError());
+  if (s->async_used) CK(cudaEventRecord(s->ev_state, su.use));  // later asynchronous readbacks follow it
   return AGIMP_OK;
 }
 

@@ -37,6 +37,11 @@ struct agimp_sim {
   int stage_next = 0;           // slot of the next asynchronous readback
   bool stage_busy[2] = {false, false};
   cudaEvent_t ev_stage[2] = {nullptr, nullptr};  // the host copy out of slot k has been issued up to here
+  // the gathers of asynchronous readbacks run on their own stream, so a
+  // gather (and with it the release of the state) waits only for the state
+  // and for its slot's previous host copy, not for the last readback's copy
+  cudaStream_t gather = nullptr;
+  cudaEvent_t ev_gath[2] = {nullptr, nullptr};  // slot k's gather is done
   float* rimg = nullptr;        // headless drawing: image scratch for host outputs
   size_t rimg_floats = 0;
   int* rwin = nullptr;          // headless drawing: particle covering each pixel
@@ -86,8 +91,19 @@ struct agimp_batch {
   cudaEvent_t ev_done = nullptr, ev_read = nullptr;
   bool read_pending = false;
   long long read_step = 0;
+  // two slots: gathered positions (xstage, tot*dim floats each), the
+  // per-scene gather sources in pinned host memory (hsrc) and on the device
+  // (dsrc); the gathers run on their own stream (see agimp_sim::gather)
   float* xstage = nullptr;
-  void* dsrc = nullptr;  // per-scene sources of the gather
+  void* dsrc = nullptr;
+  void* hsrc = nullptr;
+  long long xstage_floats = 0;
+  int xs_next = 0;
+  bool xs_busy[2] = {false, false}, hsrc_busy[2] = {false, false};
+  cudaEvent_t ev_xs[2] = {nullptr, nullptr};    // slot k's host copy is done
+  cudaEvent_t ev_hsrc[2] = {nullptr, nullptr};  // slot k's source table is on the device
+  cudaEvent_t ev_gath[2] = {nullptr, nullptr};  // slot k's gather is done
+  cudaStream_t gather = nullptr;
   // surrogate return map shared by the scenes of a batch of several
   // (agimp_batch_set_surrogate): one set of slot buffers over all scenes'
   // particles and one slot counter, so one MLP launch serves the batch

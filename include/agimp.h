@@ -137,12 +137,14 @@ agimp_status agimp_get_bins(agimp_sim* s, uint64_t* keys, int32_t memory, void* 
  * once; the outputs hold the state once `stream` has run the enqueued work
  * (synchronize it or wait on an event recorded after the call).  No counterpart
  * in the reference (Taichi's to_numpy blocks).  The copy waits for the
- * substeps already issued, and later substeps, uploads or refinements that
+ * substeps, uploads and refinements already issued, and later ones that
  * would overwrite the state being copied wait for the fields to be gathered
- * into a staging slot (a short kernel), whatever streams they use: the state
- * of substep k can be read while substep k+1 runs, and its host copy can
- * overlap substeps k+1 and k+2.  Allocates its staging (two slots of
- * N x (2 dim + 2 dim^2 + 4) floats) on first use. */
+ * into a staging slot (a short kernel on the library's own stream, behind the
+ * state and the slot's previous host copy only), whatever streams they use:
+ * the state of substep k can be read while substep k+1 runs, and its host
+ * copy can overlap substeps k+1 and k+2.  Allocates its staging (two slots of
+ * N x the requested components floats) on first use, and again when a call
+ * requests more fields. */
 agimp_status agimp_get_particles_async(agimp_sim* s, float* x, float* v, float* F, float* C, float* m, int32_t* g,
                                        int32_t* fl, float* Jp, void* stream);
 
