@@ -36,6 +36,7 @@ EXPORTS = (
     "agimp_batch_kernels_per_substep", "agimp_batch_profile_substep", "agimp_batch_set_surrogate",
     "agimp_batch_surrogate_stats",
     "agimp_render_mask", "agimp_render_particles", "agimp_get_particles_async", "agimp_batch_positions_async",
+    "agimp_batch_set_particles",
     "agimp_get_level_map", "agimp_lattice_count", "agimp_lattice_fill", "agimp_random_fill",
     "agimp_set_level_map_rule", "agimp_set_coarse_level_map", "agimp_render_scene3d", "agimp_cell_lines",
 )
@@ -171,6 +172,7 @@ def load(path: str | None = None):
     L.agimp_batch_profile_substep.argtypes = [vp, ctypes.c_float, fp, ctypes.c_int32, vp]
     L.agimp_get_particles_async.argtypes = [vp, vp, vp, vp, vp, vp, vp, vp, vp, vp]
     L.agimp_batch_positions_async.argtypes = [vp, vp, vp]
+    L.agimp_batch_set_particles.argtypes = [vp, vp, vp, vp, vp, vp, vp, vp, ctypes.c_int32, vp]
     L.agimp_render_mask.argtypes = [vp, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, vp, ctypes.c_int32, vp]
     L.agimp_render_particles.argtypes = [vp, ctypes.c_int32, ctypes.c_float, vp, ctypes.c_int32, vp, ctypes.c_int32, vp]
     L.agimp_get_level_map.argtypes = [vp, vp, ip, ctypes.c_int32, vp]

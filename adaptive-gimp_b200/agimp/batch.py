@@ -94,6 +94,32 @@ class SceneBatch:
             torch.cuda.synchronize()
         return out
 
+    def set_particles(self, x=None, v=None, F=None, C=None, m=None, g=None, Jp=None):
+        """Upload every scene's particles in one call: each array holds all
+        scenes' particles concatenated in batch order (as positions() returns
+        them), host arrays (pinned for the fastest copy) or CUDA tensors."""
+        import numpy as np
+        vals = [x, v, F, C, m, g, Jp]
+        dtypes = [np.float32] * 5 + [np.int32, np.float32]
+        try:
+            import torch
+            is_t = [isinstance(a, torch.Tensor) for a in vals if a is not None]
+        except ImportError:
+            is_t = []
+        if is_t and all(is_t):
+            args = [ctypes.c_void_p(a.contiguous().data_ptr()) if a is not None else None for a in vals]
+            mem, st = _capi.AGIMP_MEM_DEVICE, _torch_stream()
+        else:
+            arrs = [np.ascontiguousarray(a, dt) if a is not None else None for a, dt in zip(vals, dtypes)]
+            n = self.n_particles
+            for a in arrs:
+                if a is not None and a.shape[0] != n:
+                    raise ValueError("batch arrays hold all %d particles of the batch, got %d" % (n, a.shape[0]))
+            args = [ctypes.c_void_p(a.ctypes.data) if a is not None else None for a in arrs]
+            mem, st = _capi.AGIMP_MEM_HOST, None
+        # argument order of the C entry point: x, v, F, C, m, g, Jp
+        _capi.check(self._L.agimp_batch_set_particles(self._h, *args, mem, st), self._h, "batch upload", batch=True)
+
     def kernels_per_substep(self):
         return int(self._L.agimp_batch_kernels_per_substep(self._h))
 

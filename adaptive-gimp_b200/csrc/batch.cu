@@ -137,6 +137,12 @@ void batch_free(agimp_batch* b) {
   if (b->xstage) cudaFree(b->xstage);
   if (b->dsrc) cudaFree(b->dsrc);
   if (b->hsrc) cudaFreeHost(b->hsrc);
+  if (b->ustage) cudaFree(b->ustage);
+  if (b->utab) cudaFree(b->utab);
+  if (b->utab_h) cudaFreeHost(b->utab_h);
+  b->ustage = nullptr;
+  b->utab = b->utab_h = nullptr;
+  b->ustage_floats = 0;
   if (b->gather) cudaStreamDestroy(b->gather);
   for (int k = 0; k < 2; ++k)
     for (cudaEvent_t* e : {&b->ev_xs[k], &b->ev_hsrc[k], &b->ev_gath[k]}) {
@@ -335,7 +341,11 @@ agimp_status batch_step(agimp_batch* b, float dt, int n, cudaStream_t use, cudaE
   // state-ready marks for asynchronous readbacks (a batch of one always
   // records it; larger batches only for scenes that read asynchronously)
   for (agimp_sim* s : b->sims)
-    if ((b->single || s->async_used) && n > 0) BCK(cudaEventRecord(s->ev_state, use));
+    if (n > 0) {
+      const bool mark = b->single || s->async_used;
+      if (mark) BCK(cudaEventRecord(s->ev_state, use));
+      s->state_marked = mark;
+    }
   if (b->ev_done && n > 0) BCK(cudaEventRecord(b->ev_done, use));
   return AGIMP_OK;
 }
@@ -427,6 +437,106 @@ agimp_status batch_positions_async(agimp_batch* b, float* x, cudaStream_t use) {
   BCK(cudaMemcpyAsync(x, xs, tot * b->dim * sizeof(float), cudaMemcpyDeviceToHost, use));
   BCK(cudaEventRecord(b->ev_xs[slot], use));
   b->xs_busy[slot] = true;
+  return AGIMP_OK;
+}
+
+namespace {
+struct ScatterDst {
+  void* dst;           // the scene's field: comps x N, slot-major per component
+  const int32_t* id;   // storage slot -> caller index
+  long long N, off;    // particles; first index in the concatenated arrays
+};
+
+// every scene's field from the concatenated caller arrays (particle-major,
+// comps values each, scenes in batch order) into its storage
+template <typename T>
+__global__ void k_scatter_in(const int* ofs, int n, const ScatterDst* tab, const T* src, int comps) {
+  const int cta = (int)blockIdx.x;
+  int lo = 0, hi = n - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (ofs[mid] <= cta)
+      lo = mid;
+    else
+      hi = mid - 1;
+  }
+  const ScatterDst t = tab[lo];
+  T* dst = (T*)t.dst;
+  const int bid = cta - ofs[lo], nblk = ofs[lo + 1] - ofs[lo];
+  for (long long s = bid * (long long)blockDim.x + threadIdx.x; s < t.N; s += (long long)nblk * blockDim.x) {
+    const long long o = (t.off + t.id[s]) * comps;
+    for (int c = 0; c < comps; ++c) dst[c * t.N + s] = src[o + c];
+  }
+}
+}  // namespace
+
+agimp_status batch_set_particles(agimp_batch* b, const float* x, const float* v, const float* F, const float* C,
+                                 const float* m, const int32_t* g, const float* Jp, int memory, cudaStream_t use) {
+  BCK(cudaSetDevice(b->device));
+  if (b->single || (memory != AGIMP_MEM_DEVICE && memory != AGIMP_MEM_HOST)) {
+    b->err = "batch upload: a batch of several scenes and a memory kind are required";
+    return AGIMP_INVALID_ARG;
+  }
+  if (!b->maps_valid) {
+    const agimp_status st = build_maps(b, use);
+    if (st != AGIMP_OK) return st;
+  }
+  const int n = (int)b->sims.size(), D = b->dim;
+  long long tot = 0;
+  for (agimp_sim* s : b->sims) tot += s->c.N;
+  // the state being overwritten may still be read by asynchronous readbacks
+  for (agimp_sim* s : b->sims) {
+    wait_readback(s, s->par, use);
+    s->bins_valid = false;
+  }
+  if (b->read_pending) BCK(cudaStreamWaitEvent(use, b->ev_read, 0));
+  const void* fields[7] = {x, v, F, C, m, Jp, g};
+  const int comps[7] = {D, D, D * D, D * D, 1, 1, 1};
+  const size_t need = (size_t)std::max<long long>(tot, 1) * D * D;
+  if (memory == AGIMP_MEM_HOST && need > b->ustage_floats) {
+    if (b->ustage) BCK(cudaFree(b->ustage));
+    b->ustage = nullptr;
+    b->ustage_floats = 0;
+    BCK(cudaMalloc(&b->ustage, need * sizeof(float)));
+    b->ustage_floats = need;
+  }
+  if (!b->utab) {
+    BCK(cudaMalloc(&b->utab, 7 * sizeof(ScatterDst) * n));
+    BCK(cudaMallocHost(&b->utab_h, 7 * sizeof(ScatterDst) * n));
+  }
+  ScatterDst* th = (ScatterDst*)b->utab_h;
+  long long off = 0;
+  for (int i = 0; i < n; ++i) {
+    agimp_sim* s = b->sims[i];
+    const Particles& P = s->buf[s->par];
+    void* dst[7] = {P.x, P.v, P.F, P.C, P.m, P.Jp, P.g};
+    for (int f = 0; f < 7; ++f) th[f * n + i] = ScatterDst{dst[f], P.id, (long long)s->c.N, off};
+    off += s->c.N;
+  }
+  BCK(cudaMemcpyAsync(b->utab, th, 7 * sizeof(ScatterDst) * n, cudaMemcpyHostToDevice, use));
+  const int G = b->nct[MAP_G];
+  for (int f = 0; f < 7; ++f) {
+    if (!fields[f] || tot == 0) continue;
+    const void* src = fields[f];
+    if (memory == AGIMP_MEM_HOST) {
+      // one field at a time through the staging buffer (stream order keeps
+      // the next field's copy behind this field's scatter)
+      BCK(cudaMemcpyAsync(b->ustage, src, tot * comps[f] * sizeof(float), cudaMemcpyHostToDevice, use));
+      src = b->ustage;
+    }
+    const ScatterDst* td = (const ScatterDst*)b->utab + (size_t)f * n;
+    if (f == 6)
+      k_scatter_in<int32_t><<<G, 256, 0, use>>>(b->dofs + MAP_G * (n + 1), n, td, (const int32_t*)src, 1);
+    else
+      k_scatter_in<float><<<G, 256, 0, use>>>(b->dofs + MAP_G * (n + 1), n, td, (const float*)src, comps[f]);
+    BCK(cudaGetLastError());
+  }
+  for (agimp_sim* s : b->sims) {
+    BCK(cudaEventRecord(s->ev_state, use));  // later asynchronous readbacks follow the upload
+    s->state_marked = true;
+  }
+  // the pinned table (and host arrays) may be reused on return
+  BCK(cudaStreamSynchronize(use));
   return AGIMP_OK;
 }
 
@@ -536,6 +646,8 @@ agimp_status batch_autotune(agimp_batch* b, float dt, int trials, agimp_tuning* 
       });
       cudaMemcpyAsync(s->c.ctr + CTR_ERR, &v.err, 4, cudaMemcpyHostToDevice, use);
       cudaMemcpyAsync(s->c.ctr + CTR_REC, &v.rec, 4, cudaMemcpyHostToDevice, use);
+      cudaEventRecord(s->ev_state, use);  // the restored state is the last write
+      s->state_marked = true;
     }
     return cudaStreamSynchronize(use);
   };

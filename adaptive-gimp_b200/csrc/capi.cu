@@ -534,7 +534,8 @@ agimp_status agimp_set_particles(agimp_sim* s, const float* x, const float* v, c
   if (m && (r = upload_soa(s, m, P.m, 1, memory, su.use))) return r;
   if (Jp && (r = upload_soa(s, Jp, P.Jp, 1, memory, su.use))) return r;
   if (g && (r = copy_i32(s, g, P.g, 1, memory, su.use))) return r;
-  if (s->async_used) CK(cudaEventRecord(s->ev_state, su.use));  // later asynchronous readbacks follow the upload
+  CK(cudaEventRecord(s->ev_state, su.use));  // later asynchronous readbacks follow the upload
+  s->state_marked = true;
   if (memory == AGIMP_MEM_HOST) CK(cudaStreamSynchronize(su.use));  // host buffers may be reused on return
   return AGIMP_OK;
 }
@@ -596,10 +597,12 @@ agimp_status agimp_get_particles_async(agimp_sim* s, float* x, float* v, float* 
   const int k = s->par;
   const Particles& P = s->buf[k];
   if (!s->async_used) {
-    // from now on every substep marks when the state is ready; the substeps
-    // issued so far were ordered before this call on the library's streams
+    // from now on every substep marks when the state is ready; if nothing
+    // marked the last write yet (a scene stepped only in a batch of several),
+    // the work issued so far on the caller's stream is the state
     s->async_used = true;
-    CK(cudaEventRecord(s->ev_state, su.use));
+    if (!s->state_marked) CK(cudaEventRecord(s->ev_state, su.use));
+    s->state_marked = true;
   }
   // Two staging slots: the fields are first gathered into caller order in
   // this call's slot (a short kernel on the gather stream, behind the state
@@ -742,7 +745,8 @@ agimp_status agimp_refine_levels(agimp_sim* s, int32_t band, void* stream) {
   wait_readback(s, s->par, su.use);  // g_p of the state being read is rewritten
   launch_refine(cur(s), band, su.use);
   CK(cudaGetLastError());
-  if (s->async_used) CK(cudaEventRecord(s->ev_state, su.use));  // later asynchronous readbacks follow it
+  CK(cudaEventRecord(s->ev_state, su.use));  // later asynchronous readbacks follow it
+  s->state_marked = true;
   return AGIMP_OK;
 }
 
@@ -1075,6 +1079,13 @@ agimp_status agimp_batch_positions_async(agimp_batch* b, float* x, void* stream)
   if (!b) return AGIMP_INVALID_ARG;
   BatchStream bs(b, stream);
   return batch_positions_async(b, x, bs.use);
+}
+
+agimp_status agimp_batch_set_particles(agimp_batch* b, const float* x, const float* v, const float* F, const float* C,
+                                       const float* m, const int32_t* g, const float* Jp, int32_t memory, void* stream) {
+  if (!b) return AGIMP_INVALID_ARG;
+  BatchStream bs(b, stream);
+  return batch_set_particles(b, x, v, F, C, m, g, Jp, memory, bs.use);
 }
 
 agimp_status agimp_batch_set_surrogate(agimp_batch* b, const agimp_mlp* m, const float* xmax, float tol) {

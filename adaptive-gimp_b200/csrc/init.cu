@@ -465,7 +465,9 @@ agimp_status agimp_lattice_fill(agimp_sim* s, int32_t per_axis, int32_t jitter, 
     else
       k_lattice_fill<3><<<grid_for(ntiles, 1), TILE, 0, use>>>(A, ntiles, offs, P, s->c.N);
     e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaEventRecord(s->ev_state, use);  // later asynchronous readbacks follow the fill
     if (e == cudaSuccess) e = cudaStreamSynchronize(use);  // before the scratch is freed
+    s->state_marked = true;
   }
   if (counts) cudaFree(counts);
   if (offs) cudaFree(offs);
@@ -529,6 +531,8 @@ agimp_status agimp_random_fill(agimp_sim* s, uint64_t seed, const agimp_random_b
       k_random_fill<3><<<grid_for(s->c.N, 256), 256, 0, use>>>(A, P, s->c.N);
   }
   cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaEventRecord(s->ev_state, use);  // later asynchronous readbacks follow the fill
+  s->state_marked = true;
   if (e == cudaSuccess && !stream) e = cudaStreamSynchronize(use);
   if (e != cudaSuccess) {
     s->err = std::string("random fill: ") + cudaGetErrorString(e);

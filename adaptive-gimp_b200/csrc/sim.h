@@ -28,6 +28,7 @@ struct agimp_sim {
   // asynchronous readback: the state is ready after ev_state; a copy of
   // buffer k is in flight until ev_read[k]
   bool async_used = false;
+  bool state_marked = false;  // ev_state was recorded after the last write of the state
   cudaEvent_t ev_state = nullptr;
   cudaEvent_t ev_read[2] = {nullptr, nullptr};
   bool read_pending[2] = {false, false};
@@ -104,6 +105,12 @@ struct agimp_batch {
   cudaEvent_t ev_hsrc[2] = {nullptr, nullptr};  // slot k's source table is on the device
   cudaEvent_t ev_gath[2] = {nullptr, nullptr};  // slot k's gather is done
   cudaStream_t gather = nullptr;
+  // batch upload (agimp_batch_set_particles): one field of all scenes in the
+  // staging at a time, the per-scene destinations of all fields in utab
+  float* ustage = nullptr;
+  size_t ustage_floats = 0;
+  void* utab = nullptr;
+  void* utab_h = nullptr;
   // surrogate return map shared by the scenes of a batch of several
   // (agimp_batch_set_surrogate): one set of slot buffers over all scenes'
   // particles and one slot counter, so one MLP launch serves the batch
@@ -131,6 +138,8 @@ void batch_drop_graphs(agimp_batch* b);
 agimp_status batch_step(agimp_batch* b, float dt, int n, cudaStream_t use, cudaEvent_t* ev);
 int batch_kernels(agimp_batch* b);
 agimp_status batch_positions_async(agimp_batch* b, float* x, cudaStream_t use);
+agimp_status batch_set_particles(agimp_batch* b, const float* x, const float* v, const float* F, const float* C,
+                                 const float* m, const int32_t* g, const float* Jp, int memory, cudaStream_t use);
 // make `use` wait for asynchronous readbacks of the buffer the next work writes
 void wait_readback(agimp_sim* s, int buf, cudaStream_t use);
 agimp_status batch_autotune(agimp_batch* b, float dt, int trials, agimp_tuning* best, cudaStream_t use);

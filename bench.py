@@ -762,29 +762,30 @@ def e2e_median(run):
 
 
 def e2e_batch(a, sc, local, tuning=None):
-    """Same metric through the public API with host buffers: every scene is
-    uploaded from pinned host memory, then per substep the batch steps and all
-    scenes' positions are read back into pinned host memory."""
+    """Same metric through the public API with host buffers: all scenes are
+    uploaded from pinned host memory in one batch upload, then per substep the
+    batch steps and all scenes' positions are read back into pinned host
+    memory."""
     import numpy as np
     import torch
 
     from agimp.batch import SceneBatch
     sims = [s.build(device=local) for s in sc]
     batch = SceneBatch(sims)
-    hosts = []
-    for s in sc:
-        n, d = s.n, s.dim
-        h = {k: torch.empty(shape, dtype=torch.float32, pin_memory=True).numpy()
-             for k, shape in (("x", (n, d)), ("v", (n, d)), ("F", (n, d, d)), ("C", (n, d, d)), ("m", (n,)))}
-        h["g"] = torch.empty((n,), dtype=torch.int32, pin_memory=True).numpy()
-        h["x"][:] = s.x
-        h["v"][:] = s.v
-        h["F"][:] = np.eye(d, dtype=np.float32)
-        h["C"][:] = 0
-        h["m"][:] = s.m
-        h["g"][:] = s.g
-        hosts.append(h)
+    # every scene's initial state concatenated in batch order, in pinned host
+    # memory: one upload call for the batch (agimp_batch_set_particles)
     n_tot = sum(s.n for s in sc)
+    d = sc[0].dim
+    h = {k: torch.empty(shape, dtype=torch.float32, pin_memory=True).numpy()
+         for k, shape in (("x", (n_tot, d)), ("v", (n_tot, d)), ("F", (n_tot, d, d)), ("C", (n_tot, d, d)),
+                          ("m", (n_tot,)))}
+    h["g"] = torch.empty((n_tot,), dtype=torch.int32, pin_memory=True).numpy()
+    h["x"][:] = np.concatenate([s.x for s in sc])
+    h["v"][:] = np.concatenate([s.v for s in sc])
+    h["F"][:] = np.eye(d, dtype=np.float32)
+    h["C"][:] = 0
+    h["m"][:] = np.concatenate([s.m for s in sc])
+    h["g"][:] = np.concatenate([s.g for s in sc])
     if tuning:
         batch.set_tuning(tuning["chunk"], tuning["ctas_per_sm"])
     import ctypes
@@ -795,8 +796,7 @@ def e2e_batch(a, sc, local, tuning=None):
     steps = max(a.steps, E2E_MIN_STEPS)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    for sim, h in zip(sims, hosts):
-        sim.set_particles(x=h["x"], v=h["v"], F=h["F"], C=h["C"], m=h["m"], g=h["g"])
+    batch.set_particles(x=h["x"], v=h["v"], F=h["F"], C=h["C"], m=h["m"], g=h["g"])
     for i in range(steps):
         batch.substep(sc[0].dt, stream=sm)
         # every scene's x_p in one gathered copy on a copy stream, overlapping

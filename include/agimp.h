@@ -369,11 +369,22 @@ int32_t agimp_batch_kernels_per_substep(const agimp_batch* b);
 /* Positions of all scenes in one copy: x [sum of N][dim] in HOST memory
  * (pinned, for overlap), scene after scene in batch order, each scene in its
  * caller's particle order.  Asynchronous like agimp_get_particles_async: the
- * copy waits for the batch's substeps already issued, and the batch's second
- * substep after it waits for the copy, so a copy overlaps the next substep.
- * (Orders only against the batch's own steps.)  Allocates its staging on first
- * use. */
+ * gather into a staging slot waits for the batch's substeps already issued,
+ * and the substep that overwrites that state waits for the gather (a short
+ * kernel on the batch's own stream), so the host copy overlaps the next
+ * substeps.  (Orders only against the batch's own steps and uploads.)
+ * Allocates its staging (two slots) on first use. */
 agimp_status agimp_batch_positions_async(agimp_batch* b, float* x, void* stream);
+/* Upload of every scene's particles in one call (a batch of several): the
+ * arrays hold all scenes' particles concatenated in batch order, each scene
+ * in its caller's particle order, shaped as agimp_set_particles takes them
+ * (x, v [sum of N][dim], F, C [sum of N][dim][dim], m, g, Jp [sum of N]); NULL
+ * fields are skipped.  One copy and one scatter kernel per field for all
+ * scenes; waits for asynchronous readbacks of the state it overwrites and
+ * returns after the upload.  No counterpart in the reference. */
+agimp_status agimp_batch_set_particles(agimp_batch* b, const float* x, const float* v, const float* F, const float* C,
+                                       const float* m, const int32_t* g, const float* Jp, int32_t memory,
+                                       void* stream);
 /* As agimp_profile_substep, for one substep of the whole batch. */
 agimp_status agimp_batch_profile_substep(agimp_batch* b, float dt, float* ms, int32_t n, void* stream);
 /* No counterpart in the reference (which has no plasticity): the surrogate

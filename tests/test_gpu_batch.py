@@ -261,3 +261,98 @@ def test_batch_positions_readback():
     rbatch.close()
     for s in sims + ref:
         s.close()
+
+
+def test_async_readbacks_follow_uploads_and_refinements():
+    """Asynchronous readbacks run their gathers on the library's own stream:
+    an upload or a refinement issued between two readbacks (on any stream)
+    is seen by the second readback and not by the first."""
+    import ctypes
+
+    import torch
+
+    from agimp import scenes
+    sc = scenes.make_config(3, scale=0.3)
+    sim = sc.build()
+    s1, s2 = torch.cuda.Stream(), torch.cuda.Stream()
+    p1, p2 = ctypes.c_void_p(s1.cuda_stream), ctypes.c_void_p(s2.cuda_stream)
+    n = sc.n
+    sim.refine_levels(sc.refine_band, stream=p1)
+    sim.substep(sc.dt, stream=p1)
+    before = [torch.empty((n, 3), dtype=torch.float32, pin_memory=True).numpy() for _ in range(2)]
+    after = [torch.empty((n, 3), dtype=torch.float32, pin_memory=True).numpy() for _ in range(2)]
+    g_before = torch.empty((n,), dtype=torch.int32, pin_memory=True).numpy()
+    g_after = torch.empty((n,), dtype=torch.int32, pin_memory=True).numpy()
+    sim.x_p.to_numpy(out=before[0], blocking=False, stream=p2)
+    sim.g_p.to_numpy(out=g_before, blocking=False, stream=p2)
+    x_new = (sim.x_p.to_numpy() * np.float32(0.5) + np.float32(0.25)).astype(np.float32)
+    sim.x_p.from_numpy(x_new)  # upload on the library's stream
+    sim.x_p.to_numpy(out=after[0], blocking=False, stream=p2)
+    sim.refine_levels(2, stream=p1)  # another band: other prescribed levels
+    sim.g_p.to_numpy(out=g_after, blocking=False, stream=p2)
+    s1.synchronize()
+    s2.synchronize()
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(after[0], x_new)
+    assert not np.array_equal(before[0], x_new)
+    ref = sc.build()
+    ref.x_p.from_numpy(x_new)
+    ref.refine_levels(2)
+    np.testing.assert_array_equal(g_after, ref.g_p.to_numpy())
+    assert not np.array_equal(g_before, g_after)
+    ref.close()
+    sim.close()
+
+
+def test_batch_upload_equals_per_scene_uploads():
+    """agimp_batch_set_particles with every scene's arrays concatenated in
+    batch order leaves each scene exactly as agimp_set_particles on each
+    would, also while an asynchronous positions readback is pending, and
+    the batch then steps to the same positions (up to the order of float
+    additions)."""
+    import ctypes
+
+    import torch
+
+    from agimp.batch import SceneBatch
+    sc = _batch_scenes()[:5] + [_batch_scenes()[6]]  # static scenes and the empty one
+    a_sims = [s.build() for s in sc]
+    b_sims = [s.build() for s in sc]
+    a, b = SceneBatch(a_sims), SceneBatch(b_sims)
+    a.substep(sc[0].dt, 2)
+    b.substep(sc[0].dt, 2)
+    rng = np.random.default_rng(3)
+    ups = []
+    for s in sc:
+        n, d = s.n, s.dim
+        ups.append(dict(x=(rng.uniform(0.3, 0.7, (n, d))).astype(np.float32),
+                        v=rng.normal(0, 1, (n, d)).astype(np.float32),
+                        F=(np.eye(d) + 0.01 * rng.normal(0, 1, (n, d, d))).astype(np.float32),
+                        C=(0.1 * rng.normal(0, 1, (n, d, d))).astype(np.float32),
+                        m=rng.uniform(0.5, 1.5, n).astype(np.float32),
+                        g=rng.integers(0, s.level, n).astype(np.int32),
+                        Jp=rng.uniform(0.9, 1.1, n).astype(np.float32)))
+    for sim, u in zip(a_sims, ups):
+        sim.set_particles(**u)
+    copy_s = torch.cuda.Stream()
+    pend = torch.empty((b.n_particles, 2), dtype=torch.float32, pin_memory=True).numpy()
+    b.positions(out=pend, blocking=False, stream=ctypes.c_void_p(copy_s.cuda_stream))
+    cat = {k: np.concatenate([u[k] for u in ups]) for k in ups[0]}
+    b.set_particles(**cat)
+    copy_s.synchronize()
+    for sa, sb in zip(a_sims, b_sims):
+        ga, gb = gpu_state(sa), gpu_state(sb)
+        for k in ga:
+            np.testing.assert_array_equal(ga[k], gb[k], err_msg=k)
+    a.substep(sc[0].dt, 3)
+    b.substep(sc[0].dt, 3)
+    for sa, sb in zip(a_sims, b_sims):
+        # float atomics: the two runs differ in the last bits only
+        xa, xb = sa.x_p.to_numpy(), sb.x_p.to_numpy()
+        assert xa.size == 0 or np.abs(xa - xb).max() <= 1e-5
+    with pytest.raises(ValueError):
+        b.set_particles(x=cat["x"][:-1])
+    a.close()
+    b.close()
+    for s in a_sims + b_sims:
+        s.close()
