@@ -168,21 +168,32 @@ static agimp_status build_maps(agimp_batch* b, cudaStream_t use) {
   long long sumN = 0;
   for (agimp_sim* s : b->sims) sumN += s->c.N;
   const long long G = (long long)b->sms * b->tune.ctas_per_sm;
+  // P2G: whole waves of resident CTAs (a partly filled last wave leaves SMs
+  // idle at the end of the kernel), at least as many CTAs as the other kinds
+  const int res = p2g_resident(b->dim, b->tune.chunk);
+  const long long wave = (long long)b->sms * res;
+  const long long GP = std::max<long long>(1, (G + wave - 1) / wave) * wave;
   int* Gm = b->hofs.data() + MAP_G * (n + 1);
   int* O = b->hofs.data() + MAP_O * (n + 1);
   int* T = b->hofs.data() + MAP_T * (n + 1);
-  Gm[0] = O[0] = T[0] = 0;
+  int* Pm = b->hofs.data() + MAP_P * (n + 1);
+  Gm[0] = O[0] = T[0] = Pm[0] = 0;
+  auto share = [&](long long tot, long long N) {
+    return n == 1 ? (int)std::max<long long>(1, tot)
+                  : (int)std::max<long long>(1, sumN ? (long long)std::llround((double)tot * N / sumN) : 1);
+  };
   for (int i = 0; i < n; ++i) {
     const long long N = b->sims[i]->c.N;
-    const int cg = n == 1 ? (int)std::max<long long>(1, G)
-                          : (int)std::max<long long>(1, sumN ? (long long)std::llround((double)G * N / sumN) : 1);
+    const int cg = share(G, N);
     Gm[i + 1] = Gm[i] + cg;
     O[i + 1] = O[i] + std::max(1, cg / 4);
     T[i + 1] = T[i] + 4 * cg;
+    Pm[i + 1] = Pm[i] + share(GP, N);
   }
   b->nct[MAP_G] = Gm[n];
   b->nct[MAP_O] = O[n];
   b->nct[MAP_T] = T[n];
+  b->nct[MAP_P] = Pm[n];
   BCK(cudaMemcpyAsync(b->dofs, b->hofs.data(), sizeof(int) * b->hofs.size(), cudaMemcpyHostToDevice, use));
   b->maps_valid = true;
   return AGIMP_OK;

@@ -792,7 +792,8 @@ __host__ __device__ __forceinline__ void axis_weights_half(float t, float* W, fl
 enum { MAP_G = 0,  // grid-stride kernels over particles, active blocks or work items
        MAP_O = 1,  // bin allocation (1024-thread CTAs)
        MAP_T = 2,  // staged level transfers (one 4^d block per CTA at a time: 4x MAP_G's CTAs)
-       NMAP = 3 };
+       MAP_P = 3,  // P2G: whole waves of the CTAs that fit an SM at once
+       NMAP = 4 };
 
 struct Batch {
   const Ctx* ctx;  // [n] scene contexts in device memory
@@ -905,6 +906,7 @@ constexpr int PHASES = 8;  // blocks, topology, binning, p2g, restrict, gridop, 
 void launch_substep(const BatchLaunch& bl, cudaStream_t s, cudaEvent_t* ev = nullptr);
 void launch_refine(const Ctx& c, int band, cudaStream_t s);
 void prepare_transfer_kernels();  // kernel attributes (shared-memory opt-in); once per device
+int p2g_resident(int dim, int chunk);  // k_p2g CTAs an SM holds at once
 // surrogate MLP forward over a device-side sample count (mlp.cu)
 void launch_mlp_forward_dev(const void* packed, const float* P, const float* X, float* Y, const int32_t* n_dev,
                             long long cap, int32_t* err, int sms, cudaStream_t s);

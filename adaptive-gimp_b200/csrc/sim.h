@@ -77,7 +77,7 @@ struct agimp_batch {
   std::vector<char> hvalid[2];
   int* dofs = nullptr;  // [NMAP][n + 1]
   std::vector<int> hofs;
-  int nct[agimp::NMAP] = {0, 0, 0};
+  int nct[agimp::NMAP] = {0, 0, 0, 0};
   bool maps_valid = false;
   cudaGraphExec_t gexec[2] = {nullptr, nullptr};
   Key gkey[2];

@@ -143,7 +143,7 @@ __device__ __forceinline__ void p2g_row_flush(float* tile, int TN, int cc, int n
 
 template <int D, int CH>
 __global__ void __launch_bounds__(CH, 1024 / CH) k_p2g(Batch B) {
-  SCENE_CTA(B, MAP_G);
+  SCENE_CTA(B, MAP_P);
   using Y = P2GLayout<D, CH>;
   extern __shared__ float4 dsm4[];
   float* pd = (float*)dsm4;             // [CH][STRIDE]
@@ -1610,6 +1610,28 @@ static void set_p2g_smem() {
   cudaFuncSetAttribute(k_p2g<D, CH>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)P2GLayout<D, CH>::bytes());
 }
 
+// CTAs of k_p2g<dim, chunk> that one SM holds at once (shared memory bound)
+int p2g_resident(int dim, int chunk) {
+  int n = 0;
+  auto occ = [&](auto k, int ch, size_t smem) { cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k, ch, smem); };
+  if (dim == 2) {
+    switch (chunk) {
+      case 64: occ(k_p2g<2, 64>, 64, P2GLayout<2, 64>::bytes()); break;
+      case 128: occ(k_p2g<2, 128>, 128, P2GLayout<2, 128>::bytes()); break;
+      case 512: occ(k_p2g<2, 512>, 512, P2GLayout<2, 512>::bytes()); break;
+      default: occ(k_p2g<2, 256>, 256, P2GLayout<2, 256>::bytes()); break;
+    }
+  } else {
+    switch (chunk) {
+      case 64: occ(k_p2g<3, 64>, 64, P2GLayout<3, 64>::bytes()); break;
+      case 128: occ(k_p2g<3, 128>, 128, P2GLayout<3, 128>::bytes()); break;
+      case 512: occ(k_p2g<3, 512>, 512, P2GLayout<3, 512>::bytes()); break;
+      default: occ(k_p2g<3, 256>, 256, P2GLayout<3, 256>::bytes()); break;
+    }
+  }
+  return n > 0 ? n : 1;
+}
+
 void prepare_transfer_kernels() {
   set_p2g_smem<2, 64>();
   set_p2g_smem<2, 128>();
@@ -1623,7 +1645,7 @@ void prepare_transfer_kernels() {
 
 template <int D>
 static void launch_p2g(const BatchLaunch& bl, cudaStream_t s, bool pdl) {
-  const int G = bl.nct[MAP_G];
+  const int G = bl.nct[MAP_P];
   switch (bl.chunk) {
     case 64: launch_k(pdl, k_p2g<D, 64>, G, 64, P2GLayout<D, 64>::bytes(), s, bl.b); break;
     case 128: launch_k(pdl, k_p2g<D, 128>, G, 128, P2GLayout<D, 128>::bytes(), s, bl.b); break;
