@@ -97,7 +97,6 @@ __device__ __forceinline__ float2 dup2(float a) { return make_float2(a, a); }
 //     further barrier.
 template <int D, int CH>
 struct P2GLayout {
-  static constexpr int NC = 1 << (2 * D);        // cells per block
   static constexpr int ROWS = (D == 2) ? 3 : 9;   // node rows per stencil
   static constexpr int SLOTS = 32 / ROWS;         // particle ranges served by one warp at once
   static constexpr int TN = (D == 2) ? 36 : 216;  // nodes of the (4+2)^d tile
@@ -801,13 +800,10 @@ __global__ void k_prolong_gather(Batch B, int l) {
   }
 }
 
-#ifndef AGIMP_TRANSFER_GATHER_3D
-#define AGIMP_TRANSFER_GATHER_3D 0
-#endif
 // 3D scenes stage their transfers through shared memory, 2D scenes gather
 template <int D>
 constexpr bool staged_transfers() {
-  return D == 3 && !AGIMP_TRANSFER_GATHER_3D;
+  return D == 3;
 }
 
 // ---------------------------------------------------------------------------
