@@ -255,7 +255,11 @@ def test_batched_surrogate_matches_scenes_alone():
     for a, b in zip(alone, together):
         assert a.errors() & ~2 == 0 and b.errors() & ~2 == 0
         xa, xb = a.x_p.to_numpy(), b.x_p.to_numpy()
-        assert np.abs(xa - xb).max() <= 1e-5, np.abs(xa - xb).max()
+        # float-atomics noise, grown through the collision: well below a
+        # finest cell (2e-3); a projection applied to the wrong scene or slot
+        # moves particles by cells
+        assert np.abs(xa - xb).max() <= 1e-4, np.abs(xa - xb).max()
+        assert np.sqrt(np.mean((xa - xb) ** 2)) <= 1e-5
     batch.close()
     for s in alone + together:
         s.close()
