@@ -167,7 +167,7 @@ def test_snow_skip_is_sound(h, dim):
 @pytest.mark.parametrize("dim", [2, 3])
 def test_corner_elements_match_elem_of(h, dim):
     """The per-axis corner indices of the binning's level search give the
-    same element (and the same in-store verdict) as elem_of / in_store for
+    same element (and the same in-store answer) as elem_of / in_store for
     every corner, block boundaries and the store's edges included."""
     rng = np.random.default_rng(11)
     nb = 19  # 64 cells per axis + 3 halo blocks
