@@ -499,6 +499,8 @@ template <int D>
 struct Stage {
   static constexpr int PER = 1 << (2 * D);
   static constexpr uint32_t NODE_BYTES = PER * 16, MASK_BYTES = PER * 4;
+  // the lanes of the first warp (a 2D CTA has 16 threads)
+  static constexpr unsigned WARP0 = PER >= 32 ? 0xffffffffu : ((1u << PER) - 1u);
 };
 
 __device__ __forceinline__ void mbar_expect_tx(uint64_t* m, uint32_t bytes) {
@@ -571,9 +573,11 @@ __global__ void __launch_bounds__(Stage<D>::PER) k_restrict(Batch B, int l) {
     int Bc[D];
     block_coords<D>(blk, (unsigned)Vc.nb, Bc);
     if (restrict_l) {
-      if (threadIdx.x == 0) {
+      if (threadIdx.x < 32) {
+        // lane t of the first warp stages fine block t (NB <= 32)
+        const int t = threadIdx.x;
         uint32_t bytes = 0;
-        for (int t = 0; t < NB; ++t) {
+        if (t < NB) {
           bool ok = true;
           unsigned fb = 0;
           int tt = t, fc[D];
@@ -586,17 +590,18 @@ __global__ void __launch_bounds__(Stage<D>::PER) k_restrict(Batch B, int l) {
 #pragma unroll
           for (int d = 0; d < D; ++d) fb = fb * (unsigned)Vf.nb + (unsigned)fc[d];
           fok[t] = ok ? (int)fb : -1;
-          if (ok) bytes += S::NODE_BYTES + S::MASK_BYTES;
+          if (ok) bytes = S::NODE_BYTES + S::MASK_BYTES;
         }
+        bytes = __reduce_add_sync(S::WARP0, bytes);
         // earlier generic reads of the tile finished at the barrier that
         // ended the previous block; order them before the async writes
         umma::fence_proxy_async();
-        mbar_expect_tx(&mbar, bytes);
-        for (int t = 0; t < NB; ++t)
-          if (fok[t] >= 0) {
-            bulk_to_shared(fn[t], Vf.node + ((long long)fok[t] << (2 * D)), S::NODE_BYTES, &mbar);
-            bulk_to_shared(fm[t], Vf.nm + ((long long)fok[t] << (2 * D)), S::MASK_BYTES, &mbar);
-          }
+        if (t == 0) mbar_expect_tx(&mbar, bytes);
+        __syncwarp(S::WARP0);
+        if (t < NB && fok[t] >= 0) {
+          bulk_to_shared(fn[t], Vf.node + ((long long)fok[t] << (2 * D)), S::NODE_BYTES, &mbar);
+          bulk_to_shared(fm[t], Vf.nm + ((long long)fok[t] << (2 * D)), S::MASK_BYTES, &mbar);
+        }
       }
       __syncthreads();  // fok
       const bool ok = stage_wait(c, &mbar, phase);
@@ -863,9 +868,11 @@ __global__ void __launch_bounds__(Stage<D>::PER) k_prolong(Batch B, int l) {
     block_coords<D>(blk, (unsigned)Vf.nb, Bf);
 #pragma unroll
     for (int d = 0; d < D; ++d) C0[d] = (2 * Bf[d] + 1) >> 2;
-    if (threadIdx.x == 0) {
+    if (threadIdx.x < 32) {
+      // lane t of the first warp stages coarse block t
+      const int t = threadIdx.x;
       uint32_t bytes = 0;
-      for (int t = 0; t < NB; ++t) {
+      if (t < NB) {
         bool ok = true;
         unsigned cb = 0;
 #pragma unroll
@@ -875,15 +882,16 @@ __global__ void __launch_bounds__(Stage<D>::PER) k_prolong(Batch B, int l) {
           cb = cb * (unsigned)Vc.nb + (unsigned)q;
         }
         cok[t] = ok ? (int)cb : -1;
-        if (ok) bytes += S::NODE_BYTES + S::MASK_BYTES;
+        if (ok) bytes = S::NODE_BYTES + S::MASK_BYTES;
       }
+      bytes = __reduce_add_sync(S::WARP0, bytes);
       umma::fence_proxy_async();
-      mbar_expect_tx(&mbar, bytes);
-      for (int t = 0; t < NB; ++t)
-        if (cok[t] >= 0) {
-          bulk_to_shared(cn[t], Vc.node + ((long long)cok[t] << (2 * D)), S::NODE_BYTES, &mbar);
-          bulk_to_shared(cm[t], Vc.nm + ((long long)cok[t] << (2 * D)), S::MASK_BYTES, &mbar);
-        }
+      if (t == 0) mbar_expect_tx(&mbar, bytes);
+      __syncwarp(S::WARP0);
+      if (t < NB && cok[t] >= 0) {
+        bulk_to_shared(cn[t], Vc.node + ((long long)cok[t] << (2 * D)), S::NODE_BYTES, &mbar);
+        bulk_to_shared(cm[t], Vc.nm + ((long long)cok[t] << (2 * D)), S::MASK_BYTES, &mbar);
+      }
     }
     __syncthreads();  // cok
     const bool okw = stage_wait(c, &mbar, phase);
