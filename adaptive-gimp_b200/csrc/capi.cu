@@ -356,6 +356,10 @@ agimp_status agimp_create(const agimp_params* p, int32_t device, agimp_sim** out
       AL(V.nm, V.nblocks * per);
       cudaMemset(V.nm, 0, V.nblocks * per * sizeof(uint32_t));
     }
+    if (l < c.L - 1) {
+      AL(V.dflag, V.nblocks);
+      cudaMemset(V.dflag, 0, V.nblocks * sizeof(uint32_t));
+    }
   }
   AL(c.ctr, CTR_COUNT);
   cudaMemset(c.ctr, 0, CTR_COUNT * sizeof(int32_t));

@@ -64,6 +64,11 @@ struct LevelDev {
   // the node mask itself; coarser levels get a copy after ghost / T-junction
   // marking, so the level transfers read whole blocks of it
   uint32_t* nm;
+  // levels below the finest: per block, 1 + the largest radius around which
+  // k_dilate has activated this substep's blocks (0: none; cleared through
+  // the touch list), so touched blocks with a common ancestor walk its
+  // neighbourhood once
+  uint32_t* dflag;
 };
 
 struct Particles {

@@ -336,6 +336,16 @@ __global__ void k_dilate(Batch B) {
       const int items = (D == 2) ? w * w : w * w * w;
       const LevelDev& V = c.lev[l];
       const int s = c.L - 1 - l;
+      if (l < c.L - 1) {
+        // the touched blocks under one block of this level share its
+        // neighbourhood: only the first with at least this radius walks it
+        unsigned ba = 0;
+#pragma unroll
+        for (int d = 0; d < D; ++d) ba = ba * (unsigned)V.nb + (unsigned)((fb[d] >> s) + 1);
+        int done = 0;
+        if (lane == 0) done = atomicMax(&V.dflag[ba], (unsigned)R + 1u) >= (unsigned)R + 1u;
+        if (__shfl_sync(0xffffffffu, done, 0)) continue;
+      }
       for (int r = lane; r < items; r += 32) {
         int tt = r;
         unsigned b = 0;
@@ -417,6 +427,23 @@ __global__ void k_resolve(Batch B) {
     c.touch_flag[key] = 0u;
     if (c.is_static)
       for (int w = 0; w < ((D == 2) ? 1 : 5); ++w) c.touch_occ[(long long)key * ((D == 2) ? 1 : 5) + w] = 0u;
+    // k_dilate's per-ancestor marks of this touched block
+    const LevelDev& Vf = c.lev[c.L - 1];
+    int fb[D];
+    unsigned k = (unsigned)key;
+#pragma unroll
+    for (int d = D - 1; d >= 0; --d) {
+      fb[d] = (int)(k % (unsigned)Vf.nb) - 1;
+      k /= (unsigned)Vf.nb;
+    }
+    for (int l = 0; l < c.L - 1; ++l) {
+      const LevelDev& V = c.lev[l];
+      const int s = c.L - 1 - l;
+      unsigned ba = 0;
+#pragma unroll
+      for (int d = 0; d < D; ++d) ba = ba * (unsigned)V.nb + (unsigned)((fb[d] >> s) + 1);
+      if (V.dflag[ba]) V.dflag[ba] = 0u;
+    }
   }
   __shared__ BlockRanges br;
   load_block_ranges(c, br);
