@@ -301,6 +301,19 @@ __device__ __forceinline__ bool decode_elem(const Ctx& c, int l0, int l1, long l
   return false;
 }
 
+// Warp-aggregated slot reservation for the lanes that call it together (one
+// atomic per warp instead of one per lane: counters shared by a whole grid
+// serialise at L2)
+__device__ __forceinline__ int reserve_slot(int32_t* counter) {
+  const unsigned mask = __activemask();
+  const int lane = threadIdx.x & 31;
+  const int leader = __ffs(mask) - 1;
+  int base = 0;
+  if (lane == leader) base = atomicAdd(counter, __popc(mask));
+  base = __shfl_sync(mask, base, leader);
+  return base + __popc(mask & ((1u << lane) - 1u));
+}
+
 // First entry of each level's active blocks in the level-by-level block
 // numbering (s[q] = active blocks of the levels below q, s[L] = all of them),
 // read from the counters once per CTA: the per-element loops then decode an

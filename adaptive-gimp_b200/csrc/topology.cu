@@ -231,7 +231,7 @@ __device__ __forceinline__ void touch_one(const Ctx& c, int p) {
   const unsigned rmax = __reduce_max_sync(grp, reach);
   if ((int)(threadIdx.x & 31) == __ffs(grp) - 1 && c.touch_flag[key] < rmax &&
       atomicMax(&c.touch_flag[key], rmax) == 0u) {
-    const int i = atomicAdd(&c.ctr[CTR_TOUCH], 1);
+    const int i = reserve_slot(&c.ctr[CTR_TOUCH]);
     c.touch_list[i] = key;
   }
 }
@@ -362,7 +362,7 @@ __global__ void k_dilate(Batch B) {
         for (int d = 0; d < D; ++d) b = b * (unsigned)V.nb + (unsigned)cb[d];
         int* bm = &V.bmap[b];
         if (*bm == -1 && atomicCAS(bm, -1, -2) == -1) {
-          const int i = atomicAdd(&c.ctr[CTR_LEVEL + l], 1);
+          const int i = reserve_slot(&c.ctr[CTR_LEVEL + l]);
           V.blist[i] = (int)b;
           *bm = i;
         }
@@ -740,7 +740,7 @@ __global__ void __launch_bounds__(1024) k_offsets(Batch B) {
     if (cnt > 0) {
       const int start = s_base.x + inc.x - cnt;
       c.bin_start[b] = start;
-      c.full_bins[atomicAdd(&c.ctr[CTR_FULL], 1)] = (int)b;
+      c.full_bins[reserve_slot(&c.ctr[CTR_FULL])] = (int)b;
       const int ch0 = s_base.y + inc.y - nch;
       int l = -1, blk = 0;  // level -1 marks the extra bin
       if (b < nblk) {

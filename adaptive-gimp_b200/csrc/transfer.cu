@@ -1012,16 +1012,6 @@ __device__ __forceinline__ void snow_clamp_rebuild(const Ctx& c, const float* U,
     }
 }
 
-// warp-aggregated slot reservation for the lanes that call it together
-__device__ __forceinline__ int reserve_slot(int32_t* counter) {
-  const unsigned mask = __activemask();
-  const int lane = threadIdx.x & 31;
-  const int leader = __ffs(mask) - 1;
-  int base = 0;
-  if (lane == leader) base = atomicAdd(counter, __popc(mask));
-  base = __shfl_sync(mask, base, leader);
-  return base + __popc(mask & ((1u << lane) - 1u));
-}
 
 // The surrogate's domain: a non-inverted trial state with positive singular
 // values and plastic ratio.
