@@ -872,6 +872,11 @@ __device__ __forceinline__ const Ctx& scene_slice(const Batch& B, Ctx* sc, int& 
   unsigned* dst = (unsigned*)sc;
   for (int i = threadIdx.x; i < (int)(sizeof(Ctx) / 4); i += blockDim.x) dst[i] = __ldg(&src[i]);
   __syncthreads();
+  // The next kernel on the stream (a programmatic dependent, launch_k with
+  // pdl) may be scheduled once every CTA of this one has started: its CTAs
+  // fill the SM slots this kernel's last wave leaves free and run their own
+  // prologue, then wait below for this kernel to complete.
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
   // Launched as a programmatic dependent of the previous kernel on the stream
   // (launch_k with pdl), the CTA may have started before that kernel finished:
   // everything above reads only host-written launch data; wait here until the
